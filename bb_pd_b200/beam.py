@@ -1,0 +1,91 @@
+"""Synthetic concrete beams: the inputs the reference's MATLAB input module
+builds (input/scripts/Gregoire_beam_tests.m), made by libbbpd's host builder.
+
+`beam(...)` returns a dict of reference-named arrays, column-major like
+MATLAB: undeformedCoordinates (nNodes x 3), BONDLIST (nBonds x 2, 1-based),
+UNDEFORMEDLENGTH, BONDSTIFFNESS, VOLUMECORRECTIONFACTORS, nFAMILYMEMBERS,
+DENSITY, massVector, CONSTRAINTFLAG, BODYFORCEFLAG (the prescribed DOFs),
+and, with per-bond critical stretch, sc.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native as N
+
+
+def spec(nx: int, ny: int, nz: int, dx: float, *, horizon_factor: float = 3.015,
+         E: float = 37e9, stiffness_factor: float = 18.0, density: float = 2346.0,
+         supports: tuple[float, ...] = (), load_midspan_top: bool = True,
+         notch_x: float | None = None, notch_depth: float = 0.0,
+         sc_lognormal: tuple[float, float] | None = None, seed: int = 20261203) -> N.BeamSpec:
+    s = N.BeamSpec()
+    s.nx, s.ny, s.nz, s.dx = nx, ny, nz, dx
+    s.horizon_factor, s.E, s.stiffness_factor, s.density = horizon_factor, E, stiffness_factor, density
+    for i, x in enumerate(supports[:2]):
+        s.support_x[i] = x
+    s.n_supports = min(len(supports), 2)
+    s.load_midspan_top = int(load_midspan_top)
+    s.notch = int(notch_x is not None)
+    s.notch_x = notch_x if notch_x is not None else 0.0
+    s.notch_depth = notch_depth
+    s.sc_lognormal = int(sc_lognormal is not None)
+    if sc_lognormal is not None:
+        s.sc_mean, s.sc_cov = sc_lognormal
+    s.seed = seed
+    return s
+
+
+def count(s: N.BeamSpec) -> N.BeamScalars:
+    out = N.BeamScalars()
+    N.check(N.lib().bbpd_beam_count(s, out))
+    return out
+
+
+def build(s: N.BeamSpec) -> dict:
+    sc_ = count(s)
+    nN, nB = sc_.n_nodes, sc_.n_bonds
+    f = lambda *shape: np.zeros(shape, dtype=np.float64, order="F")
+    a = dict(undeformedCoordinates=f(nN, 3), BONDLIST=f(nB, 2), UNDEFORMEDLENGTH=f(nB),
+             BONDSTIFFNESS=f(nB), VOLUMECORRECTIONFACTORS=f(nB), nFAMILYMEMBERS=f(nN),
+             DENSITY=f(nN), massVector=f(nN), CONSTRAINTFLAG=f(nN, 3), BODYFORCEFLAG=f(nN, 3))
+    sc = f(nB) if s.sc_lognormal else None
+    N.check(N.lib().bbpd_beam_build(
+        s, N.ptr(a["undeformedCoordinates"]), N.ptr(a["BONDLIST"]), N.ptr(a["UNDEFORMEDLENGTH"]),
+        N.ptr(a["BONDSTIFFNESS"]), N.ptr(a["VOLUMECORRECTIONFACTORS"]), N.ptr(a["nFAMILYMEMBERS"]),
+        N.ptr(a["DENSITY"]), N.ptr(a["massVector"]), N.ptr(a["CONSTRAINTFLAG"]),
+        N.ptr(a["BODYFORCEFLAG"]), N.ptr(sc)))
+    if sc is not None:
+        a["sc"] = sc
+    a.update(nNodes=nN, nBonds=nB, horizon=sc_.horizon, cellVolume=sc_.cell_volume,
+             bondStiffnessConcrete=sc_.bond_stiffness_concrete, DT=sc_.dt,
+             nSupported=sc_.n_supported, nPrescribed=sc_.n_prescribed)
+    return a
+
+
+# The beams of the benchmark configurations. Dimensions: nx along the length,
+# ny across the width, nz through the depth (loading direction z).
+def config1() -> N.BeamSpec:
+    """500 x 100 (depth) x 50 (width) mm, dx 5 mm: 100 x 10 x 20 = 20 000 nodes."""
+    return spec(100, 10, 20, 5e-3, supports=(0.05, 0.45))
+
+
+def config2() -> N.BeamSpec:
+    """Same beam at dx 1.25 mm: 400 x 40 x 80 = 1 280 000 nodes."""
+    return spec(400, 40, 80, 1.25e-3, supports=(0.05, 0.45))
+
+
+def config3() -> N.BeamSpec:
+    """400 x 100 x 50 mm at dx 2.5 mm (160 x 20 x 40 = 128 000 nodes), supports at
+    50 and 350 mm, a 40 mm notch at 0.625 half-span right of midspan, lognormal sc."""
+    L = 0.4
+    half_span = 0.15
+    notch = 0.2 + 0.625 * half_span  # 293.75 mm: between two node planes
+    return spec(160, 20, 40, 2.5e-3, supports=(0.05, 0.35), notch_x=notch, notch_depth=0.04,
+                sc_lognormal=(2e-3, 0.1))
+
+
+def small(nx: int = 24, ny: int = 5, nz: int = 6, dx: float = 5e-3, **kw) -> N.BeamSpec:
+    """A small beam for parity tests (supports at 2 dx from each end)."""
+    kw.setdefault("supports", (3 * dx, (nx - 2) * dx))
+    return spec(nx, ny, nz, dx, **kw)

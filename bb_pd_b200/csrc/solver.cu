@@ -1,0 +1,1011 @@
+// Fused solver: the whole BB_PD time loop in one persistent cooperative kernel.
+//
+// Layout in HBM (built on the host at bbpd_create):
+//   nodes   SoA float64 (x of all nodes, then y, then z), in input order or
+//           Morton order; per-node flags byte (constrained / prescribed DOFs).
+//   bonds   every undirected bond is stored twice, once in the list of each
+//           end node ("directed entries"). Lists are kept in bond order and
+//           laid out as 32-node slices (SELL-32): entry k of the node in lane l
+//           of slice s sits at slice_ptr[s] + 32 k + l, so a warp that walks
+//           its 32 nodes' lists in step reads each per-entry array with
+//           128/256-byte coalesced loads. Per entry: a 32-bit word (neighbour
+//           index + chunk / state bits), the damage state BSF (float64), and the
+//           bond constants L0, BONDSTIFFNESS, VCF (float64).
+//
+// One time step (per launch, any number of steps):
+//   phase A  each warp takes a slice; each lane walks its node's entries,
+//            computes stretch, law, damage and bond force for every bond,
+//            and sums the forces in the reference's OpenMP order (chunk
+//            partials in bond order, added in chunk order). Both copies of a
+//            bond see bit-identical stretch (the squared components do not
+//            depend on direction), so both copies of the damage state evolve
+//            identically and no atomics or cross-warp exchange are needed.
+//            Euler-Cromer integrates the node right there; ADR writes the
+//            node's Rayleigh-quotient terms reduced over the warp.
+//   barrier  (ADR) the last block to arrive reduces the slice partials in a
+//            fixed order into the damping coefficient cn.
+//   phase B  (ADR) central-difference half-step update of every node.
+//   barrier  positions of step n+1 are visible to every block.
+// Grid barriers spin with a time limit; on expiry they set an error flag and
+// the kernel returns early (status BBPD_ERR_TIMEOUT), never hanging.
+#include "bbpd_internal.h"
+#include "physics.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <thread>
+#include <vector>
+
+using namespace bbpd;
+
+namespace {
+
+constexpr uint32_t COL_MASK = 0x00FFFFFFu;
+constexpr uint32_t F_CHUNK = 1u << 24;   // first entry of a new OpenMP chunk in this list
+constexpr uint32_t F_BROKEN = 1u << 25;  // fail == 0
+constexpr uint32_t F_SOFT = 1u << 26;    // flagBondSoftening == 1
+constexpr int BT_SHIFT = 27;             // bits 27-28: BONDTYPE
+constexpr int64_t MAX_NODES = (int64_t)1 << 24;
+
+constexpr int ERR_TIMEOUT = 1;
+constexpr int ERR_NONFINITE = 2;
+
+constexpr int kBlock = 256;
+constexpr int kStrands = 1024;
+
+struct Dev {
+    int64_t n_nodes, n_slices;
+    const int64_t *slice_ptr;
+    const int32_t *slice_len;
+    const int32_t *deg;
+    uint32_t *colw;
+    double *bsf;
+    const double *l0, *bs, *vcf;
+    const double *s0e, *s1e, *sce;   // per-entry law stretches or null
+    const double *X;
+    double *xb0, *xb1;               // positions: step n reads xb[(n-1)&1], writes xb[n&1]
+    double *u, *v, *a;
+    double *F0, *F1;                 // F of step n lives in F[n&1]
+    const double *mass, *rho;
+    const uint8_t *nflag;            // bit d: held (constrained or prescribed); bit 3+d: prescribed
+    double *part;                    // 2 * n_slices
+    double *scal;                    // [0] = cn
+    unsigned *bar;                   // [0] arrivals, [1] generation
+    int *err;
+    LawScalars P;
+    double V, dt, damping;
+    int amplitude;
+    double rate, applied_final;
+    int64_t n_time_steps;
+    double guard;
+    unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ double prescribed_value(const Dev &d, int64_t n)
+{
+    if (d.amplitude == BBPD_AMP_SMOOTHSTEP) {
+        // smoothstepdata(n, 1, nTimeSteps, 0, appliedDisplacement), smoothstepdata.m:40-42
+        double v0 = 0.0, v1 = d.applied_final;
+        double xi = ((double)n - 1.0) / ((double)d.n_time_steps - 1.0);
+        return v0 + (v1 - v0) * ((xi * xi) * xi) * (10 - 15 * xi + 6 * (xi * xi));
+    }
+    return d.rate * (double)n;
+}
+
+// Fixed-order reduction of the slice partials (1024 strands, xor butterfly)
+// and the clamp of calculatedampingcoefficient.m:90-112; run by one block.
+__device__ void compute_cn(const Dev &d)
+{
+    __shared__ double a1[kStrands], a2[kStrands];
+    const int64_t ns = d.n_slices;
+    for (int r = threadIdx.x; r < kStrands; r += blockDim.x) {
+        double c1 = 0.0, c2 = 0.0;
+#pragma unroll 8
+        for (int64_t k = r; k < ns; k += kStrands) {
+            c1 = c1 + __ldcg(&d.part[k]);
+            c2 = c2 + __ldcg(&d.part[ns + k]);
+        }
+        a1[r] = c1;
+        a2[r] = c2;
+    }
+    __syncthreads();
+    constexpr int PER = kStrands / kBlock;
+    for (int off = kStrands / 2; off >= 1; off >>= 1) {
+        double n1[PER], n2[PER];
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            int r = threadIdx.x + q * kBlock;
+            n1[q] = a1[r] + a1[r ^ off];
+            n2[q] = a2[r] + a2[r ^ off];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            int r = threadIdx.x + q * kBlock;
+            a1[r] = n1[q];
+            a2[r] = n2[q];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double cn1 = a1[0], cn2 = a2[0], cn;
+        if (cn2 != 0) {
+            if ((cn1 / cn2) > 0) cn = 2 * sqrt(cn1 / cn2);
+            else cn = 0;
+        } else {
+            cn = 0;
+        }
+        if (cn > 2) cn = 1.9;
+        d.scal[0] = cn;
+        __threadfence();
+    }
+}
+
+// Wait until *word differs from `old`, at most timeout_ns. Gives up early when
+// another block already reported a timeout in *err. On expiry sets
+// ERR_TIMEOUT in *err and returns false; never waits without a limit.
+__device__ bool bounded_wait_change(volatile unsigned *word, unsigned old, int *err,
+                                    unsigned long long timeout_ns)
+{
+    const unsigned long long t0 = globaltimer();
+    while (*word == old) {
+        if (*(volatile int *)err & ERR_TIMEOUT) return false;
+        if (globaltimer() - t0 > timeout_ns) {
+            atomicOr(err, ERR_TIMEOUT);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    return true;
+}
+
+// Grid-wide barrier with a time limit. The last block to arrive optionally
+// computes cn before releasing the others. Returns false on timeout.
+__device__ bool grid_barrier(const Dev &d, bool do_cn)
+{
+    __shared__ int s_last, s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = d.bar + 1;
+        unsigned g = *gen;
+        __threadfence();
+        unsigned prev = atomicAdd(d.bar, 1u);
+        s_last = (prev == gridDim.x - 1);
+        s_ok = 1;
+        if (!s_last) s_ok = bounded_wait_change(gen, g, d.err, d.timeout_ns) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_last) {
+        if (do_cn) compute_cn(d);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            d.bar[0] = 0;
+            __threadfence();
+            atomicAdd(d.bar + 1, 1u);
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// One bond seen from node i: stretch, law and damage update (state written
+// back only when it changes), and the bond force added to the chunk partial.
+template <int LAW, int PREC>
+__device__ __forceinline__ void bond_entry(const Dev &d, int64_t e, double xi, double yi,
+                                           double zi, const double *__restrict__ xs,
+                                           double &tx, double &ty, double &tz, double &ax,
+                                           double &ay, double &az)
+{
+    const int64_t nN = d.n_nodes;
+    uint32_t w = d.colw[e];
+    int64_t j = w & COL_MASK;
+    if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
+        tx = tx + ax; ty = ty + ay; tz = tz + az;
+        ax = 0.0; ay = 0.0; az = 0.0;
+    }
+    double xj = xs[j], yj = xs[j + nN], zj = xs[j + 2 * nN];
+    double l0 = __ldg(&d.l0[e]);
+    int bt = (w >> BT_SHIFT) & 3;
+    double s0b = d.s0e ? __ldg(&d.s0e[e]) : d.P.s0;
+    double s1b = d.s1e ? __ldg(&d.s1e[e]) : d.P.s1;
+    double scb = d.sce ? __ldg(&d.sce[e]) : d.P.sc;
+    double dX, dY, dZ, L, s;
+    float dXf = 0.f, dYf = 0.f, dZf = 0.f, Lf = 0.f, sf = 0.f;
+    bool exact = true;
+    if (PREC == BBPD_PREC_FP64) {
+        bond_kinematics(xi, yi, zi, xj, yj, zj, l0, dX, dY, dZ, L, s);
+    } else {
+        // FP64 difference and squared length (no cancellation loss), FP32 rest:
+        // s = (L^2 - L0^2) / (L0 (L + L0)).
+        dX = xj - xi; dY = yj - yi; dZ = zj - zi;
+        double L2 = dX * dX + dY * dY + dZ * dZ;
+        double diff = L2 - l0 * l0;
+        float l0f = (float)l0;
+        Lf = sqrtf((float)L2);
+        sf = (float)diff / (l0f * (Lf + l0f));
+        dXf = (float)dX; dYf = (float)dY; dZf = (float)dZ;
+        // guard band: the stretch that decides breakage is recomputed in FP64
+        double crit = scb;
+        if (LAW == BBPD_LAW_LINEAR) crit = (bt == 1) ? 3 * scb : (bt == 2 ? d.P.sc_steel : scb);
+        exact = fabs((double)sf - crit) < d.guard;
+        if (exact) {
+            L = sqrt(L2);
+            s = (L - l0) / l0;
+        } else {
+            s = (double)sf;
+            L = (double)Lf;
+        }
+    }
+    double B = d.bsf[e];
+    const double B0 = B;
+    bool soft = (w & F_SOFT) != 0;
+    double failv = (w & F_BROKEN) ? 0.0 : 1.0;
+    const bool concrete = (bt == 0);
+    if (LAW == BBPD_LAW_TRILINEAR) {
+        law_trilinear(s, s0b, s1b, scb, d.P, d.s0e != nullptr || d.s1e != nullptr, concrete, B, soft);
+    } else if (LAW == BBPD_LAW_BILINEAR) {
+        law_bilinear(s, s0b, scb, concrete, B, soft);
+    } else if (LAW == BBPD_LAW_EXPONENTIAL) {
+        law_exponential(s, s0b, scb, d.P, concrete, B, soft);
+    } else {
+        law_linear(s, scb, d.P, bt, failv);
+    }
+    uint32_t w2 = (w & ~(F_SOFT | F_BROKEN)) | (soft ? F_SOFT : 0u) | (failv == 0.0 ? F_BROKEN : 0u);
+    if (w2 != w) d.colw[e] = w2;
+    if (__double_as_longlong(B) != __double_as_longlong(B0)) d.bsf[e] = B;
+    double bsv = __ldg(&d.bs[e]), vcf = __ldg(&d.vcf[e]);
+    if (PREC == BBPD_PREC_FP64 || exact) {
+        double t = bond_force_scalar(failv, bsv, B, s, 0.0, d.V, vcf);
+        ax = ax + bond_force_component(t, dX, L);
+        ay = ay + bond_force_component(t, dY, L);
+        az = az + bond_force_component(t, dZ, L);
+    } else {
+        float t = (float)(failv * bsv * (1 - B)) * sf * (float)(d.V * vcf);
+        float r = t / Lf;
+        float fx = r * dXf, fy = r * dYf, fz = r * dZf;
+        if (fx != fx) fx = 0.f;
+        if (fy != fy) fy = 0.f;
+        if (fz != fz) fz = 0.f;
+        ax = ax + (double)fx;
+        ay = ay + (double)fy;
+        az = az + (double)fz;
+    }
+}
+
+template <int LAW, int SCHEME, int PREC>
+__global__ void __launch_bounds__(kBlock) step_kernel(Dev d, int64_t step0, int64_t nsteps)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nN = d.n_nodes;
+
+    for (int64_t it = 0; it < nsteps; it++) {
+        const int64_t n = step0 + it;
+        double *Fc = (n & 1) ? d.F1 : d.F0;
+        const double *Fp = (n & 1) ? d.F0 : d.F1;
+        const double *xs = ((n - 1) & 1) ? d.xb1 : d.xb0;
+        double *xn = (n & 1) ? d.xb1 : d.xb0;
+        const double Un1 = prescribed_value(d, n + 1);
+
+        // ---- phase A: bond forces (+ Euler-Cromer / ADR terms) ----
+        for (int64_t sl = gwarp; sl < d.n_slices; sl += nwarps) {
+            const int64_t i = sl * 32 + lane;
+            const bool valid = i < nN;
+            const int dg = valid ? d.deg[i] : 0;
+            const int len = d.slice_len[sl];
+            const int64_t base = d.slice_ptr[sl] + lane;
+            double xi = 0, yi = 0, zi = 0;
+            if (valid) { xi = xs[i]; yi = xs[i + nN]; zi = xs[i + 2 * nN]; }
+            double tx = 0.0, ty = 0.0, tz = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+            for (int k = 0; k < len; k++) {
+                if (k < dg)
+                    bond_entry<LAW, PREC>(d, base + (int64_t)k * 32, xi, yi, zi, xs, tx, ty, tz, ax, ay, az);
+            }
+            tx = tx + ax; ty = ty + ay; tz = tz + az;
+            if (SCHEME == BBPD_SCHEME_EULERCROMER) {
+                if (valid) {
+                    // timeintegrationeulercromerMex.c:33-50 on the node just summed
+                    const uint8_t fl = d.nflag[i];
+                    const double Fv[3] = {tx, ty, tz};
+                    bool bad = false;
+#pragma unroll
+                    for (int dof = 0; dof < 3; dof++) {
+                        const int64_t e = i + nN * dof;
+                        Fc[e] = Fv[dof];
+                        double ae = (Fv[dof] - d.damping * d.v[e]) / d.rho[i];
+                        if (fl & (1 << dof)) ae = 0;
+                        double ve = d.v[e] + (ae * d.dt);
+                        double ue = d.u[e] + (ve * d.dt);
+                        double xe = d.X[e] + ue;
+                        if (fl & (8 << dof)) { ue = Un1; xe = d.X[e] + ue; }
+                        if (d.a) d.a[e] = ae;
+                        d.v[e] = ve; d.u[e] = ue; xn[e] = xe;
+                        bad |= !isfinite(ue) || !isfinite(ve);
+                    }
+                    if (bad) atomicOr(d.err, ERR_NONFINITE);
+                }
+            } else {
+                // calculatedampingcoefficient.m:61-85 terms of this node, then the
+                // xor butterfly over the slice's 32 lanes
+                double c1 = 0, c2 = 0;
+                if (valid) {
+                    Fc[i] = tx; Fc[i + nN] = ty; Fc[i + 2 * nN] = tz;
+                    const double m = d.mass[i];
+                    const double Fv[3] = {tx, ty, tz};
+#pragma unroll
+                    for (int dof = 0; dof < 3; dof++) {
+                        const int64_t e = i + nN * dof;
+                        double vhp = d.v[e], ue = d.u[e];
+                        if (vhp != 0) c1 = c1 - ue * ue * ((Fv[dof] / m - Fp[e] / m) / (d.dt * vhp));
+                    }
+#pragma unroll
+                    for (int dof = 0; dof < 3; dof++) {
+                        double ue = d.u[i + nN * dof];
+                        c2 = c2 + ue * ue;
+                    }
+                }
+#pragma unroll
+                for (int off = 16; off >= 1; off >>= 1) {
+                    c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
+                    c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
+                }
+                if (lane == 0) { d.part[sl] = c1; d.part[d.n_slices + sl] = c2; }
+            }
+        }
+        if (SCHEME == BBPD_SCHEME_ADR) {
+            if (!grid_barrier(d, true)) return;
+            // ---- phase B: timeintegrationADR.m:168-197 ----
+            const double cn = __ldcg(&d.scal[0]);
+            for (int64_t sl = gwarp; sl < d.n_slices; sl += nwarps) {
+                const int64_t i = sl * 32 + lane;
+                if (i >= nN) continue;
+                const uint8_t fl = d.nflag[i];
+                const double minv = 1.0 / d.mass[i];
+                bool bad = false;
+#pragma unroll
+                for (int dof = 0; dof < 3; dof++) {
+                    const int64_t e = i + nN * dof;
+                    double F = Fc[e], vh;
+                    if (n == 1) vh = 0.5 * d.dt * minv * F;
+                    else vh = (((2 - cn * d.dt) * d.v[e]) + (2 * d.dt * minv * F)) / (2 + cn * d.dt);
+                    double ue = d.u[e] + (d.dt * vh);
+                    if (fl & (1 << dof)) { ue = 0; vh = 0; }
+                    if (fl & (8 << dof)) { ue = Un1; vh = 0; }
+                    d.v[e] = vh; d.u[e] = ue; xn[e] = d.X[e] + ue;
+                    bad |= !isfinite(ue) || !isfinite(vh);
+                }
+                if (bad) atomicOr(d.err, ERR_NONFINITE);
+            }
+        }
+        if (!grid_barrier(d, false)) return;
+    }
+}
+
+// Self-test of the bounded wait: one thread waits on a word that nothing
+// writes, so the wait must expire and report ERR_TIMEOUT.
+__global__ void wait_selftest_kernel(unsigned *word, int *err, unsigned long long timeout_ns)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) bounded_wait_change(word, 0u, err, timeout_ns);
+}
+
+typedef void (*kernel_t)(Dev, int64_t, int64_t);
+
+template <int LAW, int SCHEME>
+kernel_t pick_prec(int prec)
+{
+    return prec == BBPD_PREC_FP32 ? step_kernel<LAW, SCHEME, BBPD_PREC_FP32>
+                                  : step_kernel<LAW, SCHEME, BBPD_PREC_FP64>;
+}
+
+template <int LAW>
+kernel_t pick_scheme(int scheme, int prec)
+{
+    return scheme == BBPD_SCHEME_ADR ? pick_prec<LAW, BBPD_SCHEME_ADR>(prec)
+                                     : pick_prec<LAW, BBPD_SCHEME_EULERCROMER>(prec);
+}
+
+kernel_t pick_kernel(int law, int scheme, int prec)
+{
+    switch (law) {
+    case BBPD_LAW_LINEAR: return pick_scheme<BBPD_LAW_LINEAR>(scheme, prec);
+    case BBPD_LAW_BILINEAR: return pick_scheme<BBPD_LAW_BILINEAR>(scheme, prec);
+    case BBPD_LAW_TRILINEAR: return pick_scheme<BBPD_LAW_TRILINEAR>(scheme, prec);
+    default: return pick_scheme<BBPD_LAW_EXPONENTIAL>(scheme, prec);
+    }
+}
+
+// ------------------------------------------------------------------ host side
+
+template <class F>
+void host_parallel_for(int64_t n, F fn)
+{
+    unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (n < 65536) nt = 1;
+    std::vector<std::thread> th;
+    int64_t per = (n + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; t++) {
+        int64_t lo = (int64_t)t * per, hi = std::min(n, lo + per);
+        if (lo >= hi) break;
+        th.emplace_back([=]() { for (int64_t i = lo; i < hi; i++) fn(i); });
+    }
+    for (auto &x : th) x.join();
+}
+
+inline int chunk_of_host(int64_t k, int64_t n, int T)
+{
+    int64_t q = n / T, r = n % T, big = r * (q + 1);
+    if (k < big) return (int)(k / (q + 1));
+    return (int)(r + (k - big) / q);
+}
+
+uint64_t morton3(uint32_t a, uint32_t b, uint32_t c)
+{
+    auto spread = [](uint64_t v) {
+        v &= 0x1fffff;
+        v = (v | v << 32) & 0x1f00000000ffffull;
+        v = (v | v << 16) & 0x1f0000ff0000ffull;
+        v = (v | v << 8) & 0x100f00f00f00f00full;
+        v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+        v = (v | v << 2) & 0x1249249249249249ull;
+        return v;
+    };
+    return spread(a) | (spread(b) << 1) | (spread(c) << 2);
+}
+
+template <class T>
+int upload(T **d, const std::vector<T> &h)
+{
+    size_t b = sizeof(T) * std::max<size_t>(h.size(), 1);
+    BBPD_CUDA_TRY(cudaMalloc((void **)d, b));
+    if (!h.empty()) BBPD_CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    return BBPD_OK;
+}
+
+}  // namespace
+
+struct bbpd_solver {
+    int device = 0;
+    bbpd_params prm{};
+    int64_t nN = 0, nB = 0, ns = 0, ne = 0;
+    int64_t step = 1;
+    double cn = 0;
+    std::vector<int32_t> perm;      // device position -> input node
+    std::vector<int32_t> inv;       // input node -> device position
+    std::vector<int64_t> ent_i, ent_j;  // bond -> entry positions of its two copies
+    Dev d{};
+    std::vector<void *> allocs;
+    int64_t device_bytes = 0;
+    double bytes_per_step = 0;
+    kernel_t kernel = nullptr;
+    int grid = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool has_a = false;
+
+    template <class T>
+    int alloc(T **p, size_t count)
+    {
+        size_t b = sizeof(T) * std::max<size_t>(count, 1);
+        BBPD_CUDA_TRY(cudaMalloc((void **)p, b));
+        allocs.push_back((void *)*p);
+        device_bytes += (int64_t)b;
+        return BBPD_OK;
+    }
+    template <class T>
+    int put(T **p, const std::vector<T> &h)
+    {
+        int rc = alloc(p, h.size());
+        if (rc) return rc;
+        if (!h.empty())
+            BBPD_CUDA_TRY(cudaMemcpy(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+        return BBPD_OK;
+    }
+    ~bbpd_solver()
+    {
+        for (void *p : allocs) cudaFree(p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+#define TRY(x) do { int r_ = (x); if (r_) return r_; } while (0)
+
+static int validate_01(const double *a, int64_t n, const char *name)
+{
+    if (!a) return BBPD_OK;
+    for (int64_t i = 0; i < n; i++)
+        if (!(a[i] == 0.0 || a[i] == 1.0)) return fail(BBPD_ERR_ARG, "%s[%lld] is %g, expected 0 or 1", name, (long long)i, a[i]);
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int device,
+                           bbpd_solver **out)
+{
+    clear_error();
+    if (!pb || !prm || !out) return fail(BBPD_ERR_ARG, "null argument");
+    *out = nullptr;
+    TRY(require_device());
+    const int64_t nN = pb->n_nodes, nB = pb->n_bonds;
+    if (nN < 1 || nB < 0) return fail(BBPD_ERR_ARG, "n_nodes must be >= 1 and n_bonds >= 0");
+    if (nN >= MAX_NODES) return fail(BBPD_ERR_UNSUPPORTED, "at most %lld nodes per solver", (long long)MAX_NODES - 1);
+    if (!pb->undeformed_coordinates || (nB && (!pb->bondlist || !pb->undeformed_length ||
+        !pb->bond_stiffness || !pb->volume_correction)))
+        return fail(BBPD_ERR_ARG, "missing coordinates or bond arrays");
+    if (prm->law < 0 || prm->law > 3 || prm->scheme < 0 || prm->scheme > 1 || prm->precision < 0 ||
+        prm->precision > 1 || prm->n_chunks < 1 || prm->n_chunks > 4096)
+        return fail(BBPD_ERR_ARG, "bad law/scheme/precision/n_chunks");
+    if (!(prm->failure_functionality == 0.0 || prm->failure_functionality == 1.0))
+        return fail(BBPD_ERR_UNSUPPORTED, "failure_functionality must be 0 or 1");
+    if (prm->scheme == BBPD_SCHEME_ADR && !pb->mass) return fail(BBPD_ERR_ARG, "ADR needs mass");
+    if (prm->scheme == BBPD_SCHEME_EULERCROMER && !pb->density) return fail(BBPD_ERR_ARG, "Euler-Cromer needs density");
+    if (prm->amplitude == BBPD_AMP_SMOOTHSTEP && prm->n_time_steps < 2)
+        return fail(BBPD_ERR_ARG, "smooth step needs n_time_steps >= 2");
+    TRY(validate_01(pb->fail, nB, "fail"));
+    TRY(validate_01(pb->constraint_flag, 3 * nN, "CONSTRAINTFLAG"));
+    TRY(validate_01(pb->prescribed_flag, 3 * nN, "prescribed flag"));
+    if (pb->bond_type)
+        for (int64_t k = 0; k < nB; k++) {
+            double t = pb->bond_type[k];
+            if (!(t == 0 || t == 1 || t == 2)) return fail(BBPD_ERR_ARG, "BONDTYPE[%lld] = %g", (long long)k, t);
+        }
+    if (pb->stretch_plastic)
+        for (int64_t k = 0; k < nB; k++)
+            if (pb->stretch_plastic[k] != 0)
+                return fail(BBPD_ERR_UNSUPPORTED, "non-zero stretchPlastic (steel plasticity) is not on this path");
+    // BONDLIST: integers in [1, nN], no self-bonds
+    {
+        const double *bl = pb->bondlist;
+        for (int64_t k = 0; k < nB; k++) {
+            double a = bl[k], b = bl[nB + k];
+            if (!(a >= 1 && b >= 1 && a <= (double)nN && b <= (double)nN && a == std::floor(a) &&
+                  b == std::floor(b) && a != b))
+                return fail(BBPD_ERR_ARG, "BONDLIST row %lld = (%g, %g) is not a pair of distinct node ids", (long long)k + 1, a, b);
+        }
+    }
+
+    TRY(cudaSetDevice(device) == cudaSuccess ? 0 : fail(BBPD_ERR_CUDA, "cudaSetDevice(%d)", device));
+    auto *S = new bbpd_solver;
+    std::unique_ptr<bbpd_solver> guard_(S);
+    S->device = device;
+    S->prm = *prm;
+    S->nN = nN;
+    S->nB = nB;
+    const int T = prm->n_chunks;
+
+    // node order
+    S->perm.resize(nN);
+    S->inv.resize(nN);
+    std::iota(S->perm.begin(), S->perm.end(), 0);
+    if (prm->node_order == BBPD_ORDER_MORTON) {
+        const double *X = pb->undeformed_coordinates;
+        double lo[3], hi[3];
+        for (int c = 0; c < 3; c++) {
+            lo[c] = *std::min_element(X + c * nN, X + (c + 1) * nN);
+            hi[c] = *std::max_element(X + c * nN, X + (c + 1) * nN);
+        }
+        std::vector<uint64_t> key(nN);
+        for (int64_t i = 0; i < nN; i++) {
+            uint32_t q[3];
+            for (int c = 0; c < 3; c++) {
+                double span = hi[c] - lo[c];
+                q[c] = span > 0 ? (uint32_t)((X[i + c * nN] - lo[c]) / span * 2097151.0) : 0;
+            }
+            key[i] = morton3(q[0], q[1], q[2]);
+        }
+        std::stable_sort(S->perm.begin(), S->perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    }
+    for (int64_t p = 0; p < nN; p++) S->inv[S->perm[p]] = (int32_t)p;
+
+    // SELL-32 slices
+    const int64_t ns = (nN + 31) / 32;
+    S->ns = ns;
+    std::vector<int32_t> deg(nN, 0);
+    const double *bl = pb->bondlist;
+    for (int64_t k = 0; k < nB; k++) {
+        deg[S->inv[(int64_t)bl[k] - 1]]++;
+        deg[S->inv[(int64_t)bl[nB + k] - 1]]++;
+    }
+    std::vector<int32_t> slen(ns, 0);
+    std::vector<int64_t> sptr(ns + 1, 0);
+    for (int64_t s = 0; s < ns; s++) {
+        int m = 0;
+        for (int64_t i = s * 32; i < std::min(nN, s * 32 + 32); i++) m = std::max(m, deg[i]);
+        slen[s] = m;
+        sptr[s + 1] = sptr[s] + (int64_t)m * 32;
+    }
+    const int64_t ne = sptr[ns];
+    S->ne = ne;
+    std::vector<uint32_t> colw(ne, 0);
+    std::vector<double> l0(ne, 0.0), bsv(ne, 0.0), vcf(ne, 0.0), bsf(ne, 0.0);
+    std::vector<double> s0e, s1e, sce;
+    if (pb->s0) s0e.assign(ne, 0.0);
+    if (pb->s1) s1e.assign(ne, 0.0);
+    if (pb->sc) sce.assign(ne, 0.0);
+    S->ent_i.resize(nB);
+    S->ent_j.resize(nB);
+    {
+        std::vector<int32_t> cnt(nN, 0), last(nN, -1);
+        for (int64_t k = 0; k < nB; k++) {
+            const int c = chunk_of_host(k, nB, T);
+            const int64_t a = S->inv[(int64_t)bl[k] - 1], b = S->inv[(int64_t)bl[nB + k] - 1];
+            uint32_t st = 0;
+            if (pb->fail && pb->fail[k] == 0) st |= F_BROKEN;
+            if (pb->bond_type) st |= (uint32_t)pb->bond_type[k] << BT_SHIFT;
+            for (int side = 0; side < 2; side++) {
+                const int64_t me = side ? b : a, other = side ? a : b;
+                const int64_t pos = sptr[me / 32] + (int64_t)cnt[me] * 32 + (me % 32);
+                cnt[me]++;
+                colw[pos] = (uint32_t)other | st | (c != last[me] ? F_CHUNK : 0u);
+                last[me] = c;
+                l0[pos] = pb->undeformed_length[k];
+                bsv[pos] = pb->bond_stiffness[k];
+                vcf[pos] = pb->volume_correction[k];
+                if (pb->s0) s0e[pos] = pb->s0[k];
+                if (pb->s1) s1e[pos] = pb->s1[k];
+                if (pb->sc) sce[pos] = pb->sc[k];
+                (side ? S->ent_j : S->ent_i)[k] = pos;
+            }
+        }
+    }
+
+    // node arrays in device order
+    auto perm3 = [&](const double *src, std::vector<double> &dst) {
+        dst.assign(3 * nN, 0.0);
+        if (src)
+            for (int c = 0; c < 3; c++)
+                for (int64_t p = 0; p < nN; p++) dst[p + c * nN] = src[S->perm[p] + c * nN];
+    };
+    auto perm1 = [&](const double *src, std::vector<double> &dst) {
+        dst.assign(nN, 0.0);
+        if (src)
+            for (int64_t p = 0; p < nN; p++) dst[p] = src[S->perm[p]];
+    };
+    std::vector<double> X3, mass, rho, u0(3 * nN, 0.0), x0(3 * nN, 0.0);
+    perm3(pb->undeformed_coordinates, X3);
+    perm1(pb->mass, mass);
+    perm1(pb->density, rho);
+    std::vector<uint8_t> nflag(nN, 0);
+    double U1;
+    {
+        // prescribed value at step 1 (same arithmetic as the device)
+        if (prm->amplitude == BBPD_AMP_SMOOTHSTEP) {
+            double xi = (1.0 - 1.0) / ((double)prm->n_time_steps - 1.0);
+            U1 = 0.0 + (prm->applied_final - 0.0) * ((xi * xi) * xi) * (10 - 15 * xi + 6 * (xi * xi));
+        } else {
+            U1 = prm->rate * 1.0;
+        }
+    }
+    for (int64_t p = 0; p < nN; p++) {
+        int64_t i = S->perm[p];
+        uint8_t f = 0;
+        for (int c = 0; c < 3; c++) {
+            bool cf = pb->constraint_flag && pb->constraint_flag[i + c * nN] == 1;
+            bool pf = pb->prescribed_flag && pb->prescribed_flag[i + c * nN] == 1;
+            if (cf || pf) f |= (uint8_t)(1 << c);
+            if (pf) { f |= (uint8_t)(8 << c); u0[p + c * nN] = U1; }
+            x0[p + c * nN] = X3[p + c * nN] + u0[p + c * nN];
+        }
+        nflag[p] = f;
+    }
+
+    // device buffers
+    Dev &d = S->d;
+    d.n_nodes = nN;
+    d.n_slices = ns;
+    TRY(S->put((int64_t **)&d.slice_ptr, sptr));
+    TRY(S->put((int32_t **)&d.slice_len, slen));
+    TRY(S->put((int32_t **)&d.deg, deg));
+    TRY(S->put(&d.colw, colw));
+    TRY(S->put(&d.bsf, bsf));
+    TRY(S->put((double **)&d.l0, l0));
+    TRY(S->put((double **)&d.bs, bsv));
+    TRY(S->put((double **)&d.vcf, vcf));
+    d.s0e = d.s1e = d.sce = nullptr;
+    if (pb->s0) TRY(S->put((double **)&d.s0e, s0e));
+    if (pb->s1) TRY(S->put((double **)&d.s1e, s1e));
+    if (pb->sc) TRY(S->put((double **)&d.sce, sce));
+    TRY(S->put((double **)&d.X, X3));
+    TRY(S->put(&d.xb0, x0));
+    TRY(S->put(&d.xb1, x0));
+    TRY(S->put(&d.u, u0));
+    std::vector<double> zeros3(3 * nN, 0.0);
+    TRY(S->put(&d.v, zeros3));
+    TRY(S->put(&d.F0, zeros3));
+    TRY(S->put(&d.F1, zeros3));
+    S->has_a = prm->scheme == BBPD_SCHEME_EULERCROMER;
+    d.a = nullptr;
+    if (S->has_a) TRY(S->put(&d.a, zeros3));
+    TRY(S->put((double **)&d.mass, mass));
+    TRY(S->put((double **)&d.rho, rho));
+    TRY(S->put((uint8_t **)&d.nflag, nflag));
+    TRY(S->alloc(&d.part, (size_t)(2 * ns)));
+    std::vector<double> sc4(4, 0.0);
+    TRY(S->put(&d.scal, sc4));
+    std::vector<unsigned> bar(2, 0u);
+    TRY(S->put(&d.bar, bar));
+    std::vector<int> err(1, 0);
+    TRY(S->put(&d.err, err));
+
+    // scalars
+    LawScalars &P = d.P;
+    P.s0 = prm->s0; P.s1 = prm->s1; P.sc = prm->sc;
+    P.beta = prm->beta_tri;
+    double eta = prm->s1 / prm->s0;
+    P.tri_c1 = (eta - P.beta) / (eta - 1);
+    P.tri_c2 = (1 - P.beta) / (eta - 1);
+    P.k = prm->k_exp;
+    P.alpha = prm->alpha_exp;
+    P.exp_den = 1 - std::exp(-prm->k_exp);
+    P.sc_steel = prm->sc_steel;
+    P.ff = prm->failure_functionality;
+    d.V = prm->cell_volume;
+    d.dt = prm->dt;
+    d.damping = prm->damping;
+    d.amplitude = prm->amplitude;
+    d.rate = prm->rate;
+    d.applied_final = prm->applied_final;
+    d.n_time_steps = prm->n_time_steps;
+    d.guard = prm->guard_band;
+    double to = prm->barrier_timeout_s > 0 ? prm->barrier_timeout_s : 2.0;
+    d.timeout_ns = (unsigned long long)(to * 1e9);
+
+    // kernel and grid
+    S->kernel = pick_kernel(prm->law, prm->scheme, prm->precision);
+    int nsm = 0, occ = 0, coop = 0;
+    BBPD_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    BBPD_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+    if (!coop) return fail(BBPD_ERR_UNSUPPORTED, "device lacks cooperative launch");
+    BBPD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)S->kernel, kBlock, 0));
+    if (occ < 1) return fail(BBPD_ERR_CUDA, "kernel cannot be resident");
+    int64_t want = (ns * 32 + kBlock - 1) / kBlock;   // one warp per slice at most
+    S->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * occ, want));
+    BBPD_CUDA_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    BBPD_CUDA_TRY(cudaEventCreate(&S->ev0));
+    BBPD_CUDA_TRY(cudaEventCreate(&S->ev1));
+
+    // algorithmic DRAM bytes of one step for this layout
+    {
+        double per_entry = 4 + 8 + 3 * 8 + (pb->s0 ? 8 : 0) + (pb->s1 ? 8 : 0) + (pb->sc ? 8 : 0);
+        double live = 0;
+        for (int64_t i = 0; i < nN; i++) live += deg[i];
+        double node = prm->scheme == BBPD_SCHEME_ADR
+                          ? (24 /*x*/ + 24 + 24 + 24 + 8 /*u v Fp m*/ + 24 /*F w*/ + 4 /*deg*/ +
+                             24 + 24 + 24 + 24 + 8 + 1 /*F u v X m flag*/ + 72 /*v u x w*/)
+                          : (24 + 4 + 24 /*v*/ + 24 /*u*/ + 8 /*rho*/ + 1 + 24 /*X*/ +
+                             24 * 5 /*F a v u x w*/);
+        S->bytes_per_step = live * per_entry + (double)nN * node;
+    }
+    BBPD_CUDA_TRY(cudaDeviceSynchronize());
+    *out = guard_.release();
+    return BBPD_OK;
+}
+
+static int collect_status(bbpd_solver *S)
+{
+    int h = 0;
+    BBPD_CUDA_TRY(cudaMemcpyAsync(&h, S->d.err, sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    if (h) {
+        int z = 0;
+        BBPD_CUDA_TRY(cudaMemcpy(S->d.err, &z, sizeof(int), cudaMemcpyHostToDevice));
+        if (h & ERR_TIMEOUT) return fail(BBPD_ERR_TIMEOUT, "grid barrier wait exceeded its limit; kernel returned early");
+        return fail(BBPD_ERR_NONFINITE, "non-finite displacement or velocity");
+    }
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_step_async(bbpd_solver *S, int64_t nsteps)
+{
+    if (!S || nsteps < 0) return fail(BBPD_ERR_ARG, "bad argument");
+    if (nsteps == 0) return BBPD_OK;
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    int64_t step0 = S->step;
+    void *args[] = {(void *)&S->d, (void *)&step0, (void *)&nsteps};
+    BBPD_CUDA_TRY(cudaEventRecord(S->ev0, S->stream));
+    BBPD_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)S->kernel, dim3(S->grid), dim3(kBlock), args, 0, S->stream));
+    BBPD_CUDA_TRY(cudaEventRecord(S->ev1, S->stream));
+    S->step += nsteps;
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_sync(bbpd_solver *S)
+{
+    if (!S) return fail(BBPD_ERR_ARG, "null solver");
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    int rc = collect_status(S);
+    if (rc) return rc;
+    if (S->prm.scheme == BBPD_SCHEME_ADR) {
+        BBPD_CUDA_TRY(cudaMemcpy(&S->cn, S->d.scal, sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_step(bbpd_solver *S, int64_t nsteps)
+{
+    TRY(bbpd_step_async(S, nsteps));
+    return bbpd_sync(S);
+}
+
+extern "C" int bbpd_last_kernel_ms(bbpd_solver *S, float *ms)
+{
+    if (!S || !ms) return fail(BBPD_ERR_ARG, "null argument");
+    BBPD_CUDA_TRY(cudaEventElapsedTime(ms, S->ev0, S->ev1));
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_destroy(bbpd_solver *S)
+{
+    if (!S) return BBPD_OK;
+    cudaSetDevice(S->device);
+    if (S->stream) cudaStreamSynchronize(S->stream);
+    delete S;
+    return BBPD_OK;
+}
+
+static double *field_ptr(bbpd_solver *S, int field, bool &nodal)
+{
+    Dev &d = S->d;
+    nodal = true;
+    const int64_t last = S->step - 1;  // last completed step
+    switch (field) {
+    case BBPD_FIELD_DISPLACEMENT: return d.u;
+    case BBPD_FIELD_VELOCITY: return d.v;
+    case BBPD_FIELD_FORCE: return (last & 1) ? d.F1 : d.F0;
+    case BBPD_FIELD_FORCE_PREV: return (last & 1) ? d.F0 : d.F1;
+    case BBPD_FIELD_DEFORMED: return (last & 1) ? d.xb1 : d.xb0;
+    case BBPD_FIELD_ACCELERATION: return d.a;
+    default: nodal = false; return nullptr;
+    }
+}
+
+extern "C" int bbpd_get(bbpd_solver *S, int field, double *out)
+{
+    if (!S || !out) return fail(BBPD_ERR_ARG, "null argument");
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    const int64_t nN = S->nN, nB = S->nB;
+    bool nodal;
+    double *src = field_ptr(S, field, nodal);
+    if (nodal) {
+        if (!src) return fail(BBPD_ERR_ARG, "field %d not held by this scheme", field);
+        std::vector<double> h(3 * nN);
+        BBPD_CUDA_TRY(cudaMemcpy(h.data(), src, sizeof(double) * 3 * nN, cudaMemcpyDeviceToHost));
+        for (int c = 0; c < 3; c++)
+            for (int64_t p = 0; p < nN; p++) out[S->perm[p] + c * nN] = h[p + c * nN];
+        return BBPD_OK;
+    }
+    if (field == BBPD_FIELD_BSF) {
+        std::vector<double> h(S->ne);
+        BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.bsf, sizeof(double) * S->ne, cudaMemcpyDeviceToHost));
+        for (int64_t k = 0; k < nB; k++) out[k] = h[S->ent_i[k]];
+        return BBPD_OK;
+    }
+    if (field == BBPD_FIELD_FLAG || field == BBPD_FIELD_FAIL) {
+        std::vector<uint32_t> h(S->ne);
+        BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.colw, sizeof(uint32_t) * S->ne, cudaMemcpyDeviceToHost));
+        for (int64_t k = 0; k < nB; k++) {
+            uint32_t w = h[S->ent_i[k]];
+            out[k] = field == BBPD_FIELD_FLAG ? ((w & F_SOFT) ? 1.0 : 0.0) : ((w & F_BROKEN) ? 0.0 : 1.0);
+        }
+        return BBPD_OK;
+    }
+    return fail(BBPD_ERR_ARG, "unknown field %d", field);
+}
+
+extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
+{
+    if (!S || !in) return fail(BBPD_ERR_ARG, "null argument");
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    const int64_t nN = S->nN, nB = S->nB;
+    bool nodal;
+    double *dst = field_ptr(S, field, nodal);
+    if (nodal) {
+        if (!dst) return fail(BBPD_ERR_ARG, "field %d not held by this scheme", field);
+        std::vector<double> h(3 * nN);
+        for (int c = 0; c < 3; c++)
+            for (int64_t p = 0; p < nN; p++) h[p + c * nN] = in[S->perm[p] + c * nN];
+        BBPD_CUDA_TRY(cudaMemcpy(dst, h.data(), sizeof(double) * 3 * nN, cudaMemcpyHostToDevice));
+        if (field == BBPD_FIELD_DEFORMED) {
+            // both position buffers: the next step reads the one of its parity
+            BBPD_CUDA_TRY(cudaMemcpy(dst == S->d.xb0 ? S->d.xb1 : S->d.xb0, h.data(), sizeof(double) * 3 * nN, cudaMemcpyHostToDevice));
+        }
+        return BBPD_OK;
+    }
+    if (field == BBPD_FIELD_BSF) {
+        std::vector<double> h(S->ne);
+        BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.bsf, sizeof(double) * S->ne, cudaMemcpyDeviceToHost));
+        for (int64_t k = 0; k < nB; k++) h[S->ent_i[k]] = h[S->ent_j[k]] = in[k];
+        BBPD_CUDA_TRY(cudaMemcpy(S->d.bsf, h.data(), sizeof(double) * S->ne, cudaMemcpyHostToDevice));
+        return BBPD_OK;
+    }
+    if (field == BBPD_FIELD_FLAG || field == BBPD_FIELD_FAIL) {
+        TRY(validate_01(in, nB, field == BBPD_FIELD_FLAG ? "flagBondSoftening" : "fail"));
+        std::vector<uint32_t> h(S->ne);
+        BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.colw, sizeof(uint32_t) * S->ne, cudaMemcpyDeviceToHost));
+        const uint32_t bit = field == BBPD_FIELD_FLAG ? F_SOFT : F_BROKEN;
+        for (int64_t k = 0; k < nB; k++) {
+            bool on = field == BBPD_FIELD_FLAG ? in[k] == 1 : in[k] == 0;
+            for (int64_t pos : {S->ent_i[k], S->ent_j[k]}) h[pos] = on ? (h[pos] | bit) : (h[pos] & ~bit);
+        }
+        BBPD_CUDA_TRY(cudaMemcpy(S->d.colw, h.data(), sizeof(uint32_t) * S->ne, cudaMemcpyHostToDevice));
+        return BBPD_OK;
+    }
+    return fail(BBPD_ERR_ARG, "unknown field %d", field);
+}
+
+extern "C" int bbpd_get_step(bbpd_solver *S, int64_t *step, double *cn)
+{
+    if (!S) return fail(BBPD_ERR_ARG, "null solver");
+    if (step) *step = S->step;
+    if (cn) *cn = S->cn;
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_set_step(bbpd_solver *S, int64_t step, double cn)
+{
+    if (!S || step < 1) return fail(BBPD_ERR_ARG, "bad argument");
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    // F and position buffers are addressed by step parity: keep their contents
+    // attached to the right step when the parity changes
+    if (((step - S->step) & 1) != 0) {
+        std::swap(S->d.F0, S->d.F1);
+        std::swap(S->d.xb0, S->d.xb1);
+    }
+    S->step = step;
+    S->cn = cn;
+    BBPD_CUDA_TRY(cudaMemcpy(S->d.scal, &cn, sizeof(double), cudaMemcpyHostToDevice));
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_selftest_wait_timeout(double timeout_s)
+{
+    TRY(require_device());
+    if (!(timeout_s > 0 && timeout_s <= 5)) return fail(BBPD_ERR_ARG, "timeout must be in (0, 5] s");
+    unsigned *word = nullptr;
+    int *err = nullptr;
+    BBPD_CUDA_TRY(cudaMalloc(&word, sizeof(unsigned)));
+    BBPD_CUDA_TRY(cudaMalloc(&err, sizeof(int)));
+    BBPD_CUDA_TRY(cudaMemset(word, 0, sizeof(unsigned)));
+    BBPD_CUDA_TRY(cudaMemset(err, 0, sizeof(int)));
+    wait_selftest_kernel<<<1, 32>>>(word, err, (unsigned long long)(timeout_s * 1e9));
+    cudaError_t e = cudaDeviceSynchronize();
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(word);
+    cudaFree(err);
+    if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "selftest: %s", cudaGetErrorString(e));
+    if (h & ERR_TIMEOUT) return fail(BBPD_ERR_TIMEOUT, "bounded wait expired as expected");
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_get_info(bbpd_solver *S, bbpd_info *info)
+{
+    if (!S || !info) return fail(BBPD_ERR_ARG, "null argument");
+    std::memset(info, 0, sizeof(*info));
+    info->n_nodes = S->nN;
+    info->n_bonds = S->nB;
+    info->n_entries = S->ne;
+    info->n_slices = S->ns;
+    info->grid_blocks = S->grid;
+    info->block_threads = kBlock;
+    info->device_bytes = S->device_bytes;
+    info->bytes_per_step = S->bytes_per_step;
+    info->layout = 0;
+    return BBPD_OK;
+}

@@ -1,0 +1,279 @@
+"""Benchmark of the BB_PD hot path on B200: bond-updates/s of the fused
+persistent time-step kernel (one bond-update = one undirected bond evaluated
+in one time step).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+                    [--config c1|c2|c3] [--form fp64|fp32] [--no-cpu-baseline]
+
+Default workload (N=1): the 1.28M-node beam (400 x 40 x 80 lattice at
+dx = 1.25 mm, 74.5M bonds), trilinear softening, ADR, plain FP64; synthetic
+inputs built like the reference's input scripts. A step is one time step of
+the whole beam. `value` times K steps of one persistent-kernel launch on data
+resident in HBM (CUDA events on the launching stream); `e2e` times the C-ABI
+job from host buffers (upload and layout, K steps, download of the state).
+With N > 1 (torchrun) every rank solves its own beam: independent replicas,
+no collective on the data path, value = all ranks' bond-updates / max time.
+
+`--impl reference` times the reference's CPU implementation of the path (its
+compiled MEX routines from oracle/_ref driven by the oracle's loop, the
+MATLAB-only pieces restated in C) on this host's cores, on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "c1": ("config1", "beam 100x10x20 dx=5mm (20k nodes, 1.0M bonds)"),
+    "c2": ("config2", "beam 400x40x80 dx=1.25mm (1.28M nodes, 74.5M bonds)"),
+    "c3": ("config3", "notched beam 160x20x40 dx=2.5mm (128k nodes, 7.1M bonds), lognormal sc"),
+}
+# ADR displacement control: 1e-7 mm per step at the midspan top nodes (metres)
+RATE = -1e-10
+
+
+def law_for(cfg):
+    return ("exponential", dict(law="exponential", s0=1e-4)) if cfg == "c3" else \
+        ("trilinear", dict(law="trilinear", s0=1e-4, s1=3e-4, sc=2e-3))
+
+
+def peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(nN, nB, per_bond_sc):
+    """Bytes one time step must move: per directed bond entry 4 B of neighbour
+    index + 8 B of damage state (+ 8 B of per-bond critical stretch), per node
+    181 B (x0, u, v, F_prev read and written, mass, family count, flags)."""
+    nD = 2 * nB
+    return nD * 12 + (nD * 8 if per_bond_sc else 0) + nN * 181
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_rate(inp, lawkw, budget_s, warmup, max_steps, kernels="reference"):
+    """Time the CPU implementation on `inp`: returns (bond-updates/s, steps, seconds, kind, threads)."""
+    from oracle import pyoracle as po
+    kind = "reference" if (kernels == "reference" and po.ref_available()) else "port"
+    run = po.Run(inp, scheme="adr", rate=RATE, kernels="reference" if kind == "reference" else "restated", **lawkw)
+    for _ in range(warmup):
+        run.step(1)
+    t0 = time.perf_counter()
+    run.step(1)
+    t1 = time.perf_counter() - t0
+    n = 1
+    limit = max(1, min(max_steps, int(budget_s / max(t1, 1e-9))))
+    while n < limit:
+        run.step(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)) if kind == "reference" else 1
+    return inp["nBonds"] * n / dt, n, dt, kind, threads
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=list(CONFIGS))
+    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--node-order", default="input", choices=["input", "morton"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    import bb_pd_b200 as bb
+    fn, wname = CONFIGS[args.config]
+    lawname, lawkw = law_for(args.config)
+    per_bond_sc = args.config == "c3"
+    metric, unit = "bond-updates/s", "bond-updates/s"
+    config = {"workload": f"{wname}, {lawname} law, ADR, 1e-7 mm/step midspan displacement control",
+              "nodes": None, "bonds": None, "form": args.form, "node_order": args.node_order,
+              "l2": "inputs larger than L2: every step streams the whole bond layout (GBs) through HBM",
+              "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "1 GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        inp = bb.beam.build(getattr(bb.beam, fn)())
+        config.update(nodes=inp["nNodes"], bonds=inp["nBonds"])
+        rate, n, dt, kind, threads = cpu_reference_rate(inp, lawkw, budget_s=120.0, warmup=min(args.warmup, 1),
+                                                        max_steps=args.steps)
+        line = {"metric": metric, "value": rate, "unit": unit, "n_gpus": args.gpus, "steps": n,
+                "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "impl": "reference",
+                "cpu_baseline": {"value": rate, "unit": unit, "cores": threads, "kind": kind,
+                                 "sample": f"{n} of the requested {args.steps} time steps of the full beam"},
+                "e2e": {"value": rate, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    dev = local
+    torch.cuda.set_device(dev)
+    inp = bb.beam.build(getattr(bb.beam, fn)())
+    nN, nB = inp["nNodes"], inp["nBonds"]
+    config.update(nodes=nN, bonds=nB)
+    kw = dict(lawkw, scheme="adr", rate=RATE, precision=args.form, node_order=args.node_order)
+
+    # ---- value: resident data, one persistent launch of K steps ----
+    s = bb.Solver(inp, device=dev, **kw)
+    info = s.info()
+    s.step(args.warmup)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(dev)
+    clocks.start()
+    time.sleep(0.15)
+    s.step_async(args.steps)
+    s.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = s.last_kernel_ms()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_step = ms / args.steps
+    value = nB * args.steps * world / (ms / 1e3)
+    s.close()
+    del s
+
+    # ---- e2e: the C-ABI job from host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        s2 = bb.Solver(inp, device=dev, **kw)
+        s2.step(args.steps)
+        outs = [s2.get(f) for f in ("displacement", "force", "bsf", "flag", "fail")]
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t0
+        s2.close()
+        if dist:
+            t = torch.tensor([te], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        h2d = sum(inp[k].nbytes for k in ("undeformedCoordinates", "BONDLIST", "UNDEFORMEDLENGTH",
+                                           "BONDSTIFFNESS", "VOLUMECORRECTIONFACTORS", "massVector",
+                                           "CONSTRAINTFLAG", "BODYFORCEFLAG")) + (inp["sc"].nbytes if per_bond_sc else 0)
+        d2h = sum(o.nbytes for o in outs)
+        e2e = {"value": nB * args.steps * world / te, "unit": unit,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "seconds": te, "includes": "upload of the reference arrays, layout build, K steps, download of state"}
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind = peak_hbm()
+    alg = algorithmic_bytes(nN, nB, per_bond_sc)
+    achieved = alg / (ms_step / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_step": alg, "layout_bytes_per_step": info["bytes_per_step"]}
+
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        rate, n, dt, kind, threads = cpu_reference_rate(inp, lawkw, budget_s=20.0, warmup=0, max_steps=50)
+        cpu = {"value": rate, "unit": unit, "cores": threads, "kind": kind,
+               "sample": f"{n} time steps of the same beam ({dt:.1f} s)"}
+
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+f64", "data": "synthetic",
+            "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 1,
+            "clocks": clk, "solver": {"grid_blocks": info["grid_blocks"], "entries": info["n_entries"],
+                                      "device_bytes": info["device_bytes"]}}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

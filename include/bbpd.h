@@ -1,0 +1,339 @@
+/*
+ * bbpd.h -- C ABI of libbbpd, a B200 (sm_100a) implementation of the BB_PD
+ * bond-based peridynamics hot path: per-bond deformed length and stretch,
+ * constitutive law with irreversible damage, bond force, fixed-order nodal
+ * force sum, and the Euler-Cromer / adaptive-dynamic-relaxation (ADR) time step.
+ *
+ * Conventions (identical to the reference's MEX routines):
+ *   - arrays are double precision, column-major (MATLAB): a node array of
+ *     nNodes x 3 stores x of node k at [k], y at [k + nNodes], z at [k + 2 nNodes];
+ *   - BONDLIST is nBonds x 2, node ids 1-based and stored as doubles;
+ *   - "in place" arguments are read and overwritten, as the MEX files do.
+ * Every function returns a bbpd_status; nothing long-jumps or aborts.
+ * Plain pointers and sizes only: no C++ or framework types cross this ABI.
+ *
+ * Numerics: the FP64 paths evaluate each expression in the reference's order
+ * with no fused multiply-add, and sum nodal forces in the reference's OpenMP
+ * order, so their results are bit-identical to the reference MEX chain on the
+ * same inputs (the exponential law's exp() aside, which may differ from glibc's
+ * in the last bit).
+ */
+#ifndef BBPD_H
+#define BBPD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BBPD_ABI_VERSION 1
+
+typedef enum bbpd_status {
+    BBPD_OK = 0,
+    BBPD_ERR_ARG = 1,          /* invalid argument, size or value */
+    BBPD_ERR_CUDA = 2,         /* CUDA runtime error (message in bbpd_last_error) */
+    BBPD_ERR_OOM = 3,          /* device allocation failed */
+    BBPD_ERR_TIMEOUT = 4,      /* a device-side wait gave up (kernel returned early) */
+    BBPD_ERR_NONFINITE = 5,    /* a displacement or velocity became NaN/Inf */
+    BBPD_ERR_UNSUPPORTED = 6,  /* valid input outside what this build implements */
+    BBPD_ERR_NO_DEVICE = 7     /* no CUDA device (this library has no CPU path) */
+} bbpd_status;
+
+enum { BBPD_LAW_LINEAR = 0,       /* brittle: calculatebondfailureMex.c:26-44 */
+       BBPD_LAW_BILINEAR = 1,     /* calculatebondsofteningfactor.m:159-165 */
+       BBPD_LAW_TRILINEAR = 2,    /* calculatebsftrilinear.m:80-112 */
+       BBPD_LAW_EXPONENTIAL = 3   /* calculatebsfexponentialMex.c:26-66 */ };
+enum { BBPD_SCHEME_EULERCROMER = 0, BBPD_SCHEME_ADR = 1 };
+enum { BBPD_PREC_FP64 = 0,        /* plain form: bit-identical to the reference chain */
+       BBPD_PREC_FP32 = 1         /* FP32 stretch/force, FP64 sums, FP64 guard band */ };
+enum { BBPD_AMP_LINEAR = 0,       /* U(n) = rate * n */
+       BBPD_AMP_SMOOTHSTEP = 1    /* smoothstepdata.m:40-42 from step 1 to nTimeSteps */ };
+enum { BBPD_ORDER_INPUT = 0, BBPD_ORDER_MORTON = 1 };
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *bbpd_last_error(void);
+const char *bbpd_status_string(int status);
+int bbpd_abi_version(void);
+/* Number of visible CUDA devices (0 when there is none). */
+int bbpd_device_count(void);
+
+/* ===================================================================== *
+ *  Per-routine entry points: one per reference MEX routine.             *
+ *  _dev_ variants take device pointers and a cudaStream_t (as void*,    *
+ *  NULL = legacy default stream) and return after enqueueing.           *
+ *  Host-pointer variants copy in, run, copy out and synchronize; they   *
+ *  are what the mexFunction gateways call.                              *
+ * ===================================================================== */
+
+/* replaces calculatedeformedlength, calculatedeformedlengthMex.c:27 */
+int bbpd_dev_calculatedeformedlength(const double *deformedCoordinates,
+        const double *bondlist, const double *undeformedLength, int64_t nBonds,
+        int64_t nNodes, double *deformedLength, double *deformedX,
+        double *deformedY, double *deformedZ, double *stretch, void *stream);
+int bbpd_calculatedeformedlength(const double *deformedCoordinates,
+        const double *bondlist, const double *undeformedLength, int64_t nBonds,
+        int64_t nNodes, double *deformedLength, double *deformedX,
+        double *deformedY, double *deformedZ, double *stretch);
+
+/* replaces calculatebsfexponential, calculatebsfexponentialMex.c:26 (s0, sc per bond) */
+int bbpd_dev_calculatebsfexponential(const double *stretch, const double *s0,
+        const double *sc, double k, double alpha, double *bsf,
+        double *bondSofteningFactor, const double *BONDTYPE,
+        double *flagBondSoftening, int64_t nBonds, void *stream);
+int bbpd_calculatebsfexponential(const double *stretch, const double *s0,
+        const double *sc, double k, double alpha, double *bsf,
+        double *bondSofteningFactor, const double *BONDTYPE,
+        double *flagBondSoftening, int64_t nBonds);
+
+/* replaces calculatebsftrilinear.m:1 (scalar s0, s1, sc; beta = 0.25 at :41) */
+int bbpd_dev_calculatebsftrilinear(const double *stretch, double s0, double s1,
+        double sc, double *bondSofteningFactor, const double *BONDTYPE,
+        double *flagBondSoftening, int64_t nBonds, void *stream);
+int bbpd_calculatebsftrilinear(const double *stretch, double s0, double s1,
+        double sc, double *bondSofteningFactor, const double *BONDTYPE,
+        double *flagBondSoftening, int64_t nBonds);
+
+/* replaces calculatebondsofteningfactor.m:1 (bilinear; scalar s0, sc) */
+int bbpd_dev_calculatebondsofteningfactor(const double *stretch, double s0,
+        double sc, double *flagBondSoftening, double *bondSofteningFactor,
+        const double *BONDTYPE, int64_t nBonds, void *stream);
+int bbpd_calculatebondsofteningfactor(const double *stretch, double s0,
+        double sc, double *flagBondSoftening, double *bondSofteningFactor,
+        const double *BONDTYPE, int64_t nBonds);
+
+/* replaces calculatebondfailure, calculatebondfailureMex.c:26 */
+int bbpd_dev_calculatebondfailure(double *fail, double failureFunctionality,
+        const double *BONDTYPE, const double *stretch,
+        double criticalStretchConcrete, double criticalStretchSteel,
+        int64_t nBonds, void *stream);
+int bbpd_calculatebondfailure(double *fail, double failureFunctionality,
+        const double *BONDTYPE, const double *stretch,
+        double criticalStretchConcrete, double criticalStretchSteel,
+        int64_t nBonds);
+
+/* replaces calculatebondforces, calculatebondforcesMex.c:26 */
+int bbpd_dev_calculatebondforces(double *bForceX, double *bForceY,
+        double *bForceZ, const double *fail, const double *deformedX,
+        const double *deformedY, const double *deformedZ,
+        const double *deformedLength, const double *stretch,
+        const double *stretchPlastic, const double *BONDSTIFFNESS,
+        double cellVolume, const double *VOLUMECORRECTIONFACTORS,
+        const double *bondSofteningFactor, int64_t nBonds, void *stream);
+int bbpd_calculatebondforces(double *bForceX, double *bForceY,
+        double *bForceZ, const double *fail, const double *deformedX,
+        const double *deformedY, const double *deformedZ,
+        const double *deformedLength, const double *stretch,
+        const double *stretchPlastic, const double *BONDSTIFFNESS,
+        double cellVolume, const double *VOLUMECORRECTIONFACTORS,
+        const double *bondSofteningFactor, int64_t nBonds);
+
+/* Nodal force sum. The reference scatters with per-thread private arrays
+ * (calculatenodalforcesopenmpMex.c:29-85); here a plan holds the per-node
+ * bond lists (bond order) once, and each node sums its bonds in the
+ * reference's order: nChunks contiguous bond ranges under OpenMP's static
+ * schedule (8 = the reference's forced team, 1 = the serial
+ * calculatenodalforcesMex.c), chunk partials added in chunk order.
+ * The plan owns device memory; create it once per bond list. */
+typedef struct bbpd_nodal_plan bbpd_nodal_plan;
+int bbpd_nodal_plan_create(const double *bondlist_dev, int64_t nBonds,
+        int64_t nNodes, int nChunks, void *stream, bbpd_nodal_plan **plan);
+int bbpd_nodal_plan_destroy(bbpd_nodal_plan *plan);
+/* replaces calculatenodalforces, calculatenodalforcesopenmpMex.c:29; adds into nodalForce */
+int bbpd_dev_calculatenodalforces(const bbpd_nodal_plan *plan,
+        double *nodalForce, const double *bForceX, const double *bForceY,
+        const double *bForceZ, void *stream);
+int bbpd_calculatenodalforces(const double *bondlist, int64_t nBonds,
+        int64_t nNodes, double *nodalForce, const double *bForceX,
+        const double *bForceY, const double *bForceZ, int nChunks);
+
+/* replaces timeintegrationeulercromer, timeintegrationeulercromerMex.c:26 */
+int bbpd_dev_timeintegrationeulercromer(double *nodalAcceleration,
+        const double *nodalForce, double DAMPING, double *nodalVelocity,
+        const double *DENSITY, const double *constraintFlag, double DT,
+        double *nodalDisplacement, double *deformedCoordinates,
+        const double *undeformedCoordinates, int64_t nNodes, int NOD,
+        void *stream);
+int bbpd_timeintegrationeulercromer(double *nodalAcceleration,
+        const double *nodalForce, double DAMPING, double *nodalVelocity,
+        const double *DENSITY, const double *constraintFlag, double DT,
+        double *nodalDisplacement, double *deformedCoordinates,
+        const double *undeformedCoordinates, int64_t nNodes, int NOD);
+
+/* replaces calculatedampingcoefficient.m:1 (NOD = 3). The Rayleigh-quotient
+ * sums use a fixed blocked-tree order (slices of 32 nodes, then 1024 strands),
+ * so the result is deterministic; *cn is written to host memory. Uses a
+ * scratch buffer of 2 * ceil(nNodes / 32) doubles that it allocates. */
+int bbpd_dev_calculatedampingcoefficient(const double *nodalForce,
+        const double *massVector, const double *nodalForcePrevious, double DT,
+        const double *nodalVelocityPreviousHalf, const double *nodalDisplacement,
+        int64_t nNodes, double *cn, void *stream);
+int bbpd_calculatedampingcoefficient(const double *nodalForce,
+        const double *massVector, const double *nodalForcePrevious, double DT,
+        const double *nodalVelocityPreviousHalf, const double *nodalDisplacement,
+        int64_t nNodes, double *cn);
+
+/* Free the device mirrors and cached plan of the host-pointer entry points
+ * (the gateways register it with mexAtExit). */
+int bbpd_release_mirrors(void);
+
+/* replaces timeintegrationADR.m:1 (NOD = 3) */
+int bbpd_dev_timeintegrationADR(int64_t iTimeStep, double DT,
+        double *nodalVelocityForwardHalf, const double *nodalForce,
+        const double *massVector, double cn,
+        const double *nodalVelocityPreviousHalf, double *nodalDisplacement,
+        const double *CONSTRAINTFLAG, int64_t nNodes, void *stream);
+int bbpd_timeintegrationADR(int64_t iTimeStep, double DT,
+        double *nodalVelocityForwardHalf, const double *nodalForce,
+        const double *massVector, double cn,
+        const double *nodalVelocityPreviousHalf, double *nodalDisplacement,
+        const double *CONSTRAINTFLAG, int64_t nNodes);
+
+/* ===================================================================== *
+ *  Fused solver: the whole time loop of                                  *
+ *  dynamicsolverdisplacementcontrolled.m:71-105 (Euler-Cromer) or its    *
+ *  ADR form (dynamicsolverdisplacementcontrolledADR.m:91-155 with the    *
+ *  ADR calls at :137, :142 switched on), one persistent kernel per call  *
+ *  of bbpd_step, state resident on the device between calls.            *
+ * ===================================================================== */
+
+typedef struct bbpd_params {
+    int32_t law;              /* BBPD_LAW_* */
+    int32_t scheme;           /* BBPD_SCHEME_* */
+    int32_t precision;        /* BBPD_PREC_* */
+    int32_t n_chunks;         /* nodal-force summation chunks (8 = reference) */
+    int32_t amplitude;        /* BBPD_AMP_* for prescribed DOFs */
+    int32_t node_order;       /* BBPD_ORDER_*: device-side node ordering */
+    double cell_volume;       /* cellVolume */
+    double dt;                /* simulation.DT */
+    double damping;           /* simulation.DAMPING (Euler-Cromer) */
+    double s0, s1, sc;        /* law stretches when the per-bond arrays are NULL */
+    double sc_steel;          /* brittle law, steel bonds (BONDTYPE 2) */
+    double k_exp, alpha_exp;  /* exponential law (25, 0.25 at dynamicsolverdisplacementcontrolled.m:87) */
+    double beta_tri;          /* trilinear beta (0.25 at calculatebsftrilinear.m:41) */
+    double failure_functionality; /* value fail takes on breaking (0: failure on) */
+    double rate;              /* BBPD_AMP_LINEAR: displacement per step */
+    double applied_final;     /* BBPD_AMP_SMOOTHSTEP: final displacement */
+    int64_t n_time_steps;     /* BBPD_AMP_SMOOTHSTEP: final step */
+    double guard_band;        /* BBPD_PREC_FP32: FP64 recheck when |s - sc| < guard_band */
+    double barrier_timeout_s; /* device grid-barrier wait limit (0 = 2 s) */
+} bbpd_params;
+
+/* Fill params with the reference defaults (law exponential k=25 alpha=0.25,
+ * beta=0.25, 8 chunks, failure on, FP64, Euler-Cromer, guard band 1e-5). */
+void bbpd_params_default(bbpd_params *p);
+
+typedef struct bbpd_problem {
+    int64_t n_nodes, n_bonds;
+    const double *undeformed_coordinates; /* nNodes x 3 */
+    const double *bondlist;               /* nBonds x 2, 1-based */
+    const double *undeformed_length;      /* nBonds */
+    const double *bond_stiffness;         /* nBonds (BONDSTIFFNESS) */
+    const double *volume_correction;      /* nBonds (VOLUMECORRECTIONFACTORS) */
+    const double *bond_type;              /* nBonds in {0,1,2}, or NULL = all 0 */
+    const double *fail;                   /* nBonds in {0,1}, or NULL = all 1 */
+    const double *stretch_plastic;        /* nBonds (must be 0), or NULL */
+    const double *s0, *s1, *sc;           /* nBonds each, or NULL = params scalars */
+    const double *density;                /* nNodes (Euler-Cromer), or NULL */
+    const double *mass;                   /* nNodes (ADR massVector), or NULL */
+    const double *constraint_flag;        /* nNodes x 3 in {0,1}, or NULL */
+    const double *prescribed_flag;        /* nNodes x 3 in {0,1}, or NULL */
+} bbpd_problem;
+
+typedef struct bbpd_solver bbpd_solver;
+
+/* Validate, lay out (per-node bond lists in bond order, sliced by 32 nodes)
+ * and upload a problem; the state starts at step 1 (arraypreallocation.m). */
+int bbpd_create(const bbpd_problem *problem, const bbpd_params *params,
+                int device, bbpd_solver **out);
+/* Run nsteps time steps in one persistent-kernel launch; blocks until done. */
+int bbpd_step(bbpd_solver *s, int64_t nsteps);
+/* Enqueue nsteps on the solver's stream without waiting (status of the
+ * previous work is returned by bbpd_sync). */
+int bbpd_step_async(bbpd_solver *s, int64_t nsteps);
+int bbpd_sync(bbpd_solver *s);
+int bbpd_destroy(bbpd_solver *s);
+
+enum { BBPD_FIELD_DISPLACEMENT = 0,  /* nodalDisplacement, nNodes x 3 */
+       BBPD_FIELD_VELOCITY = 1,      /* nodalVelocity (ADR: forward half step) */
+       BBPD_FIELD_FORCE = 2,         /* nodalForce of the last step */
+       BBPD_FIELD_DEFORMED = 3,      /* deformedCoordinates */
+       BBPD_FIELD_FORCE_PREV = 4,    /* nodalForcePrevious (ADR) */
+       BBPD_FIELD_ACCELERATION = 5,  /* nodalAcceleration (Euler-Cromer) */
+       BBPD_FIELD_BSF = 16,          /* bondSofteningFactor, nBonds */
+       BBPD_FIELD_FLAG = 17,         /* flagBondSoftening, nBonds */
+       BBPD_FIELD_FAIL = 18          /* fail, nBonds */ };
+
+/* Copy a field to host memory (reference layout and node order). */
+int bbpd_get(bbpd_solver *s, int field, double *host_out);
+/* Overwrite a field from host memory (restoring a checkpoint; FORCE and
+ * FORCE_PREV included). Bond fields set both directed copies of each bond. */
+int bbpd_set(bbpd_solver *s, int field, const double *host_in);
+/* Next step to run (1-based) and last ADR damping coefficient. */
+int bbpd_get_step(bbpd_solver *s, int64_t *step, double *cn);
+int bbpd_set_step(bbpd_solver *s, int64_t step, double cn);
+
+typedef struct bbpd_info {
+    int64_t n_nodes, n_bonds, n_entries;  /* entries: directed slots incl. padding */
+    int64_t n_slices;
+    int32_t grid_blocks, block_threads;
+    int64_t device_bytes;                 /* device memory held by the solver */
+    double bytes_per_step;                /* algorithmic DRAM bytes of one step */
+    int32_t layout;                       /* 0 = wide per-entry constants, 1 = compact */
+    int32_t reserved;
+} bbpd_info;
+int bbpd_get_info(bbpd_solver *s, bbpd_info *info);
+
+/* Elapsed device time of the last bbpd_step / bbpd_step_async launch (ms). */
+int bbpd_last_kernel_ms(bbpd_solver *s, float *ms);
+
+/* Diagnostic: runs the device-side bounded wait used by the solver's grid
+ * barriers on a word that nothing writes. Returns BBPD_ERR_TIMEOUT when the
+ * wait expires after timeout_s and the kernel returns (the expected outcome). */
+int bbpd_selftest_wait_timeout(double timeout_s);
+
+/* ===================================================================== *
+ *  Synthetic beam builder (the inputs of input/scripts/Gregoire_beam_    *
+ *  tests.m and the functions it calls, for a regular lattice).          *
+ * ===================================================================== */
+
+typedef struct bbpd_beam_spec {
+    int32_t nx, ny, nz;          /* nodes along length x, width y, depth z */
+    double dx;                   /* lattice spacing (m) */
+    double horizon_factor;       /* horizon = factor * dx */
+    double E;                    /* Young's modulus (Pa) */
+    double stiffness_factor;     /* c = factor * E / (pi * horizon^4) */
+    double density;              /* kg/m^3 */
+    double support_x[2];         /* pinned bottom-layer node lines (m) */
+    int32_t n_supports;
+    int32_t load_midspan_top;    /* 1: z of the midspan top nodes prescribed */
+    int32_t notch;               /* 1: remove bonds crossing the notch plane */
+    int32_t sc_lognormal;        /* 1: per-bond sc ~ lognormal(sc_mean, sc_cov) */
+    double notch_x;              /* notch plane position (m) */
+    double notch_depth;          /* notch height from the bottom face (m) */
+    double sc_mean, sc_cov;
+    uint64_t seed;
+} bbpd_beam_spec;
+
+typedef struct bbpd_beam_scalars {
+    int64_t n_nodes, n_bonds;
+    double horizon, cell_volume, bond_stiffness_concrete, dt;
+    int64_t n_supported, n_prescribed;
+} bbpd_beam_scalars;
+
+/* Sizes and scalars of a beam (no arrays). */
+int bbpd_beam_count(const bbpd_beam_spec *spec, bbpd_beam_scalars *out);
+/* Fill caller-allocated arrays (reference layouts): X (nNodes x 3), bondlist
+ * (nBonds x 2), L0, BS, VCF (nBonds), nfam, density, mass (nNodes), CF, PF
+ * (nNodes x 3) and, if sc_lognormal, sc (nBonds; may be NULL otherwise). */
+int bbpd_beam_build(const bbpd_beam_spec *spec, double *X, double *bondlist,
+                    double *L0, double *BS, double *VCF, double *nfam,
+                    double *density, double *mass, double *CF, double *PF,
+                    double *sc);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
