@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libbbpd.so")
+LIB_PATH = os.environ.get("BBPD_LIB") or os.path.join(HERE, "lib", "libbbpd.so")
 MEX_DIR = os.path.join(HERE, "mex")
 
 # status codes (bbpd_status)

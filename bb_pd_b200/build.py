@@ -52,9 +52,9 @@ def _newer(out: str, deps: list[str]) -> bool:
     return all(os.path.getmtime(d) <= t for d in deps)
 
 
-def build_lib(force: bool = False) -> str:
+def build_lib(force: bool = False, out: str | None = None) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
-    out = os.path.join(LIBDIR, "libbbpd.so")
+    out = out or os.path.join(LIBDIR, "libbbpd.so")
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".cpp", ".h"))]
     deps.append(os.path.join(INCLUDE, "bbpd.h"))
     if not force and _newer(out, deps):
@@ -67,6 +67,7 @@ def build_lib(force: bool = False) -> str:
            "-Xptxas", "-v" if os.environ.get("BBPD_PTXAS_VERBOSE") else "-O3",
            "-I", INCLUDE, "-I", CSRC,
            "-shared", "-cudart", "static", "-o", out]
+    cmd += [f"-D{d}" for d in os.environ.get("BBPD_DEFINES", "").split()]
     cmd += [os.path.join(CSRC, f) for f in CUDA_SOURCES]
     cmd += ["-lpthread"]
     _run(cmd)

@@ -2,30 +2,36 @@
 //
 // Layout in HBM (built on the host at bbpd_create):
 //   nodes   SoA float64 (x of all nodes, then y, then z), in input order or
-//           Morton order; per-node flags byte (constrained / prescribed DOFs).
+//           Morton order; one flags byte per node (held / prescribed DOFs).
 //   bonds   every undirected bond is stored twice, once in the list of each
-//           end node ("directed entries"). Lists are kept in bond order and
-//           laid out as 32-node slices (SELL-32): entry k of the node in lane l
-//           of slice s sits at slice_ptr[s] + 32 k + l, so a warp that walks
-//           its 32 nodes' lists in step reads each per-entry array with
-//           128/256-byte coalesced loads. Per entry: a 32-bit word (neighbour
-//           index + chunk / state bits), the damage state BSF (float64), and the
-//           bond constants L0, BONDSTIFFNESS, VCF (float64).
+//           end node ("directed entries"). Lists keep bond order and are laid
+//           out as 32-node slices (SELL-32): entry k of the node in lane l of
+//           slice s sits at slice_ptr[s] + 32 k + l, so a warp walking its 32
+//           nodes' lists in step reads every per-entry stream coalesced.
+//           Per entry, read every step:
+//             colw  u32  neighbour index (24 bits), chunk-start bit, BONDTYPE
+//             cid   u16  (u32 for irregular inputs) index into a dictionary of
+//                        the distinct (L0, VCF, BONDSTIFFNESS) triples (5 872 on
+//                        the 1.28M-node beam; the table stays in L1/L2)
+//             st    u8   fail / softening flag / "damaged" (BSF != 0) bits
+//           and, only for damaged entries, BSF (float64). Optional per-entry
+//           critical stretch (float64) when the law takes per-bond sc.
 //
-// One time step (per launch, any number of steps):
-//   phase A  each warp takes a slice; each lane walks its node's entries,
-//            computes stretch, law, damage and bond force for every bond,
-//            and sums the forces in the reference's OpenMP order (chunk
-//            partials in bond order, added in chunk order). Both copies of a
-//            bond see bit-identical stretch (the squared components do not
-//            depend on direction), so both copies of the damage state evolve
-//            identically and no atomics or cross-warp exchange are needed.
-//            Euler-Cromer integrates the node right there; ADR writes the
-//            node's Rayleigh-quotient terms reduced over the warp.
-//   barrier  (ADR) the last block to arrive reduces the slice partials in a
-//            fixed order into the damping coefficient cn.
-//   phase B  (ADR) central-difference half-step update of every node.
-//   barrier  positions of step n+1 are visible to every block.
+// One time step (a launch runs any number of steps):
+//   phase A  each warp takes a 32-node slice; each lane walks its node's
+//            entries with loads issued two entries ahead, computes stretch,
+//            law, damage and bond force, and sums the forces in the reference's
+//            OpenMP order (chunk partials in bond order, added in chunk order).
+//            Both copies of a bond see bit-identical stretch (the squared
+//            components do not depend on direction), so both copies of the
+//            damage state evolve identically: no atomics, no cross-warp traffic.
+//            Euler-Cromer integrates the node right there (positions
+//            double-buffered); ADR writes the node's Rayleigh-quotient terms
+//            reduced over the warp (one partial per slice).
+//   ADR      barrier; warps reduce the slice partials into 1024 strands in a
+//            fixed order; barrier, the last block to arrive folds the strands
+//            (xor butterfly) into the damping coefficient cn; phase B applies
+//            the central-difference half-step update; barrier.
 // Grid barriers spin with a time limit; on expiry they set an error flag and
 // the kernel returns early (status BBPD_ERR_TIMEOUT), never hanging.
 #include "bbpd_internal.h"
@@ -37,6 +43,7 @@
 #include <memory>
 #include <numeric>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 using namespace bbpd;
@@ -45,25 +52,34 @@ namespace {
 
 constexpr uint32_t COL_MASK = 0x00FFFFFFu;
 constexpr uint32_t F_CHUNK = 1u << 24;   // first entry of a new OpenMP chunk in this list
-constexpr uint32_t F_BROKEN = 1u << 25;  // fail == 0
-constexpr uint32_t F_SOFT = 1u << 26;    // flagBondSoftening == 1
-constexpr int BT_SHIFT = 27;             // bits 27-28: BONDTYPE
+constexpr int BT_SHIFT = 25;             // bits 25-26: BONDTYPE
+constexpr uint8_t ST_BROKEN = 1;         // fail == 0
+constexpr uint8_t ST_SOFT = 2;           // flagBondSoftening == 1
+constexpr uint8_t ST_DAMAGED = 4;        // BSF != +0.0 (BSF stored in bsf[])
 constexpr int64_t MAX_NODES = (int64_t)1 << 24;
 
 constexpr int ERR_TIMEOUT = 1;
 constexpr int ERR_NONFINITE = 2;
 
 constexpr int kBlock = 256;
+#ifndef BBPD_MIN_BLOCKS
+#define BBPD_MIN_BLOCKS 3
+#endif
 constexpr int kStrands = 1024;
+
+struct DictEntry {
+    double l0, vcf, bs, pad;
+};
 
 struct Dev {
     int64_t n_nodes, n_slices;
     const int64_t *slice_ptr;
-    const int32_t *slice_len;
     const int32_t *deg;
-    uint32_t *colw;
+    const uint32_t *colw;
+    const void *cid;
+    uint8_t *st;
     double *bsf;
-    const double *l0, *bs, *vcf;
+    const DictEntry *dict;
     const double *s0e, *s1e, *sce;   // per-entry law stretches or null
     const double *X;
     double *xb0, *xb1;               // positions: step n reads xb[(n-1)&1], writes xb[n&1]
@@ -71,7 +87,8 @@ struct Dev {
     double *F0, *F1;                 // F of step n lives in F[n&1]
     const double *mass, *rho;
     const uint8_t *nflag;            // bit d: held (constrained or prescribed); bit 3+d: prescribed
-    double *part;                    // 2 * n_slices
+    double *part;                    // 2 * n_slices slice partials
+    double *strand;                  // 2 * kStrands strand sums
     double *scal;                    // [0] = cn
     unsigned *bar;                   // [0] arrivals, [1] generation
     int *err;
@@ -102,21 +119,32 @@ __device__ __forceinline__ double prescribed_value(const Dev &d, int64_t n)
     return d.rate * (double)n;
 }
 
-// Fixed-order reduction of the slice partials (1024 strands, xor butterfly)
-// and the clamp of calculatedampingcoefficient.m:90-112; run by one block.
-__device__ void compute_cn(const Dev &d)
+// Wait until *word differs from `old`, at most timeout_ns. Gives up early when
+// another block already reported a timeout in *err. On expiry sets
+// ERR_TIMEOUT in *err and returns false; never waits without a limit.
+__device__ bool bounded_wait_change(volatile unsigned *word, unsigned old, int *err,
+                                    unsigned long long timeout_ns)
+{
+    const unsigned long long t0 = globaltimer();
+    while (*word == old) {
+        if (*(volatile int *)err & ERR_TIMEOUT) return false;
+        if (globaltimer() - t0 > timeout_ns) {
+            atomicOr(err, ERR_TIMEOUT);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    return true;
+}
+
+// Fold the 1024 strand sums (xor butterfly, offsets 512 ... 1) and apply the
+// clamp of calculatedampingcoefficient.m:90-112; run by one block.
+__device__ void fold_strands(const Dev &d)
 {
     __shared__ double a1[kStrands], a2[kStrands];
-    const int64_t ns = d.n_slices;
     for (int r = threadIdx.x; r < kStrands; r += blockDim.x) {
-        double c1 = 0.0, c2 = 0.0;
-#pragma unroll 8
-        for (int64_t k = r; k < ns; k += kStrands) {
-            c1 = c1 + __ldcg(&d.part[k]);
-            c2 = c2 + __ldcg(&d.part[ns + k]);
-        }
-        a1[r] = c1;
-        a2[r] = c2;
+        a1[r] = __ldcg(&d.strand[r]);
+        a2[r] = __ldcg(&d.strand[kStrands + r]);
     }
     __syncthreads();
     constexpr int PER = kStrands / kBlock;
@@ -151,26 +179,8 @@ __device__ void compute_cn(const Dev &d)
     }
 }
 
-// Wait until *word differs from `old`, at most timeout_ns. Gives up early when
-// another block already reported a timeout in *err. On expiry sets
-// ERR_TIMEOUT in *err and returns false; never waits without a limit.
-__device__ bool bounded_wait_change(volatile unsigned *word, unsigned old, int *err,
-                                    unsigned long long timeout_ns)
-{
-    const unsigned long long t0 = globaltimer();
-    while (*word == old) {
-        if (*(volatile int *)err & ERR_TIMEOUT) return false;
-        if (globaltimer() - t0 > timeout_ns) {
-            atomicOr(err, ERR_TIMEOUT);
-            return false;
-        }
-        __nanosleep(64);
-    }
-    return true;
-}
-
 // Grid-wide barrier with a time limit. The last block to arrive optionally
-// computes cn before releasing the others. Returns false on timeout.
+// folds the strands into cn before releasing the others. False on timeout.
 __device__ bool grid_barrier(const Dev &d, bool do_cn)
 {
     __shared__ int s_last, s_ok;
@@ -186,7 +196,7 @@ __device__ bool grid_barrier(const Dev &d, bool do_cn)
     }
     __syncthreads();
     if (s_last) {
-        if (do_cn) compute_cn(d);
+        if (do_cn) fold_strands(d);
         __syncthreads();
         if (threadIdx.x == 0) {
             d.bar[0] = 0;
@@ -199,92 +209,152 @@ __device__ bool grid_barrier(const Dev &d, bool do_cn)
     return s_ok != 0;
 }
 
-// One bond seen from node i: stretch, law and damage update (state written
-// back only when it changes), and the bond force added to the chunk partial.
-template <int LAW, int PREC>
-__device__ __forceinline__ void bond_entry(const Dev &d, int64_t e, double xi, double yi,
-                                           double zi, const double *__restrict__ xs,
-                                           double &tx, double &ty, double &tz, double &ax,
-                                           double &ay, double &az)
+__device__ __forceinline__ DictEntry ldg_dict(const DictEntry *t, uint32_t c)
 {
-    const int64_t nN = d.n_nodes;
-    uint32_t w = d.colw[e];
-    int64_t j = w & COL_MASK;
-    if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
-        tx = tx + ax; ty = ty + ay; tz = tz + az;
-        ax = 0.0; ay = 0.0; az = 0.0;
-    }
-    double xj = xs[j], yj = xs[j + nN], zj = xs[j + 2 * nN];
-    double l0 = __ldg(&d.l0[e]);
-    int bt = (w >> BT_SHIFT) & 3;
-    double s0b = d.s0e ? __ldg(&d.s0e[e]) : d.P.s0;
-    double s1b = d.s1e ? __ldg(&d.s1e[e]) : d.P.s1;
-    double scb = d.sce ? __ldg(&d.sce[e]) : d.P.sc;
-    double dX, dY, dZ, L, s;
-    float dXf = 0.f, dYf = 0.f, dZf = 0.f, Lf = 0.f, sf = 0.f;
-    bool exact = true;
-    if (PREC == BBPD_PREC_FP64) {
-        bond_kinematics(xi, yi, zi, xj, yj, zj, l0, dX, dY, dZ, L, s);
-    } else {
-        // FP64 difference and squared length (no cancellation loss), FP32 rest:
-        // s = (L^2 - L0^2) / (L0 (L + L0)).
-        dX = xj - xi; dY = yj - yi; dZ = zj - zi;
-        double L2 = dX * dX + dY * dY + dZ * dZ;
-        double diff = L2 - l0 * l0;
-        float l0f = (float)l0;
-        Lf = sqrtf((float)L2);
-        sf = (float)diff / (l0f * (Lf + l0f));
-        dXf = (float)dX; dYf = (float)dY; dZf = (float)dZ;
-        // guard band: the stretch that decides breakage is recomputed in FP64
-        double crit = scb;
-        if (LAW == BBPD_LAW_LINEAR) crit = (bt == 1) ? 3 * scb : (bt == 2 ? d.P.sc_steel : scb);
-        exact = fabs((double)sf - crit) < d.guard;
-        if (exact) {
-            L = sqrt(L2);
-            s = (L - l0) / l0;
-        } else {
-            s = (double)sf;
-            L = (double)Lf;
-        }
-    }
-    double B = d.bsf[e];
-    const double B0 = B;
-    bool soft = (w & F_SOFT) != 0;
-    double failv = (w & F_BROKEN) ? 0.0 : 1.0;
-    const bool concrete = (bt == 0);
-    if (LAW == BBPD_LAW_TRILINEAR) {
-        law_trilinear(s, s0b, s1b, scb, d.P, d.s0e != nullptr || d.s1e != nullptr, concrete, B, soft);
-    } else if (LAW == BBPD_LAW_BILINEAR) {
-        law_bilinear(s, s0b, scb, concrete, B, soft);
-    } else if (LAW == BBPD_LAW_EXPONENTIAL) {
-        law_exponential(s, s0b, scb, d.P, concrete, B, soft);
-    } else {
-        law_linear(s, scb, d.P, bt, failv);
-    }
-    uint32_t w2 = (w & ~(F_SOFT | F_BROKEN)) | (soft ? F_SOFT : 0u) | (failv == 0.0 ? F_BROKEN : 0u);
-    if (w2 != w) d.colw[e] = w2;
-    if (__double_as_longlong(B) != __double_as_longlong(B0)) d.bsf[e] = B;
-    double bsv = __ldg(&d.bs[e]), vcf = __ldg(&d.vcf[e]);
-    if (PREC == BBPD_PREC_FP64 || exact) {
-        double t = bond_force_scalar(failv, bsv, B, s, 0.0, d.V, vcf);
-        ax = ax + bond_force_component(t, dX, L);
-        ay = ay + bond_force_component(t, dY, L);
-        az = az + bond_force_component(t, dZ, L);
-    } else {
-        float t = (float)(failv * bsv * (1 - B)) * sf * (float)(d.V * vcf);
-        float r = t / Lf;
-        float fx = r * dXf, fy = r * dYf, fz = r * dZf;
-        if (fx != fx) fx = 0.f;
-        if (fy != fy) fy = 0.f;
-        if (fz != fz) fz = 0.f;
-        ax = ax + (double)fx;
-        ay = ay + (double)fy;
-        az = az + (double)fz;
-    }
+    const double2 *p = reinterpret_cast<const double2 *>(t + c);
+    double2 a = __ldg(p), b = __ldg(p + 1);
+    return DictEntry{a.x, a.y, b.x, b.y};
 }
 
-template <int LAW, int SCHEME, int PREC>
-__global__ void __launch_bounds__(kBlock) step_kernel(Dev d, int64_t step0, int64_t nsteps)
+// Forces of the 32 nodes of one slice. Lane `lane` owns node sl*32+lane and
+// walks its entries in bond order; returns the node's force (reference order).
+template <int LAW, int PREC, class CID>
+__device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
+                                             const double *xs, double &tx, double &ty,
+                                             double &tz)
+{
+    const int64_t nN = d.n_nodes;
+    const int64_t i = sl * 32 + lane;
+    const int dg = (i < nN) ? d.deg[i] : 0;
+    const int64_t base = d.slice_ptr[sl] + lane;
+    const uint32_t *__restrict__ cw = d.colw + base;
+    const CID *__restrict__ cd = reinterpret_cast<const CID *>(d.cid) + base;
+    uint8_t *__restrict__ stp = d.st + base;
+    double *__restrict__ bp = d.bsf + base;
+    const double *__restrict__ scp = d.sce ? d.sce + base : nullptr;
+    const LawScalars &P = d.P;
+
+    double xi = 0, yi = 0, zi = 0;
+    if (i < nN) { xi = xs[i]; yi = xs[i + nN]; zi = xs[i + 2 * nN]; }
+    tx = 0.0; ty = 0.0; tz = 0.0;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+
+    // software pipeline: streams two entries ahead, gathers one entry ahead
+    uint32_t w1 = 0, w2 = 0;
+    uint32_t c1 = 0, c2 = 0;
+    uint8_t s1 = 0, s2 = 0;
+    double sc1 = P.sc, sc2 = P.sc;
+    if (dg > 0) { w1 = __ldg(cw); c1 = __ldg(cd); s1 = stp[0]; if (scp) sc1 = __ldg(scp); }
+    if (dg > 1) { w2 = __ldg(cw + 32); c2 = __ldg(cd + 32); s2 = stp[32]; if (scp) sc2 = __ldg(scp + 32); }
+    double xj1 = 0, yj1 = 0, zj1 = 0;
+    DictEntry g1{0, 0, 0, 0};
+    if (dg > 0) {
+        const int64_t j = w1 & COL_MASK;
+        xj1 = xs[j]; yj1 = xs[j + nN]; zj1 = xs[j + 2 * nN];
+        g1 = ldg_dict(d.dict, c1);
+    }
+    for (int k = 0; k < dg; k++) {
+        const uint32_t w = w1;
+        const uint8_t stv = s1;
+        const double xj = xj1, yj = yj1, zj = zj1, scb = sc1;
+        const DictEntry g = g1;
+        w1 = w2; c1 = c2; s1 = s2; sc1 = sc2;
+        if (k + 1 < dg) {
+            const int64_t j = w1 & COL_MASK;
+            xj1 = xs[j]; yj1 = xs[j + nN]; zj1 = xs[j + 2 * nN];
+            g1 = ldg_dict(d.dict, c1);
+        }
+        if (k + 2 < dg) {
+            const int o = (k + 2) * 32;
+            w2 = __ldg(cw + o); c2 = __ldg(cd + o); s2 = stp[o];
+            if (scp) sc2 = __ldg(scp + o);
+        }
+
+        const int bt = (w >> BT_SHIFT) & 3;
+        const double s0b = d.s0e ? __ldg(d.s0e + base + k * 32) : P.s0;
+        const double s1b = d.s1e ? __ldg(d.s1e + base + k * 32) : P.s1;
+        double dX, dY, dZ, L, s;
+        float sf = 0.f, Lf = 0.f;
+        bool exact = true;
+        if (PREC == BBPD_PREC_FP64) {
+            bond_kinematics(xi, yi, zi, xj, yj, zj, g.l0, dX, dY, dZ, L, s);
+        } else {
+            // FP64 difference and squared length (no cancellation loss), FP32
+            // rest: s = (L^2 - L0^2) / (L0 (L + L0)).
+            dX = xj - xi; dY = yj - yi; dZ = zj - zi;
+            const double L2 = dX * dX + dY * dY + dZ * dZ;
+            const double diff = L2 - g.l0 * g.l0;
+            const float l0f = (float)g.l0;
+            Lf = sqrtf((float)L2);
+            sf = (float)diff / (l0f * (Lf + l0f));
+            // guard band: the stretch that decides breakage is recomputed in FP64
+            double crit = scb;
+            if (LAW == BBPD_LAW_LINEAR) crit = (bt == 1) ? 3 * scb : (bt == 2 ? P.sc_steel : scb);
+            exact = fabs((double)sf - crit) < d.guard;
+            if (exact) {
+                L = sqrt(L2);
+                s = (L - g.l0) / g.l0;
+            } else {
+                s = (double)sf;
+                L = (double)Lf;
+            }
+        }
+
+        // law and damage (calculatebsf*.m / calculatebondfailureMex.c)
+        const double B0 = (stv & ST_DAMAGED) ? bp[k * 32] : 0.0;
+        double B = B0;
+        bool soft = (stv & ST_SOFT) != 0;
+        double failv = (stv & ST_BROKEN) ? 0.0 : 1.0;
+        const bool concrete = (bt == 0);
+        if (LAW == BBPD_LAW_TRILINEAR) {
+            law_trilinear(s, s0b, s1b, scb, P, d.s0e != nullptr || d.s1e != nullptr, concrete, B, soft);
+        } else if (LAW == BBPD_LAW_BILINEAR) {
+            law_bilinear(s, s0b, scb, concrete, B, soft);
+        } else if (LAW == BBPD_LAW_EXPONENTIAL) {
+            law_exponential(s, s0b, scb, P, concrete, B, soft);
+        } else {
+            law_linear(s, scb, P, bt, failv);
+        }
+        const bool dmg = __double_as_longlong(B) != 0;
+        const uint8_t stn = (uint8_t)((soft ? ST_SOFT : 0) | (failv == 0.0 ? ST_BROKEN : 0) | (dmg ? ST_DAMAGED : 0));
+        if (stn != stv) stp[k * 32] = stn;
+        if (__double_as_longlong(B) != __double_as_longlong(B0)) bp[k * 32] = B;
+
+        // bond force (calculatebondforcesMex.c:34-40)
+        double fx, fy, fz;
+        if (PREC == BBPD_PREC_FP64 || exact) {
+            double t;
+            if (!(stn & (ST_BROKEN | ST_DAMAGED)))
+                t = ((g.bs * s) * d.V) * g.vcf;   // fail = 1, BSF = 0: same rounding as the full product
+            else
+                t = bond_force_scalar(failv, g.bs, B, s, 0.0, d.V, g.vcf);
+            if (isfinite(t) && L > 0 && L < INFINITY) {   // no NaN can arise
+                fx = t * (dX / L); fy = t * (dY / L); fz = t * (dZ / L);
+            } else {
+                fx = bond_force_component(t, dX, L);
+                fy = bond_force_component(t, dY, L);
+                fz = bond_force_component(t, dZ, L);
+            }
+        } else {
+            const float tf = (float)(failv * g.bs * (1 - B)) * sf * (float)(d.V * g.vcf);
+            const float r = tf / Lf;
+            float gx = r * (float)dX, gy = r * (float)dY, gz = r * (float)dZ;
+            if (gx != gx) gx = 0.f;
+            if (gy != gy) gy = 0.f;
+            if (gz != gz) gz = 0.f;
+            fx = (double)gx; fy = (double)gy; fz = (double)gz;
+        }
+        if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
+            tx = tx + ax; ty = ty + ay; tz = tz + az;
+            ax = 0.0; ay = 0.0; az = 0.0;
+        }
+        ax = ax + fx; ay = ay + fy; az = az + fz;
+    }
+    tx = tx + ax; ty = ty + ay; tz = tz + az;
+}
+
+template <int LAW, int SCHEME, int PREC, class CID>
+__global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, int64_t step0, int64_t nsteps)
 {
     const int lane = threadIdx.x & 31;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -303,17 +373,8 @@ __global__ void __launch_bounds__(kBlock) step_kernel(Dev d, int64_t step0, int6
         for (int64_t sl = gwarp; sl < d.n_slices; sl += nwarps) {
             const int64_t i = sl * 32 + lane;
             const bool valid = i < nN;
-            const int dg = valid ? d.deg[i] : 0;
-            const int len = d.slice_len[sl];
-            const int64_t base = d.slice_ptr[sl] + lane;
-            double xi = 0, yi = 0, zi = 0;
-            if (valid) { xi = xs[i]; yi = xs[i + nN]; zi = xs[i + 2 * nN]; }
-            double tx = 0.0, ty = 0.0, tz = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
-            for (int k = 0; k < len; k++) {
-                if (k < dg)
-                    bond_entry<LAW, PREC>(d, base + (int64_t)k * 32, xi, yi, zi, xs, tx, ty, tz, ax, ay, az);
-            }
-            tx = tx + ax; ty = ty + ay; tz = tz + az;
+            double tx, ty, tz;
+            slice_forces<LAW, PREC, CID>(d, sl, lane, xs, tx, ty, tz);
             if (SCHEME == BBPD_SCHEME_EULERCROMER) {
                 if (valid) {
                     // timeintegrationeulercromerMex.c:33-50 on the node just summed
@@ -347,12 +408,12 @@ __global__ void __launch_bounds__(kBlock) step_kernel(Dev d, int64_t step0, int6
 #pragma unroll
                     for (int dof = 0; dof < 3; dof++) {
                         const int64_t e = i + nN * dof;
-                        double vhp = d.v[e], ue = d.u[e];
+                        const double vhp = d.v[e], ue = d.u[e];
                         if (vhp != 0) c1 = c1 - ue * ue * ((Fv[dof] / m - Fp[e] / m) / (d.dt * vhp));
                     }
 #pragma unroll
                     for (int dof = 0; dof < 3; dof++) {
-                        double ue = d.u[i + nN * dof];
+                        const double ue = d.u[i + nN * dof];
                         c2 = c2 + ue * ue;
                     }
                 }
@@ -365,6 +426,24 @@ __global__ void __launch_bounds__(kBlock) step_kernel(Dev d, int64_t step0, int6
             }
         }
         if (SCHEME == BBPD_SCHEME_ADR) {
+            if (!grid_barrier(d, false)) return;
+            // strands: strand r sums slices r, r+1024, ... in order, from 0.0
+            const int64_t ns = d.n_slices;
+            for (int64_t r = gwarp; r < kStrands; r += nwarps) {
+                double acc1 = 0.0, acc2 = 0.0;
+                for (int64_t b0 = r; b0 < ns; b0 += (int64_t)kStrands * 32) {
+                    const int64_t idx = b0 + (int64_t)lane * kStrands;
+                    const double p1 = idx < ns ? __ldcg(&d.part[idx]) : 0.0;
+                    const double p2 = idx < ns ? __ldcg(&d.part[ns + idx]) : 0.0;
+                    const int64_t left = (ns - b0 + kStrands - 1) / kStrands;
+                    const int cnt = left < 32 ? (int)left : 32;
+                    for (int q = 0; q < cnt; q++) {
+                        acc1 = acc1 + __shfl_sync(0xffffffffu, p1, q);
+                        acc2 = acc2 + __shfl_sync(0xffffffffu, p2, q);
+                    }
+                }
+                if (lane == 0) { d.strand[r] = acc1; d.strand[kStrands + r] = acc2; }
+            }
             if (!grid_barrier(d, true)) return;
             // ---- phase B: timeintegrationADR.m:168-197 ----
             const double cn = __ldcg(&d.scal[0]);
@@ -377,7 +456,8 @@ __global__ void __launch_bounds__(kBlock) step_kernel(Dev d, int64_t step0, int6
 #pragma unroll
                 for (int dof = 0; dof < 3; dof++) {
                     const int64_t e = i + nN * dof;
-                    double F = Fc[e], vh;
+                    const double F = Fc[e];
+                    double vh;
                     if (n == 1) vh = 0.5 * d.dt * minv * F;
                     else vh = (((2 - cn * d.dt) * d.v[e]) + (2 * d.dt * minv * F)) / (2 + cn * d.dt);
                     double ue = d.u[e] + (d.dt * vh);
@@ -402,36 +482,47 @@ __global__ void wait_selftest_kernel(unsigned *word, int *err, unsigned long lon
 
 typedef void (*kernel_t)(Dev, int64_t, int64_t);
 
-template <int LAW, int SCHEME>
-kernel_t pick_prec(int prec)
+template <int LAW, int SCHEME, int PREC>
+kernel_t pick_cid(bool wide)
 {
-    return prec == BBPD_PREC_FP32 ? step_kernel<LAW, SCHEME, BBPD_PREC_FP32>
-                                  : step_kernel<LAW, SCHEME, BBPD_PREC_FP64>;
+    return wide ? step_kernel<LAW, SCHEME, PREC, uint32_t> : step_kernel<LAW, SCHEME, PREC, uint16_t>;
+}
+
+template <int LAW, int SCHEME>
+kernel_t pick_prec(int prec, bool wide)
+{
+    return prec == BBPD_PREC_FP32 ? pick_cid<LAW, SCHEME, BBPD_PREC_FP32>(wide)
+                                  : pick_cid<LAW, SCHEME, BBPD_PREC_FP64>(wide);
 }
 
 template <int LAW>
-kernel_t pick_scheme(int scheme, int prec)
+kernel_t pick_scheme(int scheme, int prec, bool wide)
 {
-    return scheme == BBPD_SCHEME_ADR ? pick_prec<LAW, BBPD_SCHEME_ADR>(prec)
-                                     : pick_prec<LAW, BBPD_SCHEME_EULERCROMER>(prec);
+    return scheme == BBPD_SCHEME_ADR ? pick_prec<LAW, BBPD_SCHEME_ADR>(prec, wide)
+                                     : pick_prec<LAW, BBPD_SCHEME_EULERCROMER>(prec, wide);
 }
 
-kernel_t pick_kernel(int law, int scheme, int prec)
+kernel_t pick_kernel(int law, int scheme, int prec, bool wide)
 {
     switch (law) {
-    case BBPD_LAW_LINEAR: return pick_scheme<BBPD_LAW_LINEAR>(scheme, prec);
-    case BBPD_LAW_BILINEAR: return pick_scheme<BBPD_LAW_BILINEAR>(scheme, prec);
-    case BBPD_LAW_TRILINEAR: return pick_scheme<BBPD_LAW_TRILINEAR>(scheme, prec);
-    default: return pick_scheme<BBPD_LAW_EXPONENTIAL>(scheme, prec);
+    case BBPD_LAW_LINEAR: return pick_scheme<BBPD_LAW_LINEAR>(scheme, prec, wide);
+    case BBPD_LAW_BILINEAR: return pick_scheme<BBPD_LAW_BILINEAR>(scheme, prec, wide);
+    case BBPD_LAW_TRILINEAR: return pick_scheme<BBPD_LAW_TRILINEAR>(scheme, prec, wide);
+    default: return pick_scheme<BBPD_LAW_EXPONENTIAL>(scheme, prec, wide);
     }
 }
 
 // ------------------------------------------------------------------ host side
 
+unsigned host_threads()
+{
+    return std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+}
+
 template <class F>
 void host_parallel_for(int64_t n, F fn)
 {
-    unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    unsigned nt = host_threads();
     if (n < 65536) nt = 1;
     std::vector<std::thread> th;
     int64_t per = (n + nt - 1) / nt;
@@ -439,6 +530,18 @@ void host_parallel_for(int64_t n, F fn)
         int64_t lo = (int64_t)t * per, hi = std::min(n, lo + per);
         if (lo >= hi) break;
         th.emplace_back([=]() { for (int64_t i = lo; i < hi; i++) fn(i); });
+    }
+    for (auto &x : th) x.join();
+}
+
+// Run fn(t, lo, hi) on T contiguous ranges of [0, n), one thread each.
+template <class F>
+void host_ranges(int64_t n, int T, F fn)
+{
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; t++) {
+        int64_t lo = n * t / T, hi = n * (t + 1) / T;
+        th.emplace_back([=]() { fn(t, lo, hi); });
     }
     for (auto &x : th) x.join();
 }
@@ -464,13 +567,25 @@ uint64_t morton3(uint32_t a, uint32_t b, uint32_t c)
     return spread(a) | (spread(b) << 1) | (spread(c) << 2);
 }
 
-template <class T>
-int upload(T **d, const std::vector<T> &h)
+struct Key3 {
+    uint64_t a, b, c;
+    bool operator==(const Key3 &o) const { return a == o.a && b == o.b && c == o.c; }
+    bool operator<(const Key3 &o) const { return a != o.a ? a < o.a : (b != o.b ? b < o.b : c < o.c); }
+};
+struct Key3Hash {
+    size_t operator()(const Key3 &k) const
+    {
+        uint64_t h = k.a * 0x9E3779B97F4A7C15ull ^ (k.b + 0x632BE59BD9B4E019ull) * 0xBF58476D1CE4E5B9ull;
+        h ^= (k.c + 0x94D049BB133111EBull) * 0xD6E8FEB86659FD93ull;
+        return (size_t)(h ^ (h >> 29));
+    }
+};
+
+inline uint64_t bits_of(double x)
 {
-    size_t b = sizeof(T) * std::max<size_t>(h.size(), 1);
-    BBPD_CUDA_TRY(cudaMalloc((void **)d, b));
-    if (!h.empty()) BBPD_CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
-    return BBPD_OK;
+    uint64_t u;
+    std::memcpy(&u, &x, 8);
+    return u;
 }
 
 }  // namespace
@@ -478,11 +593,12 @@ int upload(T **d, const std::vector<T> &h)
 struct bbpd_solver {
     int device = 0;
     bbpd_params prm{};
-    int64_t nN = 0, nB = 0, ns = 0, ne = 0;
+    int64_t nN = 0, nB = 0, ns = 0, ne = 0, ndict = 0;
+    bool wide = false;
     int64_t step = 1;
     double cn = 0;
-    std::vector<int32_t> perm;      // device position -> input node
-    std::vector<int32_t> inv;       // input node -> device position
+    std::vector<int32_t> perm;          // device position -> input node
+    std::vector<int32_t> inv;           // input node -> device position
     std::vector<int64_t> ent_i, ent_j;  // bond -> entry positions of its two copies
     Dev d{};
     std::vector<void *> allocs;
@@ -492,7 +608,6 @@ struct bbpd_solver {
     int grid = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    bool has_a = false;
 
     template <class T>
     int alloc(T **p, size_t count)
@@ -504,14 +619,15 @@ struct bbpd_solver {
         return BBPD_OK;
     }
     template <class T>
-    int put(T **p, const std::vector<T> &h)
+    int put(T **p, const T *h, size_t count)
     {
-        int rc = alloc(p, h.size());
+        int rc = alloc(p, count);
         if (rc) return rc;
-        if (!h.empty())
-            BBPD_CUDA_TRY(cudaMemcpy(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+        if (count) BBPD_CUDA_TRY(cudaMemcpy(*p, h, sizeof(T) * count, cudaMemcpyHostToDevice));
         return BBPD_OK;
     }
+    template <class T>
+    int put(T **p, const std::vector<T> &h) { return put(p, h.data(), h.size()); }
     ~bbpd_solver()
     {
         for (void *p : allocs) cudaFree(p);
@@ -541,6 +657,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     const int64_t nN = pb->n_nodes, nB = pb->n_bonds;
     if (nN < 1 || nB < 0) return fail(BBPD_ERR_ARG, "n_nodes must be >= 1 and n_bonds >= 0");
     if (nN >= MAX_NODES) return fail(BBPD_ERR_UNSUPPORTED, "at most %lld nodes per solver", (long long)MAX_NODES - 1);
+    if (nB >= ((int64_t)1 << 31)) return fail(BBPD_ERR_UNSUPPORTED, "at most 2^31 - 1 bonds per solver");
     if (!pb->undeformed_coordinates || (nB && (!pb->bondlist || !pb->undeformed_length ||
         !pb->bond_stiffness || !pb->volume_correction)))
         return fail(BBPD_ERR_ARG, "missing coordinates or bond arrays");
@@ -565,18 +682,18 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         for (int64_t k = 0; k < nB; k++)
             if (pb->stretch_plastic[k] != 0)
                 return fail(BBPD_ERR_UNSUPPORTED, "non-zero stretchPlastic (steel plasticity) is not on this path");
-    // BONDLIST: integers in [1, nN], no self-bonds
-    {
-        const double *bl = pb->bondlist;
-        for (int64_t k = 0; k < nB; k++) {
-            double a = bl[k], b = bl[nB + k];
-            if (!(a >= 1 && b >= 1 && a <= (double)nN && b <= (double)nN && a == std::floor(a) &&
-                  b == std::floor(b) && a != b))
-                return fail(BBPD_ERR_ARG, "BONDLIST row %lld = (%g, %g) is not a pair of distinct node ids", (long long)k + 1, a, b);
-        }
+    const double *bl = pb->bondlist;
+    for (int64_t k = 0; k < nB; k++) {
+        double a = bl[k], b = bl[nB + k];
+        if (!(a >= 1 && b >= 1 && a <= (double)nN && b <= (double)nN && a == std::floor(a) &&
+              b == std::floor(b) && a != b))
+            return fail(BBPD_ERR_ARG, "BONDLIST row %lld = (%g, %g) is not a pair of distinct node ids", (long long)k + 1, a, b);
     }
 
-    TRY(cudaSetDevice(device) == cudaSuccess ? 0 : fail(BBPD_ERR_CUDA, "cudaSetDevice(%d)", device));
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(BBPD_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+    }
     auto *S = new bbpd_solver;
     std::unique_ptr<bbpd_solver> guard_(S);
     S->device = device;
@@ -608,18 +725,91 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         std::stable_sort(S->perm.begin(), S->perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
     }
     for (int64_t p = 0; p < nN; p++) S->inv[S->perm[p]] = (int32_t)p;
+    const int32_t *inv = S->inv.data();
 
-    // SELL-32 slices
+    // dictionary of (L0, VCF, BONDSTIFFNESS) triples
+    std::vector<uint32_t> bond_cid(nB);
+    std::vector<DictEntry> dict;
+    {
+        const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
+        std::vector<std::unordered_map<Key3, uint32_t, Key3Hash>> local(HT);
+        host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
+            auto &m = local[t];
+            for (int64_t k = lo; k < hi; k++) {
+                Key3 key{bits_of(pb->undeformed_length[k]), bits_of(pb->volume_correction[k]), bits_of(pb->bond_stiffness[k])};
+                if (m.size() <= 70000) m.emplace(key, 0u);
+            }
+        });
+        std::vector<Key3> keys;
+        bool overflow = false;
+        {
+            std::unordered_map<Key3, uint32_t, Key3Hash> all;
+            for (auto &m : local) {
+                if (m.size() > 70000) overflow = true;
+                for (auto &kv : m) all.emplace(kv.first, 0u);
+            }
+            if (all.size() > 65535) overflow = true;
+            if (!overflow) {
+                keys.reserve(all.size());
+                for (auto &kv : all) keys.push_back(kv.first);
+            }
+        }
+        if (!overflow) {
+            std::sort(keys.begin(), keys.end());
+            std::unordered_map<Key3, uint32_t, Key3Hash> id;
+            for (size_t q = 0; q < keys.size(); q++) id.emplace(keys[q], (uint32_t)q);
+            host_ranges(nB, HT, [&](int, int64_t lo, int64_t hi) {
+                for (int64_t k = lo; k < hi; k++) {
+                    Key3 key{bits_of(pb->undeformed_length[k]), bits_of(pb->volume_correction[k]), bits_of(pb->bond_stiffness[k])};
+                    bond_cid[k] = id.find(key)->second;
+                }
+            });
+            dict.resize(keys.size());
+            for (size_t q = 0; q < keys.size(); q++) {
+                double l0, vcf, bs;
+                std::memcpy(&l0, &keys[q].a, 8);
+                std::memcpy(&vcf, &keys[q].b, 8);
+                std::memcpy(&bs, &keys[q].c, 8);
+                dict[q] = DictEntry{l0, vcf, bs, 0.0};
+            }
+        } else {
+            // irregular input: one dictionary entry per bond, 32-bit ids
+            S->wide = true;
+            dict.resize(nB);
+            for (int64_t k = 0; k < nB; k++) {
+                dict[k] = DictEntry{pb->undeformed_length[k], pb->volume_correction[k], pb->bond_stiffness[k], 0.0};
+                bond_cid[k] = (uint32_t)k;
+            }
+        }
+        if (dict.empty()) dict.push_back(DictEntry{1.0, 0.0, 0.0, 0.0});
+        S->ndict = (int64_t)dict.size();
+    }
+
+    // per-node lists in bond order, laid out in 32-node slices. Stable
+    // counting sort over HT contiguous bond ranges.
     const int64_t ns = (nN + 31) / 32;
     S->ns = ns;
+    const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
+    std::vector<std::vector<int32_t>> cnt(HT, std::vector<int32_t>(nN, 0));
+    host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
+        int32_t *c = cnt[t].data();
+        for (int64_t k = lo; k < hi; k++) {
+            c[inv[(int64_t)bl[k] - 1]]++;
+            c[inv[(int64_t)bl[nB + k] - 1]]++;
+        }
+    });
     std::vector<int32_t> deg(nN, 0);
-    const double *bl = pb->bondlist;
-    for (int64_t k = 0; k < nB; k++) {
-        deg[S->inv[(int64_t)bl[k] - 1]]++;
-        deg[S->inv[(int64_t)bl[nB + k] - 1]]++;
-    }
-    std::vector<int32_t> slen(ns, 0);
+    host_parallel_for(nN, [&](int64_t p) {
+        int32_t acc = 0;
+        for (int t = 0; t < HT; t++) {
+            int32_t c = cnt[t][p];
+            cnt[t][p] = acc;   // becomes the thread's first rank in node p's list
+            acc += c;
+        }
+        deg[p] = acc;
+    });
     std::vector<int64_t> sptr(ns + 1, 0);
+    std::vector<int32_t> slen(ns, 0);
     for (int64_t s = 0; s < ns; s++) {
         int m = 0;
         for (int64_t i = s * 32; i < std::min(nN, s * 32 + 32); i++) m = std::max(m, deg[i]);
@@ -629,37 +819,53 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     const int64_t ne = sptr[ns];
     S->ne = ne;
     std::vector<uint32_t> colw(ne, 0);
-    std::vector<double> l0(ne, 0.0), bsv(ne, 0.0), vcf(ne, 0.0), bsf(ne, 0.0);
+    std::vector<uint16_t> cid16;
+    std::vector<uint32_t> cid32;
+    if (S->wide) cid32.assign(ne, 0);
+    else cid16.assign(ne, 0);
+    std::vector<uint8_t> st(ne, 0);
+    std::vector<int32_t> bond_of(ne, -1);
     std::vector<double> s0e, s1e, sce;
     if (pb->s0) s0e.assign(ne, 0.0);
     if (pb->s1) s1e.assign(ne, 0.0);
     if (pb->sc) sce.assign(ne, 0.0);
     S->ent_i.resize(nB);
     S->ent_j.resize(nB);
-    {
-        std::vector<int32_t> cnt(nN, 0), last(nN, -1);
-        for (int64_t k = 0; k < nB; k++) {
-            const int c = chunk_of_host(k, nB, T);
-            const int64_t a = S->inv[(int64_t)bl[k] - 1], b = S->inv[(int64_t)bl[nB + k] - 1];
-            uint32_t st = 0;
-            if (pb->fail && pb->fail[k] == 0) st |= F_BROKEN;
-            if (pb->bond_type) st |= (uint32_t)pb->bond_type[k] << BT_SHIFT;
+    host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
+        int32_t *rank = cnt[t].data();
+        for (int64_t k = lo; k < hi; k++) {
+            const int64_t a = inv[(int64_t)bl[k] - 1], b = inv[(int64_t)bl[nB + k] - 1];
+            const uint32_t bt = pb->bond_type ? (uint32_t)pb->bond_type[k] << BT_SHIFT : 0u;
+            const uint8_t st0 = (pb->fail && pb->fail[k] == 0) ? ST_BROKEN : 0;
             for (int side = 0; side < 2; side++) {
                 const int64_t me = side ? b : a, other = side ? a : b;
-                const int64_t pos = sptr[me / 32] + (int64_t)cnt[me] * 32 + (me % 32);
-                cnt[me]++;
-                colw[pos] = (uint32_t)other | st | (c != last[me] ? F_CHUNK : 0u);
-                last[me] = c;
-                l0[pos] = pb->undeformed_length[k];
-                bsv[pos] = pb->bond_stiffness[k];
-                vcf[pos] = pb->volume_correction[k];
+                const int64_t pos = sptr[me / 32] + (int64_t)rank[me] * 32 + (me % 32);
+                rank[me]++;
+                colw[pos] = (uint32_t)other | bt;
+                if (S->wide) cid32[pos] = bond_cid[k];
+                else cid16[pos] = (uint16_t)bond_cid[k];
+                st[pos] = st0;
+                bond_of[pos] = (int32_t)k;
                 if (pb->s0) s0e[pos] = pb->s0[k];
                 if (pb->s1) s1e[pos] = pb->s1[k];
                 if (pb->sc) sce[pos] = pb->sc[k];
                 (side ? S->ent_j : S->ent_i)[k] = pos;
             }
         }
-    }
+    });
+    // chunk starts: an entry whose bond lies in another OpenMP chunk than the
+    // previous entry of the same list
+    host_parallel_for(nN, [&](int64_t me) {
+        int prev = -1;
+        for (int32_t r = 0; r < deg[me]; r++) {
+            const int64_t pos = sptr[me / 32] + (int64_t)r * 32 + (me % 32);
+            const int c = chunk_of_host(bond_of[pos], nB, T);
+            if (c != prev) colw[pos] |= F_CHUNK;
+            prev = c;
+        }
+    });
+    std::vector<int32_t>().swap(bond_of);
+    cnt.clear();
 
     // node arrays in device order
     auto perm3 = [&](const double *src, std::vector<double> &dst) {
@@ -679,14 +885,12 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     perm1(pb->density, rho);
     std::vector<uint8_t> nflag(nN, 0);
     double U1;
-    {
-        // prescribed value at step 1 (same arithmetic as the device)
-        if (prm->amplitude == BBPD_AMP_SMOOTHSTEP) {
-            double xi = (1.0 - 1.0) / ((double)prm->n_time_steps - 1.0);
-            U1 = 0.0 + (prm->applied_final - 0.0) * ((xi * xi) * xi) * (10 - 15 * xi + 6 * (xi * xi));
-        } else {
-            U1 = prm->rate * 1.0;
-        }
+    if (prm->amplitude == BBPD_AMP_SMOOTHSTEP) {
+        // prescribed value at step 1, same arithmetic as the device
+        double xi = (1.0 - 1.0) / ((double)prm->n_time_steps - 1.0);
+        U1 = 0.0 + (prm->applied_final - 0.0) * ((xi * xi) * xi) * (10 - 15 * xi + 6 * (xi * xi));
+    } else {
+        U1 = prm->rate * 1.0;
     }
     for (int64_t p = 0; p < nN; p++) {
         int64_t i = S->perm[p];
@@ -706,13 +910,14 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     d.n_nodes = nN;
     d.n_slices = ns;
     TRY(S->put((int64_t **)&d.slice_ptr, sptr));
-    TRY(S->put((int32_t **)&d.slice_len, slen));
     TRY(S->put((int32_t **)&d.deg, deg));
-    TRY(S->put(&d.colw, colw));
-    TRY(S->put(&d.bsf, bsf));
-    TRY(S->put((double **)&d.l0, l0));
-    TRY(S->put((double **)&d.bs, bsv));
-    TRY(S->put((double **)&d.vcf, vcf));
+    TRY(S->put((uint32_t **)&d.colw, colw));
+    if (S->wide) TRY(S->put((uint32_t **)&d.cid, cid32));
+    else TRY(S->put((uint16_t **)&d.cid, cid16));
+    TRY(S->put(&d.st, st));
+    TRY(S->alloc(&d.bsf, (size_t)ne));
+    BBPD_CUDA_TRY(cudaMemset(d.bsf, 0, sizeof(double) * std::max<int64_t>(ne, 1)));
+    TRY(S->put((DictEntry **)&d.dict, dict));
     d.s0e = d.s1e = d.sce = nullptr;
     if (pb->s0) TRY(S->put((double **)&d.s0e, s0e));
     if (pb->s1) TRY(S->put((double **)&d.s1e, s1e));
@@ -725,13 +930,13 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     TRY(S->put(&d.v, zeros3));
     TRY(S->put(&d.F0, zeros3));
     TRY(S->put(&d.F1, zeros3));
-    S->has_a = prm->scheme == BBPD_SCHEME_EULERCROMER;
     d.a = nullptr;
-    if (S->has_a) TRY(S->put(&d.a, zeros3));
+    if (prm->scheme == BBPD_SCHEME_EULERCROMER) TRY(S->put(&d.a, zeros3));
     TRY(S->put((double **)&d.mass, mass));
     TRY(S->put((double **)&d.rho, rho));
     TRY(S->put((uint8_t **)&d.nflag, nflag));
     TRY(S->alloc(&d.part, (size_t)(2 * ns)));
+    TRY(S->alloc(&d.strand, (size_t)(2 * kStrands)));
     std::vector<double> sc4(4, 0.0);
     TRY(S->put(&d.scal, sc4));
     std::vector<unsigned> bar(2, 0u);
@@ -763,7 +968,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     d.timeout_ns = (unsigned long long)(to * 1e9);
 
     // kernel and grid
-    S->kernel = pick_kernel(prm->law, prm->scheme, prm->precision);
+    S->kernel = pick_kernel(prm->law, prm->scheme, prm->precision, S->wide);
     int nsm = 0, occ = 0, coop = 0;
     BBPD_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     BBPD_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
@@ -776,17 +981,15 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     BBPD_CUDA_TRY(cudaEventCreate(&S->ev0));
     BBPD_CUDA_TRY(cudaEventCreate(&S->ev1));
 
-    // algorithmic DRAM bytes of one step for this layout
+    // DRAM bytes one step moves with this layout (streams of the live entries,
+    // node arrays; dictionary and damaged-bond BSF reads excluded)
     {
-        double per_entry = 4 + 8 + 3 * 8 + (pb->s0 ? 8 : 0) + (pb->s1 ? 8 : 0) + (pb->sc ? 8 : 0);
-        double live = 0;
-        for (int64_t i = 0; i < nN; i++) live += deg[i];
+        double per_entry = 4 + (S->wide ? 4 : 2) + 1 + (pb->s0 ? 8 : 0) + (pb->s1 ? 8 : 0) + (pb->sc ? 8 : 0);
         double node = prm->scheme == BBPD_SCHEME_ADR
-                          ? (24 /*x*/ + 24 + 24 + 24 + 8 /*u v Fp m*/ + 24 /*F w*/ + 4 /*deg*/ +
-                             24 + 24 + 24 + 24 + 8 + 1 /*F u v X m flag*/ + 72 /*v u x w*/)
-                          : (24 + 4 + 24 /*v*/ + 24 /*u*/ + 8 /*rho*/ + 1 + 24 /*X*/ +
-                             24 * 5 /*F a v u x w*/);
-        S->bytes_per_step = live * per_entry + (double)nN * node;
+                          ? (24 /*x*/ + 4 /*deg*/ + 24 * 3 + 8 /*u v Fp m*/ + 24 /*F w*/ +
+                             24 * 4 + 8 + 1 /*F u v X m flag*/ + 72 /*v u x w*/)
+                          : (24 + 4 + 24 * 3 + 8 + 1 /*x v u X rho flag*/ + 24 * 5 /*F a v u x w*/);
+        S->bytes_per_step = 2.0 * (double)nB * per_entry + (double)nN * node;
     }
     BBPD_CUDA_TRY(cudaDeviceSynchronize());
     *out = guard_.release();
@@ -889,17 +1092,17 @@ extern "C" int bbpd_get(bbpd_solver *S, int field, double *out)
         return BBPD_OK;
     }
     if (field == BBPD_FIELD_BSF) {
-        std::vector<double> h(S->ne);
+        std::vector<double> h(std::max<int64_t>(S->ne, 1));
         BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.bsf, sizeof(double) * S->ne, cudaMemcpyDeviceToHost));
         for (int64_t k = 0; k < nB; k++) out[k] = h[S->ent_i[k]];
         return BBPD_OK;
     }
     if (field == BBPD_FIELD_FLAG || field == BBPD_FIELD_FAIL) {
-        std::vector<uint32_t> h(S->ne);
-        BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.colw, sizeof(uint32_t) * S->ne, cudaMemcpyDeviceToHost));
+        std::vector<uint8_t> h(std::max<int64_t>(S->ne, 1));
+        BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.st, S->ne, cudaMemcpyDeviceToHost));
         for (int64_t k = 0; k < nB; k++) {
-            uint32_t w = h[S->ent_i[k]];
-            out[k] = field == BBPD_FIELD_FLAG ? ((w & F_SOFT) ? 1.0 : 0.0) : ((w & F_BROKEN) ? 0.0 : 1.0);
+            const uint8_t w = h[S->ent_i[k]];
+            out[k] = field == BBPD_FIELD_FLAG ? ((w & ST_SOFT) ? 1.0 : 0.0) : ((w & ST_BROKEN) ? 0.0 : 1.0);
         }
         return BBPD_OK;
     }
@@ -926,26 +1129,33 @@ extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
         }
         return BBPD_OK;
     }
+    if (field != BBPD_FIELD_BSF && field != BBPD_FIELD_FLAG && field != BBPD_FIELD_FAIL)
+        return fail(BBPD_ERR_ARG, "unknown field %d", field);
+    if (field != BBPD_FIELD_BSF) TRY(validate_01(in, nB, field == BBPD_FIELD_FLAG ? "flagBondSoftening" : "fail"));
+    const int64_t ne1 = std::max<int64_t>(S->ne, 1);
+    std::vector<uint8_t> st(ne1);
+    BBPD_CUDA_TRY(cudaMemcpy(st.data(), S->d.st, S->ne, cudaMemcpyDeviceToHost));
     if (field == BBPD_FIELD_BSF) {
-        std::vector<double> h(S->ne);
+        std::vector<double> h(ne1);
         BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.bsf, sizeof(double) * S->ne, cudaMemcpyDeviceToHost));
-        for (int64_t k = 0; k < nB; k++) h[S->ent_i[k]] = h[S->ent_j[k]] = in[k];
-        BBPD_CUDA_TRY(cudaMemcpy(S->d.bsf, h.data(), sizeof(double) * S->ne, cudaMemcpyHostToDevice));
-        return BBPD_OK;
-    }
-    if (field == BBPD_FIELD_FLAG || field == BBPD_FIELD_FAIL) {
-        TRY(validate_01(in, nB, field == BBPD_FIELD_FLAG ? "flagBondSoftening" : "fail"));
-        std::vector<uint32_t> h(S->ne);
-        BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.colw, sizeof(uint32_t) * S->ne, cudaMemcpyDeviceToHost));
-        const uint32_t bit = field == BBPD_FIELD_FLAG ? F_SOFT : F_BROKEN;
         for (int64_t k = 0; k < nB; k++) {
-            bool on = field == BBPD_FIELD_FLAG ? in[k] == 1 : in[k] == 0;
-            for (int64_t pos : {S->ent_i[k], S->ent_j[k]}) h[pos] = on ? (h[pos] | bit) : (h[pos] & ~bit);
+            const bool dmg = bits_of(in[k]) != 0;
+            for (int64_t pos : {S->ent_i[k], S->ent_j[k]}) {
+                h[pos] = in[k];
+                st[pos] = dmg ? (uint8_t)(st[pos] | ST_DAMAGED) : (uint8_t)(st[pos] & ~ST_DAMAGED);
+            }
         }
-        BBPD_CUDA_TRY(cudaMemcpy(S->d.colw, h.data(), sizeof(uint32_t) * S->ne, cudaMemcpyHostToDevice));
-        return BBPD_OK;
+        BBPD_CUDA_TRY(cudaMemcpy(S->d.bsf, h.data(), sizeof(double) * S->ne, cudaMemcpyHostToDevice));
+    } else {
+        const uint8_t bit = field == BBPD_FIELD_FLAG ? ST_SOFT : ST_BROKEN;
+        for (int64_t k = 0; k < nB; k++) {
+            const bool on = field == BBPD_FIELD_FLAG ? in[k] == 1 : in[k] == 0;
+            for (int64_t pos : {S->ent_i[k], S->ent_j[k]})
+                st[pos] = on ? (uint8_t)(st[pos] | bit) : (uint8_t)(st[pos] & ~bit);
+        }
     }
-    return fail(BBPD_ERR_ARG, "unknown field %d", field);
+    BBPD_CUDA_TRY(cudaMemcpy(S->d.st, st.data(), S->ne, cudaMemcpyHostToDevice));
+    return BBPD_OK;
 }
 
 extern "C" int bbpd_get_step(bbpd_solver *S, int64_t *step, double *cn)
@@ -1006,6 +1216,7 @@ extern "C" int bbpd_get_info(bbpd_solver *S, bbpd_info *info)
     info->block_threads = kBlock;
     info->device_bytes = S->device_bytes;
     info->bytes_per_step = S->bytes_per_step;
-    info->layout = 0;
+    info->layout = S->wide ? 2 : 1;
+    info->reserved = (int32_t)std::min<int64_t>(S->ndict, INT32_MAX);
     return BBPD_OK;
 }

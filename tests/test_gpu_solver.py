@@ -33,11 +33,16 @@ def same(a, b):
     return a.shape == b.shape and bool(np.all((a == b) | (np.isnan(a) & np.isnan(b))))
 
 
-def compare(s, r, law, fields=NODAL + BOND, rtol=1e-10):
+def compare(s, r, law, fields=NODAL + BOND, rtol=1e-9):
+    """Bit-identical, except the exponential law: CUDA's exp() and glibc's may
+    differ in the last bit, and undamped dynamics carry that along; there nodal
+    fields must agree within 1e-9 of their largest magnitude, damage within
+    1e-8, and softening flags and the broken-bond set exactly."""
     for f in fields:
         a, b = s.get(f), r.get(f)
         if law == "exponential" and f not in ("flag", "fail"):
-            np.testing.assert_allclose(a, b, rtol=rtol, atol=rtol * max(np.abs(b).max(), 1e-300), err_msg=f)
+            atol = 1e-8 if f == "bsf" else rtol * max(np.abs(b).max(), 1e-300)
+            np.testing.assert_allclose(a, b, rtol=0, atol=atol, err_msg=f)
         else:
             assert same(a, b), f"{f}: {np.sum(a != b)} of {a.size} differ"
     assert np.array_equal(s.get("bsf") == 1, r.get("bsf") == 1)
