@@ -116,6 +116,7 @@ def lib() -> C.CDLL:
         L.bbpd_get_info.argtypes = [C.c_void_p, C.POINTER(Info)]
         L.bbpd_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
         L.bbpd_selftest_wait_timeout.argtypes = [C.c_double]
+        L.bbpd_selftest_division.argtypes = [C.c_int64, C.c_uint64] + [C.POINTER(C.c_int64)] * 3 + [_P]
         L.bbpd_beam_count.argtypes = [C.POINTER(BeamSpec), C.POINTER(BeamScalars)]
         L.bbpd_beam_build.argtypes = [C.POINTER(BeamSpec)] + [_P] * 11
         _lib = L

@@ -35,6 +35,7 @@
 // Grid barriers spin with a time limit; on expiry they set an error flag and
 // the kernel returns early (status BBPD_ERR_TIMEOUT), never hanging.
 #include "bbpd_internal.h"
+#include "divide.cuh"
 #include "physics.cuh"
 
 #include <algorithm>
@@ -67,8 +68,15 @@ constexpr int kBlock = 256;
 #endif
 constexpr int kStrands = 1024;
 
+// One dictionary entry: the bond constants in FP64, RN(1/L0) for the shared-
+// divisor division, the FP32 product BONDSTIFFNESS * cellVolume * VCF for the
+// FP32 form, and flags (bit 0: a constant is not finite or L0 lies outside
+// [2^-100, 2^100]; entries using it take the general path).
 struct DictEntry {
-    double l0, vcf, bs, pad;
+    double l0, rl0, vcf, bs;
+    float k32;
+    uint32_t flags;
+    double pad;
 };
 
 struct Dev {
@@ -91,6 +99,8 @@ struct Dev {
     double *strand;                  // 2 * kStrands strand sums
     double *scal;                    // [0] = cn
     unsigned *bar;                   // [0] arrivals, [1] generation
+    unsigned *sticky;                // bit 0: a coordinate left the range of the fast division
+    const int64_t *wrange;           // slices [wrange[w], wrange[w+1]) belong to warp w
     int *err;
     LawScalars P;
     double V, dt, damping;
@@ -212,14 +222,196 @@ __device__ bool grid_barrier(const Dev &d, bool do_cn)
 __device__ __forceinline__ DictEntry ldg_dict(const DictEntry *t, uint32_t c)
 {
     const double2 *p = reinterpret_cast<const double2 *>(t + c);
-    double2 a = __ldg(p), b = __ldg(p + 1);
-    return DictEntry{a.x, a.y, b.x, b.y};
+    const double2 a = __ldg(p), b = __ldg(p + 1), m = __ldg(p + 2);
+    DictEntry e;
+    e.l0 = a.x;
+    e.rl0 = a.y;
+    e.vcf = b.x;
+    e.bs = b.y;
+    e.k32 = __int_as_float(__double2loint(m.x));
+    e.flags = (uint32_t)__double2hiint(m.x);
+    e.pad = 0;
+    return e;
+}
+
+// Per-entry data, fetched before the arithmetic of the entry.
+struct Fetch {
+    uint32_t w;
+    uint32_t sv;
+    double xj, yj, zj, sc;
+    DictEntry g;
+};
+
+template <class CID>
+__device__ __forceinline__ void fetch(const Dev &d, const uint32_t *__restrict__ cw,
+                                      const CID *__restrict__ cd, const uint8_t *stp,
+                                      const double *__restrict__ scp,
+                                      const double *x0, const double *x1, const double *x2,
+                                      int o, Fetch &f)
+{
+    f.w = __ldg(cw + o);
+    const uint32_t c = __ldg(cd + o);
+    f.sv = stp[o];
+    f.sc = scp ? __ldg(scp + o) : d.P.sc;
+    const uint32_t j = f.w & COL_MASK;
+    f.xj = x0[j];
+    f.yj = x1[j];
+    f.zj = x2[j];
+    f.g = ldg_dict(d.dict, c);
+}
+
+// Critical stretch whose crossing breaks a bond under the brittle law
+// (calculatebondfailureMex.c:36-38).
+__device__ __forceinline__ double linear_crit(const LawScalars &P, int bt, double sc)
+{
+    return (bt == 1) ? 3 * sc : (bt == 2 ? P.sc_steel : sc);
+}
+
+// True when the law cannot change the state of an intact, undamaged bond
+// (state byte 0) at stretch s; NaN stretch counts as quiet.
+template <int LAW>
+__device__ __forceinline__ bool law_quiet(const LawScalars &P, int bt, double s, double s0,
+                                          double sc)
+{
+    if (LAW == BBPD_LAW_LINEAR) return !(s > linear_crit(P, bt, sc));
+    return !(bt == 0 && s > s0);
+}
+
+// One entry in full generality: law, damage state written back when it
+// changes, bond force with the NaN guards of calculatebondforcesMex.c. Kept
+// out of line: intact bonds whose law is quiet never come here.
+#ifdef BBPD_GENERAL_OUTLINE
+#define BBPD_GENERAL_ATTR __noinline__
+#else
+#define BBPD_GENERAL_ATTR __forceinline__
+#endif
+template <int LAW, int PREC>
+__device__ BBPD_GENERAL_ATTR double3 entry_general(const Dev &d, int64_t e, uint32_t w, uint32_t sv,
+                                              DictEntry g, double scb, double xi, double yi,
+                                              double zi, double xj, double yj, double zj)
+{
+    const LawScalars &P = d.P;
+    const int bt = (w >> BT_SHIFT) & 3;
+    const double s0b = d.s0e ? __ldg(d.s0e + e) : P.s0;
+    const double s1b = d.s1e ? __ldg(d.s1e + e) : P.s1;
+    double dX, dY, dZ, L, s;
+    float sf = 0.f, Lf = 0.f;
+    bool exact = true;
+    if (PREC == BBPD_PREC_FP64) {
+        bond_kinematics(xi, yi, zi, xj, yj, zj, g.l0, dX, dY, dZ, L, s);
+    } else {
+        dX = xj - xi; dY = yj - yi; dZ = zj - zi;
+        const double L2 = dX * dX + dY * dY + dZ * dZ;
+        const double diff = L2 - g.l0 * g.l0;
+        const float l0f = (float)g.l0;
+        Lf = sqrtf((float)L2);
+        sf = (float)diff / (l0f * (Lf + l0f));
+        const double crit = (LAW == BBPD_LAW_LINEAR) ? linear_crit(P, bt, scb) : scb;
+        exact = fabs((double)sf - crit) < d.guard;
+        if (exact) {
+            L = sqrt(L2);
+            s = (L - g.l0) / g.l0;
+        } else {
+            s = (double)sf;
+            L = (double)Lf;
+        }
+    }
+    // law and damage (calculatebsf*.m / calculatebondfailureMex.c)
+    const double B0 = (sv & ST_DAMAGED) ? d.bsf[e] : 0.0;
+    double B = B0;
+    bool soft = (sv & ST_SOFT) != 0;
+    double failv = (sv & ST_BROKEN) ? 0.0 : 1.0;
+    const bool concrete = (bt == 0);
+    if (LAW == BBPD_LAW_TRILINEAR) {
+        law_trilinear(s, s0b, s1b, scb, P, d.s0e != nullptr || d.s1e != nullptr, concrete, B, soft);
+    } else if (LAW == BBPD_LAW_BILINEAR) {
+        law_bilinear(s, s0b, scb, concrete, B, soft);
+    } else if (LAW == BBPD_LAW_EXPONENTIAL) {
+        law_exponential(s, s0b, scb, P, concrete, B, soft);
+    } else {
+        law_linear(s, scb, P, bt, failv);
+    }
+    const bool dmg = __double_as_longlong(B) != 0;
+    const uint32_t stn = (soft ? ST_SOFT : 0u) | (failv == 0.0 ? ST_BROKEN : 0u) | (dmg ? ST_DAMAGED : 0u);
+    if (stn != sv) d.st[e] = (uint8_t)stn;
+    if (__double_as_longlong(B) != __double_as_longlong(B0)) d.bsf[e] = B;
+    // bond force (calculatebondforcesMex.c:34-40)
+    double3 f;
+    if (PREC == BBPD_PREC_FP64 || exact) {
+        const double t = bond_force_scalar(failv, g.bs, B, s, 0.0, d.V, g.vcf);
+        f.x = bond_force_component(t, dX, L);
+        f.y = bond_force_component(t, dY, L);
+        f.z = bond_force_component(t, dZ, L);
+    } else {
+        const float tf = (float)(failv * g.bs * (1 - B)) * sf * (float)(d.V * g.vcf);
+        const float r = tf / Lf;
+        float gx = r * (float)dX, gy = r * (float)dY, gz = r * (float)dZ;
+        if (gx != gx) gx = 0.f;
+        if (gy != gy) gy = 0.f;
+        if (gz != gz) gz = 0.f;
+        f.x = (double)gx; f.y = (double)gy; f.z = (double)gz;
+    }
+    return f;
+}
+
+// Force of one entry. The common case, an intact and undamaged bond whose law
+// stays quiet, is computed inline: with fail = 1 and BSF = 0 the reference
+// product fail*BS*(1-BSF)*s*V*VCF rounds exactly like ((BS*s)*V)*VCF, and with
+// 0 < L < inf and a regular dictionary entry no NaN can arise.
+template <int LAW, int PREC>
+__device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fetch &f, bool safe,
+                                               double xi, double yi, double zi)
+{
+    const int bt = (f.w >> BT_SHIFT) & 3;
+    const double s0b = d.s0e ? __ldg(d.s0e + e) : d.P.s0;
+    double3 r;
+    if (PREC == BBPD_PREC_FP64) {
+        // calculatedeformedlengthMex.c:37-43 with its two divisions by L0 and
+        // the three of calculatebondforcesMex.c:34-36 by L done as
+        // correctly rounded quotients with shared reciprocals (divide.cuh):
+        // bit-identical to IEEE division whenever `safe` holds.
+        const double dX = f.xj - xi, dY = f.yj - yi, dZ = f.zj - zi;
+        const double L = sqrt(dX * dX + dY * dY + dZ * dZ);
+        const double s = quot_rn(L - f.g.l0, f.g.l0, f.g.rl0);
+        bool okr;
+        const double rL = recip_rn(L, okr);
+        if (safe && okr && f.sv == 0 && f.g.flags == 0 && L > 0 &&
+            law_quiet<LAW>(d.P, bt, s, s0b, f.sc)) {
+            const double t = ((f.g.bs * s) * d.V) * f.g.vcf;
+            r.x = t * quot_rn(dX, L, rL);
+            r.y = t * quot_rn(dY, L, rL);
+            r.z = t * quot_rn(dZ, L, rL);
+            return r;
+        }
+    } else {
+        // FP64 difference and squared length (no cancellation loss), FP32 rest:
+        // s = (L^2 - L0^2) / (L0 (L + L0)); FP64 sums of the FP32 forces.
+        const double dX = f.xj - xi, dY = f.yj - yi, dZ = f.zj - zi;
+        const double L2 = dX * dX + dY * dY + dZ * dZ;
+        const double diff = L2 - f.g.l0 * f.g.l0;
+        const float L2f = (float)L2, l0f = (float)f.g.l0;
+        const float ri = rsqrtf(L2f);
+        const float Lf = L2f * ri;
+        const float sf = __fdividef((float)diff, l0f * (Lf + l0f));
+        const double crit = (LAW == BBPD_LAW_LINEAR) ? linear_crit(d.P, bt, f.sc) : f.sc;
+        // guard band: near the critical stretch the general path decides in FP64
+        if (f.sv == 0 && f.g.flags == 0 && L2f > 0.f && L2f < INFINITY &&
+            !(fabs((double)sf - crit) < d.guard) && law_quiet<LAW>(d.P, bt, (double)sf, s0b, f.sc)) {
+            const float q = f.g.k32 * sf * ri;
+            r.x = (double)(q * (float)dX);
+            r.y = (double)(q * (float)dY);
+            r.z = (double)(q * (float)dZ);
+            return r;
+        }
+    }
+    return entry_general<LAW, PREC>(d, e, f.w, f.sv, f.g, f.sc, xi, yi, zi, f.xj, f.yj, f.zj);
 }
 
 // Forces of the 32 nodes of one slice. Lane `lane` owns node sl*32+lane and
-// walks its entries in bond order; returns the node's force (reference order).
+// walks its entries in bond order, two entries fetched per round; returns the
+// node's force summed in the reference's order.
 template <int LAW, int PREC, class CID>
-__device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
+__device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane, bool safe,
                                              const double *xs, double &tx, double &ty,
                                              double &tz)
 {
@@ -229,128 +421,45 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
     const int64_t base = d.slice_ptr[sl] + lane;
     const uint32_t *__restrict__ cw = d.colw + base;
     const CID *__restrict__ cd = reinterpret_cast<const CID *>(d.cid) + base;
-    uint8_t *__restrict__ stp = d.st + base;
-    double *__restrict__ bp = d.bsf + base;
+    const uint8_t *stp = d.st + base;
     const double *__restrict__ scp = d.sce ? d.sce + base : nullptr;
-    const LawScalars &P = d.P;
+    const double *x0 = xs, *x1 = xs + nN, *x2 = xs + 2 * nN;
 
     double xi = 0, yi = 0, zi = 0;
-    if (i < nN) { xi = xs[i]; yi = xs[i + nN]; zi = xs[i + 2 * nN]; }
+    if (i < nN) { xi = x0[i]; yi = x1[i]; zi = x2[i]; }
     tx = 0.0; ty = 0.0; tz = 0.0;
     double ax = 0.0, ay = 0.0, az = 0.0;
-
-    // software pipeline: streams two entries ahead, gathers one entry ahead
-    uint32_t w1 = 0, w2 = 0;
-    uint32_t c1 = 0, c2 = 0;
-    uint8_t s1 = 0, s2 = 0;
-    double sc1 = P.sc, sc2 = P.sc;
-    if (dg > 0) { w1 = __ldg(cw); c1 = __ldg(cd); s1 = stp[0]; if (scp) sc1 = __ldg(scp); }
-    if (dg > 1) { w2 = __ldg(cw + 32); c2 = __ldg(cd + 32); s2 = stp[32]; if (scp) sc2 = __ldg(scp + 32); }
-    double xj1 = 0, yj1 = 0, zj1 = 0;
-    DictEntry g1{0, 0, 0, 0};
-    if (dg > 0) {
-        const int64_t j = w1 & COL_MASK;
-        xj1 = xs[j]; yj1 = xs[j + nN]; zj1 = xs[j + 2 * nN];
-        g1 = ldg_dict(d.dict, c1);
-    }
-    for (int k = 0; k < dg; k++) {
-        const uint32_t w = w1;
-        const uint8_t stv = s1;
-        const double xj = xj1, yj = yj1, zj = zj1, scb = sc1;
-        const DictEntry g = g1;
-        w1 = w2; c1 = c2; s1 = s2; sc1 = sc2;
-        if (k + 1 < dg) {
-            const int64_t j = w1 & COL_MASK;
-            xj1 = xs[j]; yj1 = xs[j + nN]; zj1 = xs[j + 2 * nN];
-            g1 = ldg_dict(d.dict, c1);
-        }
-        if (k + 2 < dg) {
-            const int o = (k + 2) * 32;
-            w2 = __ldg(cw + o); c2 = __ldg(cd + o); s2 = stp[o];
-            if (scp) sc2 = __ldg(scp + o);
-        }
-
-        const int bt = (w >> BT_SHIFT) & 3;
-        const double s0b = d.s0e ? __ldg(d.s0e + base + k * 32) : P.s0;
-        const double s1b = d.s1e ? __ldg(d.s1e + base + k * 32) : P.s1;
-        double dX, dY, dZ, L, s;
-        float sf = 0.f, Lf = 0.f;
-        bool exact = true;
-        if (PREC == BBPD_PREC_FP64) {
-            bond_kinematics(xi, yi, zi, xj, yj, zj, g.l0, dX, dY, dZ, L, s);
-        } else {
-            // FP64 difference and squared length (no cancellation loss), FP32
-            // rest: s = (L^2 - L0^2) / (L0 (L + L0)).
-            dX = xj - xi; dY = yj - yi; dZ = zj - zi;
-            const double L2 = dX * dX + dY * dY + dZ * dZ;
-            const double diff = L2 - g.l0 * g.l0;
-            const float l0f = (float)g.l0;
-            Lf = sqrtf((float)L2);
-            sf = (float)diff / (l0f * (Lf + l0f));
-            // guard band: the stretch that decides breakage is recomputed in FP64
-            double crit = scb;
-            if (LAW == BBPD_LAW_LINEAR) crit = (bt == 1) ? 3 * scb : (bt == 2 ? P.sc_steel : scb);
-            exact = fabs((double)sf - crit) < d.guard;
-            if (exact) {
-                L = sqrt(L2);
-                s = (L - g.l0) / g.l0;
-            } else {
-                s = (double)sf;
-                L = (double)Lf;
-            }
-        }
-
-        // law and damage (calculatebsf*.m / calculatebondfailureMex.c)
-        const double B0 = (stv & ST_DAMAGED) ? bp[k * 32] : 0.0;
-        double B = B0;
-        bool soft = (stv & ST_SOFT) != 0;
-        double failv = (stv & ST_BROKEN) ? 0.0 : 1.0;
-        const bool concrete = (bt == 0);
-        if (LAW == BBPD_LAW_TRILINEAR) {
-            law_trilinear(s, s0b, s1b, scb, P, d.s0e != nullptr || d.s1e != nullptr, concrete, B, soft);
-        } else if (LAW == BBPD_LAW_BILINEAR) {
-            law_bilinear(s, s0b, scb, concrete, B, soft);
-        } else if (LAW == BBPD_LAW_EXPONENTIAL) {
-            law_exponential(s, s0b, scb, P, concrete, B, soft);
-        } else {
-            law_linear(s, scb, P, bt, failv);
-        }
-        const bool dmg = __double_as_longlong(B) != 0;
-        const uint8_t stn = (uint8_t)((soft ? ST_SOFT : 0) | (failv == 0.0 ? ST_BROKEN : 0) | (dmg ? ST_DAMAGED : 0));
-        if (stn != stv) stp[k * 32] = stn;
-        if (__double_as_longlong(B) != __double_as_longlong(B0)) bp[k * 32] = B;
-
-        // bond force (calculatebondforcesMex.c:34-40)
-        double fx, fy, fz;
-        if (PREC == BBPD_PREC_FP64 || exact) {
-            double t;
-            if (!(stn & (ST_BROKEN | ST_DAMAGED)))
-                t = ((g.bs * s) * d.V) * g.vcf;   // fail = 1, BSF = 0: same rounding as the full product
-            else
-                t = bond_force_scalar(failv, g.bs, B, s, 0.0, d.V, g.vcf);
-            if (isfinite(t) && L > 0 && L < INFINITY) {   // no NaN can arise
-                fx = t * (dX / L); fy = t * (dY / L); fz = t * (dZ / L);
-            } else {
-                fx = bond_force_component(t, dX, L);
-                fy = bond_force_component(t, dY, L);
-                fz = bond_force_component(t, dZ, L);
-            }
-        } else {
-            const float tf = (float)(failv * g.bs * (1 - B)) * sf * (float)(d.V * g.vcf);
-            const float r = tf / Lf;
-            float gx = r * (float)dX, gy = r * (float)dY, gz = r * (float)dZ;
-            if (gx != gx) gx = 0.f;
-            if (gy != gy) gy = 0.f;
-            if (gz != gz) gz = 0.f;
-            fx = (double)gx; fy = (double)gy; fz = (double)gz;
-        }
+    auto add = [&](uint32_t w, const double3 &f) {
         if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
             tx = tx + ax; ty = ty + ay; tz = tz + az;
             ax = 0.0; ay = 0.0; az = 0.0;
         }
-        ax = ax + fx; ay = ay + fy; az = az + fz;
+        ax = ax + f.x; ay = ay + f.y; az = az + f.z;
+    };
+    int k = 0;
+    for (; k + 1 < dg; k += 2) {
+        Fetch fa, fb;
+        fetch<CID>(d, cw, cd, stp, scp, x0, x1, x2, k * 32, fa);
+        fetch<CID>(d, cw, cd, stp, scp, x0, x1, x2, k * 32 + 32, fb);
+        const double3 ra = entry_force<LAW, PREC>(d, base + (int64_t)k * 32, fa, safe, xi, yi, zi);
+        const double3 rb = entry_force<LAW, PREC>(d, base + (int64_t)k * 32 + 32, fb, safe, xi, yi, zi);
+        add(fa.w, ra);
+        add(fb.w, rb);
+    }
+    if (k < dg) {
+        Fetch fa;
+        fetch<CID>(d, cw, cd, stp, scp, x0, x1, x2, k * 32, fa);
+        add(fa.w, entry_force<LAW, PREC>(d, base + (int64_t)k * 32, fa, safe, xi, yi, zi));
     }
     tx = tx + ax; ty = ty + ay; tz = tz + az;
+}
+
+// Coordinates for which the shared-divisor division of divide.cuh is exact:
+// 0, or a magnitude in [2^-100, 2^100].
+__device__ __forceinline__ bool coord_out_of_range(double x)
+{
+    const double a = fabs(x);
+    return a != 0 && !(a >= 0x1p-100 && a <= 0x1p100);
 }
 
 template <int LAW, int SCHEME, int PREC, class CID>
@@ -360,6 +469,8 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t nN = d.n_nodes;
+    // contiguous slice range of this warp, balanced by entry count on the host
+    const int64_t sl0 = d.wrange[gwarp], sl1 = d.wrange[gwarp + 1];
 
     for (int64_t it = 0; it < nsteps; it++) {
         const int64_t n = step0 + it;
@@ -368,19 +479,20 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
         const double *xs = ((n - 1) & 1) ? d.xb1 : d.xb0;
         double *xn = (n & 1) ? d.xb1 : d.xb0;
         const double Un1 = prescribed_value(d, n + 1);
+        const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
 
         // ---- phase A: bond forces (+ Euler-Cromer / ADR terms) ----
-        for (int64_t sl = gwarp; sl < d.n_slices; sl += nwarps) {
+        for (int64_t sl = sl0; sl < sl1; sl++) {
             const int64_t i = sl * 32 + lane;
             const bool valid = i < nN;
             double tx, ty, tz;
-            slice_forces<LAW, PREC, CID>(d, sl, lane, xs, tx, ty, tz);
+            slice_forces<LAW, PREC, CID>(d, sl, lane, safe, xs, tx, ty, tz);
             if (SCHEME == BBPD_SCHEME_EULERCROMER) {
                 if (valid) {
                     // timeintegrationeulercromerMex.c:33-50 on the node just summed
                     const uint8_t fl = d.nflag[i];
                     const double Fv[3] = {tx, ty, tz};
-                    bool bad = false;
+                    bool bad = false, far = false;
 #pragma unroll
                     for (int dof = 0; dof < 3; dof++) {
                         const int64_t e = i + nN * dof;
@@ -394,8 +506,10 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
                         if (d.a) d.a[e] = ae;
                         d.v[e] = ve; d.u[e] = ue; xn[e] = xe;
                         bad |= !isfinite(ue) || !isfinite(ve);
+                        far |= coord_out_of_range(xe);
                     }
                     if (bad) atomicOr(d.err, ERR_NONFINITE);
+                    if (far) atomicOr(d.sticky, 1u);
                 }
             } else {
                 // calculatedampingcoefficient.m:61-85 terms of this node, then the
@@ -447,12 +561,12 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
             if (!grid_barrier(d, true)) return;
             // ---- phase B: timeintegrationADR.m:168-197 ----
             const double cn = __ldcg(&d.scal[0]);
-            for (int64_t sl = gwarp; sl < d.n_slices; sl += nwarps) {
+            for (int64_t sl = sl0; sl < sl1; sl++) {
                 const int64_t i = sl * 32 + lane;
                 if (i >= nN) continue;
                 const uint8_t fl = d.nflag[i];
                 const double minv = 1.0 / d.mass[i];
-                bool bad = false;
+                bool bad = false, far = false;
 #pragma unroll
                 for (int dof = 0; dof < 3; dof++) {
                     const int64_t e = i + nN * dof;
@@ -463,10 +577,13 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
                     double ue = d.u[e] + (d.dt * vh);
                     if (fl & (1 << dof)) { ue = 0; vh = 0; }
                     if (fl & (8 << dof)) { ue = Un1; vh = 0; }
-                    d.v[e] = vh; d.u[e] = ue; xn[e] = d.X[e] + ue;
+                    const double xe = d.X[e] + ue;
+                    d.v[e] = vh; d.u[e] = ue; xn[e] = xe;
                     bad |= !isfinite(ue) || !isfinite(vh);
+                    far |= coord_out_of_range(xe);
                 }
                 if (bad) atomicOr(d.err, ERR_NONFINITE);
+                if (far) atomicOr(d.sticky, 1u);
             }
         }
         if (!grid_barrier(d, false)) return;
@@ -580,6 +697,28 @@ struct Key3Hash {
         return (size_t)(h ^ (h >> 29));
     }
 };
+
+DictEntry make_entry(double l0, double vcf, double bs, double V)
+{
+    DictEntry e;
+    e.l0 = l0;
+    e.rl0 = 1.0 / l0;                 // IEEE division: RN(1/L0)
+    e.vcf = vcf;
+    e.bs = bs;
+    e.k32 = (float)(bs * V * vcf);
+    const bool regular = std::isfinite(vcf) && std::isfinite(bs) && l0 >= 0x1p-100 && l0 <= 0x1p100;
+    e.flags = regular ? 0u : 1u;
+    e.pad = 0;
+    return e;
+}
+
+// Coordinates for which the shared-divisor division is exact: 0, or a
+// magnitude in [2^-100, 2^100].
+inline bool coord_safe(double x)
+{
+    const double a = std::fabs(x);
+    return a == 0 || (a >= 0x1p-100 && a <= 0x1p100);
+}
 
 inline uint64_t bits_of(double x)
 {
@@ -770,18 +909,18 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
                 std::memcpy(&l0, &keys[q].a, 8);
                 std::memcpy(&vcf, &keys[q].b, 8);
                 std::memcpy(&bs, &keys[q].c, 8);
-                dict[q] = DictEntry{l0, vcf, bs, 0.0};
+                dict[q] = make_entry(l0, vcf, bs, prm->cell_volume);
             }
         } else {
             // irregular input: one dictionary entry per bond, 32-bit ids
             S->wide = true;
             dict.resize(nB);
             for (int64_t k = 0; k < nB; k++) {
-                dict[k] = DictEntry{pb->undeformed_length[k], pb->volume_correction[k], pb->bond_stiffness[k], 0.0};
+                dict[k] = make_entry(pb->undeformed_length[k], pb->volume_correction[k], pb->bond_stiffness[k], prm->cell_volume);
                 bond_cid[k] = (uint32_t)k;
             }
         }
-        if (dict.empty()) dict.push_back(DictEntry{1.0, 0.0, 0.0, 0.0});
+        if (dict.empty()) dict.push_back(make_entry(1.0, 0.0, 0.0, prm->cell_volume));
         S->ndict = (int64_t)dict.size();
     }
 
@@ -943,6 +1082,10 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     TRY(S->put(&d.bar, bar));
     std::vector<int> err(1, 0);
     TRY(S->put(&d.err, err));
+    std::vector<unsigned> sticky(1, 0u);
+    for (int64_t e = 0; e < 3 * nN; e++)
+        if (!coord_safe(x0[e])) sticky[0] = 1u;
+    TRY(S->put(&d.sticky, sticky));
 
     // scalars
     LawScalars &P = d.P;
@@ -977,6 +1120,23 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     if (occ < 1) return fail(BBPD_ERR_CUDA, "kernel cannot be resident");
     int64_t want = (ns * 32 + kBlock - 1) / kBlock;   // one warp per slice at most
     S->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * occ, want));
+    {
+        // contiguous slice ranges per warp with equal work: a slice costs its
+        // longest list (the warp's trip count) plus a few trips of node work
+        const int64_t nw = (int64_t)S->grid * (kBlock / 32);
+        std::vector<double> pre(ns + 1, 0.0);
+        for (int64_t s = 0; s < ns; s++) pre[s + 1] = pre[s] + (double)slen[s] + 4.0;
+        std::vector<int64_t> wr(nw + 1, 0);
+        int64_t s = 0;
+        for (int64_t w = 1; w < nw; w++) {
+            const double target = pre[ns] * (double)w / (double)nw;
+            while (s < ns && pre[s + 1] <= target) s++;
+            if (s < ns && target - pre[s] > pre[s + 1] - target) s++;  // nearer boundary
+            wr[w] = std::max(s, wr[w - 1]);
+        }
+        wr[nw] = ns;
+        TRY(S->put((int64_t **)&d.wrange, wr));
+    }
     BBPD_CUDA_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
     BBPD_CUDA_TRY(cudaEventCreate(&S->ev0));
     BBPD_CUDA_TRY(cudaEventCreate(&S->ev1));
@@ -1126,6 +1286,12 @@ extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
         if (field == BBPD_FIELD_DEFORMED) {
             // both position buffers: the next step reads the one of its parity
             BBPD_CUDA_TRY(cudaMemcpy(dst == S->d.xb0 ? S->d.xb1 : S->d.xb0, h.data(), sizeof(double) * 3 * nN, cudaMemcpyHostToDevice));
+            bool far = false;
+            for (double x : h) far |= !coord_safe(x);
+            if (far) {   // sticky: from now on the kernels divide with IEEE division
+                const unsigned one = 1u;
+                BBPD_CUDA_TRY(cudaMemcpy(S->d.sticky, &one, sizeof(unsigned), cudaMemcpyHostToDevice));
+            }
         }
         return BBPD_OK;
     }

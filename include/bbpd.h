@@ -293,6 +293,15 @@ int bbpd_last_kernel_ms(bbpd_solver *s, float *ms);
  * wait expires after timeout_s and the kernel returns (the expected outcome). */
 int bbpd_selftest_wait_timeout(double timeout_s);
 
+/* Diagnostic: compares the kernels' correctly rounded division by a shared
+ * divisor (Markstein's reciprocal and quotient corrections) with IEEE double
+ * division on n seeded samples on the device; reports the mismatches of the
+ * reciprocal and of the quotients, the samples compared, and the largest
+ * relative error of the hardware reciprocal approximation. */
+int bbpd_selftest_division(int64_t n, uint64_t seed, int64_t *recip_mismatches,
+                           int64_t *quot_mismatches, int64_t *samples,
+                           double *rcp_approx_max_relerr);
+
 /* ===================================================================== *
  *  Synthetic beam builder (the inputs of input/scripts/Gregoire_beam_    *
  *  tests.m and the functions it calls, for a regular lattice).          *

@@ -188,3 +188,16 @@ def test_wait_timeout_selftest():
     rc = bb._native.lib().bbpd_selftest_wait_timeout(0.2)
     assert rc == bb._native.ERR_TIMEOUT
     assert time.time() - t < 10
+
+
+def test_division_selftest():
+    """The kernels' division by a shared divisor (Markstein) equals IEEE
+    division bit for bit on 2e8 seeded samples, hard rounding cases included."""
+    import ctypes as C
+    rb, qb, n = C.c_int64(), C.c_int64(), C.c_int64()
+    err = C.c_double()
+    bb._native.check(bb._native.lib().bbpd_selftest_division(200_000_000, 20261203, C.byref(rb), C.byref(qb),
+                                                              C.byref(n), C.byref(err)))
+    print(f"samples {n.value}, rcp.approx max rel err {err.value:.3e}")
+    assert n.value > 150_000_000
+    assert rb.value == 0 and qb.value == 0, (rb.value, qb.value)
