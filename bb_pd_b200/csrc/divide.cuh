@@ -12,9 +12,9 @@
 //                 fused multiply-add), q = RN(q0 + r y) = RN(a / b).
 //
 // Preconditions (no underflow or overflow in any step): b and a / b normal and
-// well inside the exponent range. The kernels use these only when every
-// coordinate is 0 or of magnitude in [2^-100, 2^100] and L0 lies in the same
-// range; outside it they fall back to IEEE division. bbpd_selftest_division
+// well inside the exponent range, a not -0. The kernels use these only when
+// every coordinate is +0 or of magnitude in [2^-100, 2^100] and L0 lies in the
+// same range; outside it they fall back to IEEE division. bbpd_selftest_division
 // compares both against IEEE `/` bit for bit on the device.
 #pragma once
 
@@ -27,8 +27,9 @@ __device__ __forceinline__ double rcp_approx(double b)
     return y;
 }
 
-// RN(1/b) for normal positive b in [2^-200, 2^200]; *ok = false when the
-// significand of b is all ones (the one case the final step does not cover).
+// RN(1/b) for normal positive b in [2^-200, 2^200]; ok = false when the low
+// 32 bits of the significand are all ones, which includes the all-ones
+// significand (the one case the final step does not cover).
 __device__ __forceinline__ double recip_rn(double b, bool &ok)
 {
     double y = rcp_approx(b);
@@ -38,16 +39,17 @@ __device__ __forceinline__ double recip_rn(double b, bool &ok)
     y = __fma_rn(y, e, y);
     e = __fma_rn(-b, y, 1.0);
     y = __fma_rn(y, e, y);
-    ok = (__double2loint(b) != -1) || ((__double2hiint(b) & 0x000FFFFF) != 0x000FFFFF);
+    ok = __double2loint(b) != -1;
     return y;
 }
 
-// RN(a / b) given y = RN(1/b), for a = 0 or |a / b| normal (see preconditions).
+// RN(a / b) given y = RN(1/b), for a = +0 or |a / b| normal (see
+// preconditions). An exact q0 leaves r = +0 and q0 unchanged.
 __device__ __forceinline__ double quot_rn(double a, double b, double y)
 {
     const double q0 = __dmul_rn(a, y);
     const double r = __fma_rn(-q0, b, a);
-    return (r == 0.0) ? q0 : __fma_rn(r, y, q0);
+    return __fma_rn(r, y, q0);
 }
 
 }  // namespace bbpd

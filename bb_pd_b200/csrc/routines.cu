@@ -210,31 +210,38 @@ __global__ void k_damping_slices(const double *__restrict__ F, const double *__r
     }
 }
 
-// 1024 strands then an xor-butterfly over them, one block of 1024 threads;
-// then the clamp of calculatedampingcoefficient.m:90-112.
-__global__ void __launch_bounds__(1024) k_damping_final(const double *part, int64_t nsl, double *cn_out)
+// Upper levels of the 32-ary tree over the slice partials (groups of 32
+// consecutive partials, xor butterfly, missing members 0.0) until one value is
+// left; one block of 1024 threads, ping-pong buffers a/b of ceil(nsl/32) each.
+// Then the clamp of calculatedampingcoefficient.m:90-112.
+__global__ void __launch_bounds__(1024) k_damping_final(const double *part, int64_t nsl, double *a,
+                                                        double *b, double *cn_out)
 {
-    __shared__ double a1[1024], a2[1024];
-    int r = threadIdx.x;
-    double c1 = 0.0, c2 = 0.0;
-    for (int64_t k = r; k < nsl; k += 1024) {
-        c1 = c1 + part[k];
-        c2 = c2 + part[nsl + k];
-    }
-    a1[r] = c1; a2[r] = c2;
-    __syncthreads();
-    for (int off = 512; off >= 32; off >>= 1) {
-        double n1 = a1[r] + a1[r ^ off], n2 = a2[r] + a2[r ^ off];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double *src = part;
+    int64_t cnt = nsl;
+    double *dst = a;
+    // src holds cnt pairs as [cnt1 ..., cnt2 ...] with stride `sstride`
+    int64_t sstride = nsl;
+    while (cnt > 1) {
+        const int64_t m = (cnt + 31) / 32;
+        for (int64_t g = warp; g < m; g += 32) {
+            const int64_t idx = g * 32 + lane;
+            double c1 = idx < cnt ? src[idx] : 0.0, c2 = idx < cnt ? src[sstride + idx] : 0.0;
+            for (int off = 16; off >= 1; off >>= 1) {
+                c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
+                c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
+            }
+            if (lane == 0) { dst[g] = c1; dst[m + g] = c2; }
+        }
         __syncthreads();
-        a1[r] = n1; a2[r] = n2;
-        __syncthreads();
+        src = dst;
+        sstride = m;
+        cnt = m;
+        dst = (dst == a) ? b : a;
     }
-    c1 = a1[r]; c2 = a2[r];
-    for (int off = 16; off >= 1; off >>= 1) {
-        c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
-        c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
-    }
-    if (r == 0) {
+    if (threadIdx.x == 0) {
+        const double c1 = nsl > 0 ? src[0] : 0.0, c2 = nsl > 0 ? src[sstride] : 0.0;
         double cn;
         if (c2 != 0) {
             if ((c1 / c2) > 0) cn = 2 * sqrt(c1 / c2);
@@ -429,15 +436,17 @@ extern "C" int bbpd_dev_calculatedampingcoefficient(const double *F, const doubl
     if (rc) return rc;
     cudaStream_t st = as_stream(stream);
     int64_t nsl = (nN + 31) / 32;
-    double *scratch = nullptr;   // 2 * nsl slice partials + 1 result
-    BBPD_CUDA_TRY(cudaMallocAsync(&scratch, sizeof(double) * (size_t)(2 * nsl + 1), st));
+    const int64_t lv = 2 * ((nsl + 31) / 32) + 2;   // one level of the tree, both sums
+    double *scratch = nullptr;   // 2 * nsl slice partials, 2 level buffers, 1 result
+    BBPD_CUDA_TRY(cudaMallocAsync(&scratch, sizeof(double) * (size_t)(2 * nsl + 2 * lv + 1), st));
+    double *res = scratch + 2 * nsl + 2 * lv;
     if (nsl > 0)
         k_damping_slices<<<blocks_for(nsl * 32), kThreads, 0, st>>>(F, m, Fp, dt, vhp, u, nN, nsl, scratch);
-    k_damping_final<<<1, 1024, 0, st>>>(scratch, nsl, scratch + 2 * nsl);
+    k_damping_final<<<1, 1024, 0, st>>>(scratch, nsl, scratch + 2 * nsl, scratch + 2 * nsl + lv, res);
     rc = launch_check();
     double h = 0;
     if (rc == BBPD_OK) {
-        cudaError_t e = cudaMemcpyAsync(&h, scratch + 2 * nsl, sizeof(double), cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = fail(BBPD_ERR_CUDA, "damping coefficient: %s", cudaGetErrorString(e));
     }

@@ -61,7 +61,7 @@ __global__ void division_selftest_kernel(int64_t n, uint64_t seed, Counts *c)
             const double ulp = make_double(0, ((int)((__double_as_longlong(q) >> 52) & 0x7FF) - 1023) - 52);
             a = __fma_rn(q, b, (0.5 * ulp) * b);   // RN((q + ulp/2) b): a / b sits next to a midpoint
         }
-        if ((h4 >> 63) & 1) a = -a;
+        if (((h4 >> 63) & 1) && a != 0.0) a = -a;   // -0 is outside the precondition
         const double q = quot_rn(a, b, y);
         if (__double_as_longlong(q) != __double_as_longlong(a / b)) qb++;
     }

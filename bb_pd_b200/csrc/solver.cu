@@ -28,10 +28,10 @@
 //            Euler-Cromer integrates the node right there (positions
 //            double-buffered); ADR writes the node's Rayleigh-quotient terms
 //            reduced over the warp (one partial per slice).
-//   ADR      barrier; warps reduce the slice partials into 1024 strands in a
-//            fixed order; barrier, the last block to arrive folds the strands
-//            (xor butterfly) into the damping coefficient cn; phase B applies
-//            the central-difference half-step update; barrier.
+//   ADR      the slice partials enter a fixed 32-ary tree whose groups are
+//            folded by the warp that completes them, the root giving the
+//            damping coefficient cn; barrier; phase B applies the central-
+//            difference half-step update; barrier.
 // Grid barriers spin with a time limit; on expiry they set an error flag and
 // the kernel returns early (status BBPD_ERR_TIMEOUT), never hanging.
 #include "bbpd_internal.h"
@@ -66,28 +66,36 @@ constexpr int kBlock = 256;
 #ifndef BBPD_MIN_BLOCKS
 #define BBPD_MIN_BLOCKS 3
 #endif
-constexpr int kStrands = 1024;
+constexpr int kMaxLevels = 8;     // 32-ary reduction tree over the slices
 
-// One dictionary entry: the bond constants in FP64, RN(1/L0) for the shared-
-// divisor division, the FP32 product BONDSTIFFNESS * cellVolume * VCF for the
-// FP32 form, and flags (bit 0: a constant is not finite or L0 lies outside
-// [2^-100, 2^100]; entries using it take the general path).
+// Entry k of the list of lane `lane` in the slice whose entries start at sbase:
+// each lane's entries come in groups of 4 contiguous slots, lanes interleaved
+// group by group, so a lane reads 4 entries of a stream with one vector load
+// and a warp reads 32 such groups contiguously.
+__host__ __device__ __forceinline__ int64_t entry_pos(int64_t sbase, int64_t k, int lane)
+{
+    return sbase + ((k >> 2) * 32 + lane) * 4 + (k & 3);
+}
+
+// One dictionary entry: the bond constants in FP64 and RN(1/L0) for the
+// shared-divisor division. rl0 is set to -1 when a constant is not finite or
+// L0 lies outside [2^-100, 2^100]: entries using it take the general path. A
+// parallel float table holds BONDSTIFFNESS * cellVolume * VCF for the FP32 form.
 struct DictEntry {
     double l0, rl0, vcf, bs;
-    float k32;
-    uint32_t flags;
-    double pad;
 };
 
 struct Dev {
     int64_t n_nodes, n_slices;
     const int64_t *slice_ptr;
     const int32_t *deg;
+    const int32_t *slice_len;        // longest list of each slice
     const uint32_t *colw;
     const void *cid;
     uint8_t *st;
     double *bsf;
     const DictEntry *dict;
+    const float *dict32;             // BONDSTIFFNESS * cellVolume * VCF per dictionary entry (FP32 form)
     const double *s0e, *s1e, *sce;   // per-entry law stretches or null
     const double *X;
     double *xb0, *xb1;               // positions: step n reads xb[(n-1)&1], writes xb[n&1]
@@ -95,8 +103,12 @@ struct Dev {
     double *F0, *F1;                 // F of step n lives in F[n&1]
     const double *mass, *rho;
     const uint8_t *nflag;            // bit d: held (constrained or prescribed); bit 3+d: prescribed
-    double *part;                    // 2 * n_slices slice partials
-    double *strand;                  // 2 * kStrands strand sums
+    double2 *tree;                   // partial sums (cn1, cn2) of every tree level
+    unsigned *tcnt;                  // arrival counters of the groups of levels >= 2
+    int64_t lvl_cnt[kMaxLevels];     // values at level L (level 1: one per slice)
+    int64_t lvl_off[kMaxLevels];     // offset of level L in tree[]
+    int64_t cnt_off[kMaxLevels];     // offset in tcnt[] of the groups forming level L
+    int n_levels;
     double *scal;                    // [0] = cn
     unsigned *bar;                   // [0] arrivals, [1] generation
     unsigned *sticky;                // bit 0: a coordinate left the range of the fast division
@@ -147,51 +159,65 @@ __device__ bool bounded_wait_change(volatile unsigned *word, unsigned old, int *
     return true;
 }
 
-// Fold the 1024 strand sums (xor butterfly, offsets 512 ... 1) and apply the
-// clamp of calculatedampingcoefficient.m:90-112; run by one block.
-__device__ void fold_strands(const Dev &d)
+// Clamp of calculatedampingcoefficient.m:90-112 applied to the two sums.
+__device__ __forceinline__ double cn_from_sums(double cn1, double cn2)
 {
-    __shared__ double a1[kStrands], a2[kStrands];
-    for (int r = threadIdx.x; r < kStrands; r += blockDim.x) {
-        a1[r] = __ldcg(&d.strand[r]);
-        a2[r] = __ldcg(&d.strand[kStrands + r]);
+    double cn;
+    if (cn2 != 0) {
+        if ((cn1 / cn2) > 0) cn = 2 * sqrt(cn1 / cn2);
+        else cn = 0;
+    } else {
+        cn = 0;
     }
-    __syncthreads();
-    constexpr int PER = kStrands / kBlock;
-    for (int off = kStrands / 2; off >= 1; off >>= 1) {
-        double n1[PER], n2[PER];
-#pragma unroll
-        for (int q = 0; q < PER; q++) {
-            int r = threadIdx.x + q * kBlock;
-            n1[q] = a1[r] + a1[r ^ off];
-            n2[q] = a2[r] + a2[r ^ off];
+    if (cn > 2) cn = 1.9;
+    return cn;
+}
+
+// The Rayleigh-quotient sums of one slice enter the fixed 32-ary tree: the
+// warp stores its partial, and the warp that completes a group of 32 partials
+// (arrival counter, fence) folds the group with the xor butterfly and carries
+// the result one level up, until the root yields cn. The order of every
+// addition depends on slice indices only, never on timing or launch shape.
+__device__ void tree_publish(const Dev &d, int64_t sl, int lane, double c1, double c2)
+{
+    int L = 1;
+    int64_t idx = sl;
+    for (;;) {
+        if (lane == 0) d.tree[d.lvl_off[L] + idx] = make_double2(c1, c2);
+        const int64_t cnt = d.lvl_cnt[L];
+        if (cnt == 1) {   // root
+            if (lane == 0) {
+                d.scal[0] = cn_from_sums(c1, c2);
+                d.scal[1] = c1;
+                d.scal[2] = c2;
+            }
+            return;
         }
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < PER; q++) {
-            int r = threadIdx.x + q * kBlock;
-            a1[r] = n1[q];
-            a2[r] = n2[q];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        double cn1 = a1[0], cn2 = a2[0], cn;
-        if (cn2 != 0) {
-            if ((cn1 / cn2) > 0) cn = 2 * sqrt(cn1 / cn2);
-            else cn = 0;
-        } else {
-            cn = 0;
-        }
-        if (cn > 2) cn = 1.9;
-        d.scal[0] = cn;
+        const int64_t g = idx >> 5;
+        const int gsize = (int)min((int64_t)32, cnt - g * 32);
         __threadfence();
+        unsigned old = 0;
+        if (lane == 0) old = atomicAdd(&d.tcnt[d.cnt_off[L + 1] + g], 1u);
+        old = __shfl_sync(0xffffffffu, old, 0);
+        if ((int)old != gsize - 1) return;   // another warp completes this group
+        if (lane == 0) d.tcnt[d.cnt_off[L + 1] + g] = 0u;
+        __threadfence();
+        double2 v = make_double2(0.0, 0.0);
+        if (lane < gsize) v = __ldcg(&d.tree[d.lvl_off[L] + g * 32 + lane]);
+        c1 = v.x;
+        c2 = v.y;
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
+            c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
+        }
+        L++;
+        idx = g;
     }
 }
 
-// Grid-wide barrier with a time limit. The last block to arrive optionally
-// folds the strands into cn before releasing the others. False on timeout.
-__device__ bool grid_barrier(const Dev &d, bool do_cn)
+// Grid-wide barrier with a time limit. False on timeout.
+__device__ bool grid_barrier(const Dev &d)
 {
     __shared__ int s_last, s_ok;
     __syncthreads();
@@ -206,8 +232,6 @@ __device__ bool grid_barrier(const Dev &d, bool do_cn)
     }
     __syncthreads();
     if (s_last) {
-        if (do_cn) fold_strands(d);
-        __syncthreads();
         if (threadIdx.x == 0) {
             d.bar[0] = 0;
             __threadfence();
@@ -222,42 +246,63 @@ __device__ bool grid_barrier(const Dev &d, bool do_cn)
 __device__ __forceinline__ DictEntry ldg_dict(const DictEntry *t, uint32_t c)
 {
     const double2 *p = reinterpret_cast<const double2 *>(t + c);
-    const double2 a = __ldg(p), b = __ldg(p + 1), m = __ldg(p + 2);
+    const double2 a = __ldg(p), b = __ldg(p + 1);
     DictEntry e;
     e.l0 = a.x;
     e.rl0 = a.y;
     e.vcf = b.x;
     e.bs = b.y;
-    e.k32 = __int_as_float(__double2loint(m.x));
-    e.flags = (uint32_t)__double2hiint(m.x);
-    e.pad = 0;
     return e;
 }
 
-// Per-entry data, fetched before the arithmetic of the entry.
+// Per-entry data, fetched before the arithmetic of the entry. sc is the
+// per-entry critical stretch when the law takes one (SCE), else the scalar.
 struct Fetch {
     uint32_t w;
     uint32_t sv;
+    uint32_t c;
     double xj, yj, zj, sc;
     DictEntry g;
 };
 
+// The streams of one group of 4 entries of one lane.
+template <class CID> struct Group;
+template <> struct Group<uint16_t> {
+    uint4 w;
+    uint2 c;
+    uint32_t s;
+    __device__ __forceinline__ uint32_t cid(int q) const
+    {
+        const uint32_t h = (q < 2) ? c.x : c.y;
+        return (q & 1) ? (h >> 16) : (h & 0xFFFFu);
+    }
+};
+template <> struct Group<uint32_t> {
+    uint4 w;
+    uint4 c;
+    uint32_t s;
+    __device__ __forceinline__ uint32_t cid(int q) const
+    {
+        return q == 0 ? c.x : q == 1 ? c.y : q == 2 ? c.z : c.w;
+    }
+};
+
 template <class CID>
-__device__ __forceinline__ void fetch(const Dev &d, const uint32_t *__restrict__ cw,
-                                      const CID *__restrict__ cd, const uint8_t *stp,
-                                      const double *__restrict__ scp,
-                                      const double *x0, const double *x1, const double *x2,
-                                      int o, Fetch &f)
+__device__ __forceinline__ uint32_t group_w(const Group<CID> &G, int q)
 {
-    f.w = __ldg(cw + o);
-    const uint32_t c = __ldg(cd + o);
-    f.sv = stp[o];
-    f.sc = scp ? __ldg(scp + o) : d.P.sc;
-    const uint32_t j = f.w & COL_MASK;
-    f.xj = x0[j];
-    f.yj = x1[j];
-    f.zj = x2[j];
-    f.g = ldg_dict(d.dict, c);
+    return q == 0 ? G.w.x : q == 1 ? G.w.y : q == 2 ? G.w.z : G.w.w;
+}
+
+// Streams are read once per step: evict-first, so the node arrays keep L2.
+template <class CID>
+__device__ __forceinline__ void load_group(const Dev &d, int64_t e0, Group<CID> &G)
+{
+    G.w = __ldcs(reinterpret_cast<const uint4 *>(d.colw + e0));
+    if constexpr (sizeof(CID) == 2)
+        G.c = __ldcs(reinterpret_cast<const uint2 *>(reinterpret_cast<const uint16_t *>(d.cid) + e0));
+    else
+        G.c = __ldcs(reinterpret_cast<const uint4 *>(reinterpret_cast<const uint32_t *>(d.cid) + e0));
+    G.s = __ldcs(reinterpret_cast<const uint32_t *>(d.st + e0));
 }
 
 // Critical stretch whose crossing breaks a bond under the brittle law
@@ -357,7 +402,7 @@ __device__ BBPD_GENERAL_ATTR double3 entry_general(const Dev &d, int64_t e, uint
 // Force of one entry. The common case, an intact and undamaged bond whose law
 // stays quiet, is computed inline: with fail = 1 and BSF = 0 the reference
 // product fail*BS*(1-BSF)*s*V*VCF rounds exactly like ((BS*s)*V)*VCF, and with
-// 0 < L < inf and a regular dictionary entry no NaN can arise.
+// 0 < L < inf and a regular dictionary entry (rl0 > 0) no NaN can arise.
 template <int LAW, int PREC>
 __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fetch &f, bool safe,
                                                double xi, double yi, double zi)
@@ -366,16 +411,16 @@ __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fe
     const double s0b = d.s0e ? __ldg(d.s0e + e) : d.P.s0;
     double3 r;
     if (PREC == BBPD_PREC_FP64) {
-        // calculatedeformedlengthMex.c:37-43 with its two divisions by L0 and
-        // the three of calculatebondforcesMex.c:34-36 by L done as
-        // correctly rounded quotients with shared reciprocals (divide.cuh):
-        // bit-identical to IEEE division whenever `safe` holds.
+        // calculatedeformedlengthMex.c:37-43 with its division by L0 and the
+        // three of calculatebondforcesMex.c:34-36 by L done as correctly
+        // rounded quotients with shared reciprocals (divide.cuh): bit-identical
+        // to IEEE division whenever `safe` holds.
         const double dX = f.xj - xi, dY = f.yj - yi, dZ = f.zj - zi;
         const double L = sqrt(dX * dX + dY * dY + dZ * dZ);
         const double s = quot_rn(L - f.g.l0, f.g.l0, f.g.rl0);
         bool okr;
         const double rL = recip_rn(L, okr);
-        if (safe && okr && f.sv == 0 && f.g.flags == 0 && L > 0 &&
+        if (safe && okr && f.sv == 0 && f.g.rl0 > 0 && L > 0 &&
             law_quiet<LAW>(d.P, bt, s, s0b, f.sc)) {
             const double t = ((f.g.bs * s) * d.V) * f.g.vcf;
             r.x = t * quot_rn(dX, L, rL);
@@ -395,9 +440,9 @@ __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fe
         const float sf = __fdividef((float)diff, l0f * (Lf + l0f));
         const double crit = (LAW == BBPD_LAW_LINEAR) ? linear_crit(d.P, bt, f.sc) : f.sc;
         // guard band: near the critical stretch the general path decides in FP64
-        if (f.sv == 0 && f.g.flags == 0 && L2f > 0.f && L2f < INFINITY &&
+        if (f.sv == 0 && f.g.rl0 > 0 && L2f > 0.f && L2f < INFINITY &&
             !(fabs((double)sf - crit) < d.guard) && law_quiet<LAW>(d.P, bt, (double)sf, s0b, f.sc)) {
-            const float q = f.g.k32 * sf * ri;
+            const float q = __ldg(&d.dict32[f.c]) * sf * ri;
             r.x = (double)(q * (float)dX);
             r.y = (double)(q * (float)dY);
             r.z = (double)(q * (float)dZ);
@@ -408,9 +453,11 @@ __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fe
 }
 
 // Forces of the 32 nodes of one slice. Lane `lane` owns node sl*32+lane and
-// walks its entries in bond order, two entries fetched per round; returns the
-// node's force summed in the reference's order.
-template <int LAW, int PREC, class CID>
+// walks its entries in bond order, a group of 4 at a time: the next group's
+// streams load while the current group's 12 coordinate gathers are issued
+// together and its entries computed. Returns the node's force summed in the
+// reference's order.
+template <int LAW, int PREC, class CID, bool SCE>
 __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane, bool safe,
                                              const double *xs, double &tx, double &ty,
                                              double &tz)
@@ -418,56 +465,74 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
     const int64_t nN = d.n_nodes;
     const int64_t i = sl * 32 + lane;
     const int dg = (i < nN) ? d.deg[i] : 0;
-    const int64_t base = d.slice_ptr[sl] + lane;
-    const uint32_t *__restrict__ cw = d.colw + base;
-    const CID *__restrict__ cd = reinterpret_cast<const CID *>(d.cid) + base;
-    const uint8_t *stp = d.st + base;
-    const double *__restrict__ scp = d.sce ? d.sce + base : nullptr;
+    const int64_t sb = d.slice_ptr[sl];
     const double *x0 = xs, *x1 = xs + nN, *x2 = xs + 2 * nN;
 
     double xi = 0, yi = 0, zi = 0;
     if (i < nN) { xi = x0[i]; yi = x1[i]; zi = x2[i]; }
     tx = 0.0; ty = 0.0; tz = 0.0;
     double ax = 0.0, ay = 0.0, az = 0.0;
-    auto add = [&](uint32_t w, const double3 &f) {
-        if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
-            tx = tx + ax; ty = ty + ay; tz = tz + az;
-            ax = 0.0; ay = 0.0; az = 0.0;
-        }
-        ax = ax + f.x; ay = ay + f.y; az = az + f.z;
-    };
-    int k = 0;
-    for (; k + 1 < dg; k += 2) {
-        Fetch fa, fb;
-        fetch<CID>(d, cw, cd, stp, scp, x0, x1, x2, k * 32, fa);
-        fetch<CID>(d, cw, cd, stp, scp, x0, x1, x2, k * 32 + 32, fb);
-        const double3 ra = entry_force<LAW, PREC>(d, base + (int64_t)k * 32, fa, safe, xi, yi, zi);
-        const double3 rb = entry_force<LAW, PREC>(d, base + (int64_t)k * 32 + 32, fb, safe, xi, yi, zi);
-        add(fa.w, ra);
-        add(fb.w, rb);
+
+    const int ng = (dg + 3) >> 2;
+    Group<CID> Gc, Gn;
+    double2 sca = make_double2(0, 0), scb = make_double2(0, 0), sna = sca, snb = sca;
+    int64_t e0 = entry_pos(sb, 0, lane);
+    if (ng > 0) {
+        load_group<CID>(d, e0, Gc);
+        if (SCE) { sca = __ldcs(reinterpret_cast<const double2 *>(d.sce + e0)); scb = __ldcs(reinterpret_cast<const double2 *>(d.sce + e0) + 1); }
     }
-    if (k < dg) {
-        Fetch fa;
-        fetch<CID>(d, cw, cd, stp, scp, x0, x1, x2, k * 32, fa);
-        add(fa.w, entry_force<LAW, PREC>(d, base + (int64_t)k * 32, fa, safe, xi, yi, zi));
+    for (int g = 0; g < ng; g++, e0 += 128) {
+        if (g + 1 < ng) {
+            load_group<CID>(d, e0 + 128, Gn);
+            if (SCE) { sna = __ldcs(reinterpret_cast<const double2 *>(d.sce + e0 + 128)); snb = __ldcs(reinterpret_cast<const double2 *>(d.sce + e0 + 128) + 1); }
+        }
+        const int nq = min(4, dg - 4 * g);
+        double xj[4], yj[4], zj[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (q < nq) {
+                const uint32_t j = group_w(Gc, q) & COL_MASK;
+                xj[q] = x0[j]; yj[q] = x1[j]; zj[q] = x2[j];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (q < nq) {
+                Fetch f;
+                f.w = group_w(Gc, q);
+                f.c = Gc.cid(q);
+                f.sv = (Gc.s >> (8 * q)) & 0xFFu;
+                f.sc = SCE ? (q == 0 ? sca.x : q == 1 ? sca.y : q == 2 ? scb.x : scb.y) : d.P.sc;
+                f.xj = xj[q]; f.yj = yj[q]; f.zj = zj[q];
+                f.g = ldg_dict(d.dict, f.c);
+                const double3 r = entry_force<LAW, PREC>(d, e0 + q, f, safe, xi, yi, zi);
+                if (f.w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
+                    tx = tx + ax; ty = ty + ay; tz = tz + az;
+                    ax = 0.0; ay = 0.0; az = 0.0;
+                }
+                ax = ax + r.x; ay = ay + r.y; az = az + r.z;
+            }
+        }
+        Gc = Gn;
+        if (SCE) { sca = sna; scb = snb; }
     }
     tx = tx + ax; ty = ty + ay; tz = tz + az;
 }
 
 // Coordinates for which the shared-divisor division of divide.cuh is exact:
-// 0, or a magnitude in [2^-100, 2^100].
+// +0, or a magnitude in [2^-100, 2^100] (a -0 coordinate could make a -0
+// numerator, whose quotient sign the fast division does not track).
 __device__ __forceinline__ bool coord_out_of_range(double x)
 {
     const double a = fabs(x);
-    return a != 0 && !(a >= 0x1p-100 && a <= 0x1p100);
+    return (a != 0 || signbit(x)) && !(a >= 0x1p-100 && a <= 0x1p100);
 }
 
-template <int LAW, int SCHEME, int PREC, class CID>
+template <int LAW, int SCHEME, int PREC, class CID, bool SCE>
 __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, int64_t step0, int64_t nsteps)
 {
     const int lane = threadIdx.x & 31;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t nN = d.n_nodes;
     // contiguous slice range of this warp, balanced by entry count on the host
     const int64_t sl0 = d.wrange[gwarp], sl1 = d.wrange[gwarp + 1];
@@ -486,7 +551,7 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
             const int64_t i = sl * 32 + lane;
             const bool valid = i < nN;
             double tx, ty, tz;
-            slice_forces<LAW, PREC, CID>(d, sl, lane, safe, xs, tx, ty, tz);
+            slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, xs, tx, ty, tz);
             if (SCHEME == BBPD_SCHEME_EULERCROMER) {
                 if (valid) {
                     // timeintegrationeulercromerMex.c:33-50 on the node just summed
@@ -536,29 +601,11 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
                     c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
                     c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
                 }
-                if (lane == 0) { d.part[sl] = c1; d.part[d.n_slices + sl] = c2; }
+                tree_publish(d, sl, lane, c1, c2);
             }
         }
         if (SCHEME == BBPD_SCHEME_ADR) {
-            if (!grid_barrier(d, false)) return;
-            // strands: strand r sums slices r, r+1024, ... in order, from 0.0
-            const int64_t ns = d.n_slices;
-            for (int64_t r = gwarp; r < kStrands; r += nwarps) {
-                double acc1 = 0.0, acc2 = 0.0;
-                for (int64_t b0 = r; b0 < ns; b0 += (int64_t)kStrands * 32) {
-                    const int64_t idx = b0 + (int64_t)lane * kStrands;
-                    const double p1 = idx < ns ? __ldcg(&d.part[idx]) : 0.0;
-                    const double p2 = idx < ns ? __ldcg(&d.part[ns + idx]) : 0.0;
-                    const int64_t left = (ns - b0 + kStrands - 1) / kStrands;
-                    const int cnt = left < 32 ? (int)left : 32;
-                    for (int q = 0; q < cnt; q++) {
-                        acc1 = acc1 + __shfl_sync(0xffffffffu, p1, q);
-                        acc2 = acc2 + __shfl_sync(0xffffffffu, p2, q);
-                    }
-                }
-                if (lane == 0) { d.strand[r] = acc1; d.strand[kStrands + r] = acc2; }
-            }
-            if (!grid_barrier(d, true)) return;
+            if (!grid_barrier(d)) return;
             // ---- phase B: timeintegrationADR.m:168-197 ----
             const double cn = __ldcg(&d.scal[0]);
             for (int64_t sl = sl0; sl < sl1; sl++) {
@@ -586,7 +633,7 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
                 if (far) atomicOr(d.sticky, 1u);
             }
         }
-        if (!grid_barrier(d, false)) return;
+        if (!grid_barrier(d)) return;
     }
 }
 
@@ -599,33 +646,37 @@ __global__ void wait_selftest_kernel(unsigned *word, int *err, unsigned long lon
 
 typedef void (*kernel_t)(Dev, int64_t, int64_t);
 
+// Instances: law x scheme x precision x dictionary-index width x per-entry
+// critical stretch. Irregular inputs (32-bit dictionary indices) are served
+// with the per-entry critical stretch stream in every case.
 template <int LAW, int SCHEME, int PREC>
-kernel_t pick_cid(bool wide)
+kernel_t pick_cid(bool wide, bool sce)
 {
-    return wide ? step_kernel<LAW, SCHEME, PREC, uint32_t> : step_kernel<LAW, SCHEME, PREC, uint16_t>;
+    if (wide) return step_kernel<LAW, SCHEME, PREC, uint32_t, true>;
+    return sce ? step_kernel<LAW, SCHEME, PREC, uint16_t, true> : step_kernel<LAW, SCHEME, PREC, uint16_t, false>;
 }
 
 template <int LAW, int SCHEME>
-kernel_t pick_prec(int prec, bool wide)
+kernel_t pick_prec(int prec, bool wide, bool sce)
 {
-    return prec == BBPD_PREC_FP32 ? pick_cid<LAW, SCHEME, BBPD_PREC_FP32>(wide)
-                                  : pick_cid<LAW, SCHEME, BBPD_PREC_FP64>(wide);
+    return prec == BBPD_PREC_FP32 ? pick_cid<LAW, SCHEME, BBPD_PREC_FP32>(wide, sce)
+                                  : pick_cid<LAW, SCHEME, BBPD_PREC_FP64>(wide, sce);
 }
 
 template <int LAW>
-kernel_t pick_scheme(int scheme, int prec, bool wide)
+kernel_t pick_scheme(int scheme, int prec, bool wide, bool sce)
 {
-    return scheme == BBPD_SCHEME_ADR ? pick_prec<LAW, BBPD_SCHEME_ADR>(prec, wide)
-                                     : pick_prec<LAW, BBPD_SCHEME_EULERCROMER>(prec, wide);
+    return scheme == BBPD_SCHEME_ADR ? pick_prec<LAW, BBPD_SCHEME_ADR>(prec, wide, sce)
+                                     : pick_prec<LAW, BBPD_SCHEME_EULERCROMER>(prec, wide, sce);
 }
 
-kernel_t pick_kernel(int law, int scheme, int prec, bool wide)
+kernel_t pick_kernel(int law, int scheme, int prec, bool wide, bool sce)
 {
     switch (law) {
-    case BBPD_LAW_LINEAR: return pick_scheme<BBPD_LAW_LINEAR>(scheme, prec, wide);
-    case BBPD_LAW_BILINEAR: return pick_scheme<BBPD_LAW_BILINEAR>(scheme, prec, wide);
-    case BBPD_LAW_TRILINEAR: return pick_scheme<BBPD_LAW_TRILINEAR>(scheme, prec, wide);
-    default: return pick_scheme<BBPD_LAW_EXPONENTIAL>(scheme, prec, wide);
+    case BBPD_LAW_LINEAR: return pick_scheme<BBPD_LAW_LINEAR>(scheme, prec, wide, sce);
+    case BBPD_LAW_BILINEAR: return pick_scheme<BBPD_LAW_BILINEAR>(scheme, prec, wide, sce);
+    case BBPD_LAW_TRILINEAR: return pick_scheme<BBPD_LAW_TRILINEAR>(scheme, prec, wide, sce);
+    default: return pick_scheme<BBPD_LAW_EXPONENTIAL>(scheme, prec, wide, sce);
     }
 }
 
@@ -698,26 +749,23 @@ struct Key3Hash {
     }
 };
 
-DictEntry make_entry(double l0, double vcf, double bs, double V)
+DictEntry make_entry(double l0, double vcf, double bs)
 {
     DictEntry e;
     e.l0 = l0;
-    e.rl0 = 1.0 / l0;                 // IEEE division: RN(1/L0)
     e.vcf = vcf;
     e.bs = bs;
-    e.k32 = (float)(bs * V * vcf);
     const bool regular = std::isfinite(vcf) && std::isfinite(bs) && l0 >= 0x1p-100 && l0 <= 0x1p100;
-    e.flags = regular ? 0u : 1u;
-    e.pad = 0;
+    e.rl0 = regular ? 1.0 / l0 : -1.0;   // IEEE division: RN(1/L0); -1 marks irregular
     return e;
 }
 
-// Coordinates for which the shared-divisor division is exact: 0, or a
+// Coordinates for which the shared-divisor division is exact: +0, or a
 // magnitude in [2^-100, 2^100].
 inline bool coord_safe(double x)
 {
     const double a = std::fabs(x);
-    return a == 0 || (a >= 0x1p-100 && a <= 0x1p100);
+    return (a == 0 && !std::signbit(x)) || (a >= 0x1p-100 && a <= 0x1p100);
 }
 
 inline uint64_t bits_of(double x)
@@ -909,18 +957,18 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
                 std::memcpy(&l0, &keys[q].a, 8);
                 std::memcpy(&vcf, &keys[q].b, 8);
                 std::memcpy(&bs, &keys[q].c, 8);
-                dict[q] = make_entry(l0, vcf, bs, prm->cell_volume);
+                dict[q] = make_entry(l0, vcf, bs);
             }
         } else {
             // irregular input: one dictionary entry per bond, 32-bit ids
             S->wide = true;
             dict.resize(nB);
             for (int64_t k = 0; k < nB; k++) {
-                dict[k] = make_entry(pb->undeformed_length[k], pb->volume_correction[k], pb->bond_stiffness[k], prm->cell_volume);
+                dict[k] = make_entry(pb->undeformed_length[k], pb->volume_correction[k], pb->bond_stiffness[k]);
                 bond_cid[k] = (uint32_t)k;
             }
         }
-        if (dict.empty()) dict.push_back(make_entry(1.0, 0.0, 0.0, prm->cell_volume));
+        if (dict.empty()) dict.push_back(make_entry(1.0, 0.0, 0.0));
         S->ndict = (int64_t)dict.size();
     }
 
@@ -952,6 +1000,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     for (int64_t s = 0; s < ns; s++) {
         int m = 0;
         for (int64_t i = s * 32; i < std::min(nN, s * 32 + 32); i++) m = std::max(m, deg[i]);
+        m = (m + 3) & ~3;   // whole groups of 4 entries per lane
         slen[s] = m;
         sptr[s + 1] = sptr[s] + (int64_t)m * 32;
     }
@@ -967,7 +1016,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     std::vector<double> s0e, s1e, sce;
     if (pb->s0) s0e.assign(ne, 0.0);
     if (pb->s1) s1e.assign(ne, 0.0);
-    if (pb->sc) sce.assign(ne, 0.0);
+    if (pb->sc || S->wide) sce.assign(ne, prm->sc);   // 32-bit-index instances always read a stream
     S->ent_i.resize(nB);
     S->ent_j.resize(nB);
     host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
@@ -978,7 +1027,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
             const uint8_t st0 = (pb->fail && pb->fail[k] == 0) ? ST_BROKEN : 0;
             for (int side = 0; side < 2; side++) {
                 const int64_t me = side ? b : a, other = side ? a : b;
-                const int64_t pos = sptr[me / 32] + (int64_t)rank[me] * 32 + (me % 32);
+                const int64_t pos = entry_pos(sptr[me / 32], rank[me], (int)(me % 32));
                 rank[me]++;
                 colw[pos] = (uint32_t)other | bt;
                 if (S->wide) cid32[pos] = bond_cid[k];
@@ -997,7 +1046,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     host_parallel_for(nN, [&](int64_t me) {
         int prev = -1;
         for (int32_t r = 0; r < deg[me]; r++) {
-            const int64_t pos = sptr[me / 32] + (int64_t)r * 32 + (me % 32);
+            const int64_t pos = entry_pos(sptr[me / 32], r, (int)(me % 32));
             const int c = chunk_of_host(bond_of[pos], nB, T);
             if (c != prev) colw[pos] |= F_CHUNK;
             prev = c;
@@ -1050,6 +1099,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     d.n_slices = ns;
     TRY(S->put((int64_t **)&d.slice_ptr, sptr));
     TRY(S->put((int32_t **)&d.deg, deg));
+    TRY(S->put((int32_t **)&d.slice_len, slen));
     TRY(S->put((uint32_t **)&d.colw, colw));
     if (S->wide) TRY(S->put((uint32_t **)&d.cid, cid32));
     else TRY(S->put((uint16_t **)&d.cid, cid16));
@@ -1057,10 +1107,15 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     TRY(S->alloc(&d.bsf, (size_t)ne));
     BBPD_CUDA_TRY(cudaMemset(d.bsf, 0, sizeof(double) * std::max<int64_t>(ne, 1)));
     TRY(S->put((DictEntry **)&d.dict, dict));
+    {
+        std::vector<float> k32(dict.size());
+        for (size_t q = 0; q < dict.size(); q++) k32[q] = (float)(dict[q].bs * prm->cell_volume * dict[q].vcf);
+        TRY(S->put((float **)&d.dict32, k32));
+    }
     d.s0e = d.s1e = d.sce = nullptr;
     if (pb->s0) TRY(S->put((double **)&d.s0e, s0e));
     if (pb->s1) TRY(S->put((double **)&d.s1e, s1e));
-    if (pb->sc) TRY(S->put((double **)&d.sce, sce));
+    if (pb->sc || S->wide) TRY(S->put((double **)&d.sce, sce));
     TRY(S->put((double **)&d.X, X3));
     TRY(S->put(&d.xb0, x0));
     TRY(S->put(&d.xb1, x0));
@@ -1074,8 +1129,30 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     TRY(S->put((double **)&d.mass, mass));
     TRY(S->put((double **)&d.rho, rho));
     TRY(S->put((uint8_t **)&d.nflag, nflag));
-    TRY(S->alloc(&d.part, (size_t)(2 * ns)));
-    TRY(S->alloc(&d.strand, (size_t)(2 * kStrands)));
+    {
+        // levels of the reduction tree: level 1 has one value per slice,
+        // level L+1 one per group of 32 values of level L
+        int64_t off = 0, coff = 0, c = ns;
+        int L = 1;
+        d.lvl_cnt[L] = c;
+        d.lvl_off[L] = 0;
+        d.cnt_off[L] = 0;
+        off = c;
+        while (c > 1) {
+            if (L + 1 >= kMaxLevels) return fail(BBPD_ERR_UNSUPPORTED, "too many slices for the reduction tree");
+            c = (c + 31) / 32;
+            L++;
+            d.lvl_cnt[L] = c;
+            d.lvl_off[L] = off;
+            d.cnt_off[L] = coff;
+            off += c;
+            coff += c;
+        }
+        d.n_levels = L;
+        TRY(S->alloc(&d.tree, (size_t)std::max<int64_t>(off, 1)));
+        std::vector<unsigned> tc((size_t)std::max<int64_t>(coff, 1), 0u);
+        TRY(S->put(&d.tcnt, tc));
+    }
     std::vector<double> sc4(4, 0.0);
     TRY(S->put(&d.scal, sc4));
     std::vector<unsigned> bar(2, 0u);
@@ -1111,7 +1188,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     d.timeout_ns = (unsigned long long)(to * 1e9);
 
     // kernel and grid
-    S->kernel = pick_kernel(prm->law, prm->scheme, prm->precision, S->wide);
+    S->kernel = pick_kernel(prm->law, prm->scheme, prm->precision, S->wide, pb->sc != nullptr);
     int nsm = 0, occ = 0, coop = 0;
     BBPD_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     BBPD_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));

@@ -254,30 +254,43 @@ double orc_damping_coefficient_seq(const double *F, const double *m,
     return orc_cn_from_sums(cn1, cn2);
 }
 
+/* xor butterfly over 32 values (offsets 16, 8, 4, 2, 1); value of lane 0 */
+static double butterfly32(double v[32])
+{
+    double w[32];
+    for (int off = 16; off >= 1; off /= 2) {
+        for (int l = 0; l < 32; l++) w[l] = v[l] + v[l ^ off];
+        memcpy(v, w, sizeof(w));
+    }
+    return v[0];
+}
+
 double orc_tree_sum(const double *t, int64_t n)
 {
-    enum { W = 32, R = 1024 };
-    int64_t nsl = (n + W - 1) / W;
-    double acc[R];
-    for (int r = 0; r < R; r++) acc[r] = 0.0;
-    for (int64_t sl = 0; sl < nsl; sl++) {
-        double v[W], w[W];
-        for (int l = 0; l < W; l++) {
-            int64_t idx = sl * W + l;
-            v[l] = (idx < n) ? t[idx] : 0.0;
+    if (n <= 0) return 0.0;
+    int64_t m = (n + 31) / 32;
+    double *p = (double *)malloc(sizeof(double) * (size_t)m);
+    const double *src = t;
+    int64_t cnt = n;
+    /* level 1 reduces the terms, every further level the previous partials,
+     * 32 consecutive values at a time, until one value is left */
+    for (;;) {
+        m = (cnt + 31) / 32;
+        for (int64_t g = 0; g < m; g++) {
+            double v[32];
+            for (int l = 0; l < 32; l++) {
+                int64_t idx = g * 32 + l;
+                v[l] = (idx < cnt) ? src[idx] : 0.0;
+            }
+            p[g] = butterfly32(v);   /* g < m <= index of src being read: in place is safe */
         }
-        for (int off = W / 2; off >= 1; off /= 2) {
-            for (int l = 0; l < W; l++) w[l] = v[l] + v[l ^ off];
-            memcpy(v, w, sizeof(v));
-        }
-        acc[sl % R] = acc[sl % R] + v[0];
+        if (m == 1) break;
+        src = p;
+        cnt = m;
     }
-    for (int off = R / 2; off >= 1; off /= 2) {
-        double w[R];
-        for (int r = 0; r < R; r++) w[r] = acc[r] + acc[r ^ off];
-        memcpy(acc, w, sizeof(acc));
-    }
-    return acc[0];
+    double r = p[0];
+    free(p);
+    return r;
 }
 
 double orc_damping_coefficient_tree(const double *F, const double *m,

@@ -104,13 +104,12 @@ double orc_damping_coefficient_tree(const double *F, const double *m,
 /* Clamp of calculatedampingcoefficient.m:90-112 applied to two sums. */
 double orc_cn_from_sums(double cn1, double cn2);
 
-/* Fixed reduction order over per-node terms t[0..n):
- *   level 1: slices of 32 consecutive nodes, xor-butterfly over the 32 lanes
- *            (offsets 16, 8, 4, 2, 1; lane l adds lane l^off), result of lane 0;
- *   level 2: 1024 strands, strand r sums slices r, r+1024, ... sequentially
- *            starting from 0.0, then an xor-butterfly over the 1024 strands
- *            (offsets 512 ... 1), result of strand 0.
- * Missing lanes/strands contribute 0.0. */
+/* Fixed reduction order over per-node terms t[0..n): a 32-ary tree. Level 1
+ * takes slices of 32 consecutive nodes, every further level groups of 32
+ * consecutive partials of the level below; each group is folded by an xor
+ * butterfly (offsets 16, 8, 4, 2, 1; lane l adds lane l^off; the result is
+ * lane 0's), missing members count as 0.0; levels repeat until one value is
+ * left. */
 double orc_tree_sum(const double *t, int64_t n);
 
 /* timeintegrationADR.m:168-197 (ADR central-difference half-step update). */

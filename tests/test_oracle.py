@@ -263,22 +263,23 @@ def test_kat_adr_damping():
 def test_tree_sum_order():
     """orc_tree_sum follows its documented pairing (restated here in numpy)."""
     rng = np.random.default_rng(3)
-    for n in (1, 31, 32, 33, 1000, 40000, 70001):
-        t = rng.normal(size=n) * 10.0 ** rng.integers(-8, 8, n)
-        nsl = -(-n // 32)
-        v = np.zeros(nsl * 32)
-        v[:n] = t
-        v = v.reshape(nsl, 32)
+
+    def level(x):
+        m = -(-len(x) // 32)
+        v = np.zeros(m * 32)
+        v[:len(x)] = x
+        v = v.reshape(m, 32)
         for off in (16, 8, 4, 2, 1):
             v = v + v[:, np.arange(32) ^ off]
-        part = v[:, 0]
-        acc = np.zeros(1024)
-        for k in range(nsl):           # sequential per strand
-            acc[k % 1024] = acc[k % 1024] + part[k]
-        for off in (512, 256, 128, 64, 32, 16, 8, 4, 2, 1):
-            acc = acc + acc[np.arange(1024) ^ off]
-        assert po.tree_sum(t) == acc[0]
-        assert abs(acc[0] - t.sum()) <= 1e-12 * np.abs(t).sum()
+        return v[:, 0]
+
+    for n in (1, 31, 32, 33, 1000, 1025, 40000, 70001, 1280000):
+        t = rng.normal(size=n) * 10.0 ** rng.integers(-8, 8, n)
+        p = level(t)
+        while len(p) > 1:
+            p = level(p)
+        assert po.tree_sum(t) == p[0]
+        assert abs(p[0] - t.sum()) <= 1e-12 * np.abs(t).sum()
 
 
 def test_chunk_rule_matches_libgomp(tmp_path):
