@@ -64,9 +64,16 @@ constexpr int ERR_NONFINITE = 2;
 
 constexpr int kBlock = 256;
 #ifndef BBPD_MIN_BLOCKS
-#define BBPD_MIN_BLOCKS 3
+#define BBPD_MIN_BLOCKS 2       // resident blocks per SM, FP64 kernels
+#endif
+#ifndef BBPD_MIN_BLOCKS_F32
+#define BBPD_MIN_BLOCKS_F32 2   // resident blocks per SM, FP32 dictionary-vector kernels
 #endif
 constexpr int kMaxLevels = 8;     // 32-ary reduction tree over the slices
+
+// Kernel precision variants. The FP32 form runs as kP32X when the bond vectors
+// compress into the dictionary and as kP32D (FP64 differences) otherwise.
+constexpr int kP64 = 0, kP32D = 1, kP32X = 2;
 
 // Entry k of the list of lane `lane` in the slice whose entries start at sbase:
 // each lane's entries come in groups of 4 contiguous slots, lanes interleaved
@@ -96,6 +103,8 @@ struct Dev {
     double *bsf;
     const DictEntry *dict;
     const float *dict32;             // BONDSTIFFNESS * cellVolume * VCF per dictionary entry (FP32 form)
+    const float4 *dictx;             // FP32 form, 2 per entry: (xi_x, xi_y, xi_z, L0), (k32, |xi|^2-L0^2, regular, 0)
+    float4 *ur0, *ur1;               // FP32 form: per node (uh, ul) FP32 split of the displacement, 32 B, ping-pong like positions
     const double *s0e, *s1e, *sce;   // per-entry law stretches or null
     const double *X;
     double *xb0, *xb1;               // positions: step n reads xb[(n-1)&1], writes xb[n&1]
@@ -342,7 +351,7 @@ __device__ BBPD_GENERAL_ATTR double3 entry_general(const Dev &d, int64_t e, uint
     double dX, dY, dZ, L, s;
     float sf = 0.f, Lf = 0.f;
     bool exact = true;
-    if (PREC == BBPD_PREC_FP64) {
+    if (PREC == kP64) {
         bond_kinematics(xi, yi, zi, xj, yj, zj, g.l0, dX, dY, dZ, L, s);
     } else {
         dX = xj - xi; dY = yj - yi; dZ = zj - zi;
@@ -382,7 +391,7 @@ __device__ BBPD_GENERAL_ATTR double3 entry_general(const Dev &d, int64_t e, uint
     if (__double_as_longlong(B) != __double_as_longlong(B0)) d.bsf[e] = B;
     // bond force (calculatebondforcesMex.c:34-40)
     double3 f;
-    if (PREC == BBPD_PREC_FP64 || exact) {
+    if (PREC == kP64 || exact) {
         const double t = bond_force_scalar(failv, g.bs, B, s, 0.0, d.V, g.vcf);
         f.x = bond_force_component(t, dX, L);
         f.y = bond_force_component(t, dY, L);
@@ -410,7 +419,7 @@ __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fe
     const int bt = (f.w >> BT_SHIFT) & 3;
     const double s0b = d.s0e ? __ldg(d.s0e + e) : d.P.s0;
     double3 r;
-    if (PREC == BBPD_PREC_FP64) {
+    if (PREC == kP64) {
         // calculatedeformedlengthMex.c:37-43 with its division by L0 and the
         // three of calculatebondforcesMex.c:34-36 by L done as correctly
         // rounded quotients with shared reciprocals (divide.cuh): bit-identical
@@ -452,11 +461,11 @@ __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fe
     return entry_general<LAW, PREC>(d, e, f.w, f.sv, f.g, f.sc, xi, yi, zi, f.xj, f.yj, f.zj);
 }
 
-// Forces of the 32 nodes of one slice. Lane `lane` owns node sl*32+lane and
-// walks its entries in bond order, a group of 4 at a time: the next group's
-// streams load while the current group's 12 coordinate gathers are issued
-// together and its entries computed. Returns the node's force summed in the
-// reference's order.
+// Forces of the 32 nodes of one slice (FP64 form and FP32 difference form).
+// Lane `lane` owns node sl*32+lane and walks its entries in bond order, a group
+// of 4 at a time: the next group's streams load while the current group's 12
+// coordinate gathers are issued together and its entries computed. Returns the
+// node's force summed in the reference's order.
 template <int LAW, int PREC, class CID, bool SCE>
 __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane, bool safe,
                                              const double *xs, double &tx, double &ty,
@@ -475,17 +484,10 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
 
     const int ng = (dg + 3) >> 2;
     Group<CID> Gc, Gn;
-    double2 sca = make_double2(0, 0), scb = make_double2(0, 0), sna = sca, snb = sca;
     int64_t e0 = entry_pos(sb, 0, lane);
-    if (ng > 0) {
-        load_group<CID>(d, e0, Gc);
-        if (SCE) { sca = __ldcs(reinterpret_cast<const double2 *>(d.sce + e0)); scb = __ldcs(reinterpret_cast<const double2 *>(d.sce + e0) + 1); }
-    }
+    if (ng > 0) load_group<CID>(d, e0, Gc);
     for (int g = 0; g < ng; g++, e0 += 128) {
-        if (g + 1 < ng) {
-            load_group<CID>(d, e0 + 128, Gn);
-            if (SCE) { sna = __ldcs(reinterpret_cast<const double2 *>(d.sce + e0 + 128)); snb = __ldcs(reinterpret_cast<const double2 *>(d.sce + e0 + 128) + 1); }
-        }
+        if (g + 1 < ng) load_group<CID>(d, e0 + 128, Gn);
         const int nq = min(4, dg - 4 * g);
         double xj[4], yj[4], zj[4];
 #pragma unroll
@@ -502,7 +504,7 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
                 f.w = group_w(Gc, q);
                 f.c = Gc.cid(q);
                 f.sv = (Gc.s >> (8 * q)) & 0xFFu;
-                f.sc = SCE ? (q == 0 ? sca.x : q == 1 ? sca.y : q == 2 ? scb.x : scb.y) : d.P.sc;
+                f.sc = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
                 f.xj = xj[q]; f.yj = yj[q]; f.zj = zj[q];
                 f.g = ldg_dict(d.dict, f.c);
                 const double3 r = entry_force<LAW, PREC>(d, e0 + q, f, safe, xi, yi, zi);
@@ -514,10 +516,105 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
             }
         }
         Gc = Gn;
-        if (SCE) { sca = sna; scb = snb; }
     }
     tx = tx + ax; ty = ty + ay; tz = tz + az;
 }
+
+// General path of the FP32 dictionary-vector form, out of line so that the
+// fast path keeps its registers: FP64 positions of both nodes, then the
+// general entry in difference form.
+template <int LAW>
+__device__ __noinline__ double3 entry_general_x(const Dev &d, int64_t e, uint32_t w, uint32_t sv,
+                                                uint32_t c, double scd, int64_t i, const double *xs)
+{
+    const int64_t nN = d.n_nodes;
+    const uint32_t j = w & COL_MASK;
+    return entry_general<LAW, kP32D>(d, e, w, sv, ldg_dict(d.dict, c), scd, xs[i], xs[i + nN],
+                                     xs[i + 2 * nN], xs[j], xs[j + nN], xs[j + 2 * nN]);
+}
+
+// FP32 form, dictionary bond vectors (kP32X). Lane `lane` owns node sl*32+lane.
+// The deformed bond vector is e = xi + eta: xi = X_j - X_i from the dictionary
+// (FP32), eta = (uh_j - uh_i) + (ul_j - ul_i) from a 32-byte record per node
+// holding the displacement split into FP32 high and low parts (one sector per
+// gather; eta keeps close to FP64 accuracy under rigid translation), and
+//   L^2 - L0^2 = eta . (2 xi + eta) + (|xi|^2 - L0^2),  s = (L^2 - L0^2) / (L0 (L + L0))
+// is computed without cancellation; force = BS V VCF s e / L in FP32, summed in
+// FP64 in the reference's order. Bonds whose stretch lies within the guard band
+// of the critical stretch, damaged or broken bonds and bonds whose law is active
+// take the general path with FP64 positions.
+template <int LAW, class CID, bool SCE>
+__device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lane, const double *xs,
+                                               const float4 *ur, double &tx, double &ty, double &tz)
+{
+    const int64_t nN = d.n_nodes;
+    const int64_t i = sl * 32 + lane;
+    const int dg = (i < nN) ? d.deg[i] : 0;
+    const int64_t sb = d.slice_ptr[sl];
+
+    float4 ui = make_float4(0.f, 0.f, 0.f, 0.f), li = ui;
+    if (i < nN) { ui = ur[2 * i]; li = ur[2 * i + 1]; }
+    tx = 0.0; ty = 0.0; tz = 0.0;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    const float s0f = (float)d.P.s0, guardf = (float)d.guard;
+
+    const int ng = (dg + 3) >> 2;
+    Group<CID> Gc, Gn;
+    int64_t e0 = entry_pos(sb, 0, lane);
+    if (ng > 0) load_group<CID>(d, e0, Gc);
+    for (int g = 0; g < ng; g++, e0 += 128) {
+        if (g + 1 < ng) load_group<CID>(d, e0 + 128, Gn);
+        const int nq = min(4, dg - 4 * g);
+        float4 uj[4], lj[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (q < nq) {
+                const uint32_t j = group_w(Gc, q) & COL_MASK;
+                uj[q] = ur[2 * j];
+                lj[q] = ur[2 * j + 1];
+            }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (q < nq) {
+                const int64_t e = e0 + q;
+                const uint32_t w = group_w(Gc, q), c = Gc.cid(q), sv = (Gc.s >> (8 * q)) & 0xFFu;
+                const double scd = SCE ? __ldcs(d.sce + e) : d.P.sc;
+                const int bt = (w >> BT_SHIFT) & 3;
+                const float4 A = __ldg(&d.dictx[2 * c]), Bv = __ldg(&d.dictx[2 * c + 1]);
+                const float etx = (uj[q].x - ui.x) + (lj[q].x - li.x);
+                const float ety = (uj[q].y - ui.y) + (lj[q].y - li.y);
+                const float etz = (uj[q].z - ui.z) + (lj[q].z - li.z);
+                const float ex = A.x + etx, ey = A.y + ety, ez = A.z + etz;
+                const float L2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
+                const float rL = rsqrtf(L2);
+                const float L = L2 * rL;
+                const float num = __fmaf_rn(etz, A.z + ez, __fmaf_rn(ety, A.y + ey, __fmaf_rn(etx, A.x + ex, Bv.y)));
+                const float sf = __fdividef(num, A.w * (L + A.w));
+                const float crit = (float)((LAW == BBPD_LAW_LINEAR) ? linear_crit(d.P, bt, scd) : scd);
+                const float s0b = d.s0e ? (float)__ldg(d.s0e + e) : s0f;
+                const bool quiet = (LAW == BBPD_LAW_LINEAR) ? !(sf > crit) : !(bt == 0 && sf > s0b);
+                double3 r;
+                if (sv == 0 && Bv.z != 0.f && L2 > 0.f && L2 < INFINITY && !(fabsf(sf - crit) < guardf) && quiet) {
+                    const float qf = Bv.x * sf * rL;
+                    r.x = (double)(qf * ex);
+                    r.y = (double)(qf * ey);
+                    r.z = (double)(qf * ez);
+                } else {
+                    r = entry_general_x<LAW>(d, e, w, sv, c, scd, i, xs);
+                }
+                if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
+                    tx = tx + ax; ty = ty + ay; tz = tz + az;
+                    ax = 0.0; ay = 0.0; az = 0.0;
+                }
+                ax = ax + r.x; ay = ay + r.y; az = az + r.z;
+            }
+        }
+        Gc = Gn;
+    }
+    tx = tx + ax; ty = ty + ay; tz = tz + az;
+}
+
+
 
 // Coordinates for which the shared-divisor division of divide.cuh is exact:
 // +0, or a magnitude in [2^-100, 2^100] (a -0 coordinate could make a -0
@@ -529,7 +626,7 @@ __device__ __forceinline__ bool coord_out_of_range(double x)
 }
 
 template <int LAW, int SCHEME, int PREC, class CID, bool SCE>
-__global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, int64_t step0, int64_t nsteps)
+__global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : BBPD_MIN_BLOCKS) step_kernel(Dev d, int64_t step0, int64_t nsteps)
 {
     const int lane = threadIdx.x & 31;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -543,6 +640,8 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
         const double *Fp = (n & 1) ? d.F0 : d.F1;
         const double *xs = ((n - 1) & 1) ? d.xb1 : d.xb0;
         double *xn = (n & 1) ? d.xb1 : d.xb0;
+        const float4 *urs = ((n - 1) & 1) ? d.ur1 : d.ur0;
+        float4 *urn = (n & 1) ? d.ur1 : d.ur0;
         const double Un1 = prescribed_value(d, n + 1);
         const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
 
@@ -551,12 +650,14 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
             const int64_t i = sl * 32 + lane;
             const bool valid = i < nN;
             double tx, ty, tz;
-            slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, xs, tx, ty, tz);
+            if (PREC == kP32X) slice_forces_x<LAW, CID, SCE>(d, sl, lane, xs, urs, tx, ty, tz);
+            else slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, xs, tx, ty, tz);
             if (SCHEME == BBPD_SCHEME_EULERCROMER) {
                 if (valid) {
                     // timeintegrationeulercromerMex.c:33-50 on the node just summed
                     const uint8_t fl = d.nflag[i];
                     const double Fv[3] = {tx, ty, tz};
+                    float uh[3], ul[3];
                     bool bad = false, far = false;
 #pragma unroll
                     for (int dof = 0; dof < 3; dof++) {
@@ -570,8 +671,13 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
                         if (fl & (8 << dof)) { ue = Un1; xe = d.X[e] + ue; }
                         if (d.a) d.a[e] = ae;
                         d.v[e] = ve; d.u[e] = ue; xn[e] = xe;
+                        uh[dof] = (float)ue; ul[dof] = (float)(ue - (double)uh[dof]);
                         bad |= !isfinite(ue) || !isfinite(ve);
                         far |= coord_out_of_range(xe);
+                    }
+                    if (PREC == kP32X) {
+                        urn[2 * i] = make_float4(uh[0], uh[1], uh[2], 0.f);
+                        urn[2 * i + 1] = make_float4(ul[0], ul[1], ul[2], 0.f);
                     }
                     if (bad) atomicOr(d.err, ERR_NONFINITE);
                     if (far) atomicOr(d.sticky, 1u);
@@ -613,6 +719,7 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
                 if (i >= nN) continue;
                 const uint8_t fl = d.nflag[i];
                 const double minv = 1.0 / d.mass[i];
+                float uh[3], ul[3];
                 bool bad = false, far = false;
 #pragma unroll
                 for (int dof = 0; dof < 3; dof++) {
@@ -626,8 +733,13 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) step_kernel(Dev d, in
                     if (fl & (8 << dof)) { ue = Un1; vh = 0; }
                     const double xe = d.X[e] + ue;
                     d.v[e] = vh; d.u[e] = ue; xn[e] = xe;
+                    uh[dof] = (float)ue; ul[dof] = (float)(ue - (double)uh[dof]);
                     bad |= !isfinite(ue) || !isfinite(vh);
                     far |= coord_out_of_range(xe);
+                }
+                if (PREC == kP32X) {
+                    urn[2 * i] = make_float4(uh[0], uh[1], uh[2], 0.f);
+                    urn[2 * i + 1] = make_float4(ul[0], ul[1], ul[2], 0.f);
                 }
                 if (bad) atomicOr(d.err, ERR_NONFINITE);
                 if (far) atomicOr(d.sticky, 1u);
@@ -652,15 +764,18 @@ typedef void (*kernel_t)(Dev, int64_t, int64_t);
 template <int LAW, int SCHEME, int PREC>
 kernel_t pick_cid(bool wide, bool sce)
 {
-    if (wide) return step_kernel<LAW, SCHEME, PREC, uint32_t, true>;
+    if constexpr (PREC != kP32X) {   // the dictionary-vector form only runs with 16-bit ids
+        if (wide) return step_kernel<LAW, SCHEME, PREC, uint32_t, true>;
+    }
     return sce ? step_kernel<LAW, SCHEME, PREC, uint16_t, true> : step_kernel<LAW, SCHEME, PREC, uint16_t, false>;
 }
 
 template <int LAW, int SCHEME>
 kernel_t pick_prec(int prec, bool wide, bool sce)
 {
-    return prec == BBPD_PREC_FP32 ? pick_cid<LAW, SCHEME, BBPD_PREC_FP32>(wide, sce)
-                                  : pick_cid<LAW, SCHEME, BBPD_PREC_FP64>(wide, sce);
+    if (prec == kP32X) return pick_cid<LAW, SCHEME, kP32X>(wide, sce);
+    if (prec == kP32D) return pick_cid<LAW, SCHEME, kP32D>(wide, sce);
+    return pick_cid<LAW, SCHEME, kP64>(wide, sce);
 }
 
 template <int LAW>
@@ -735,6 +850,36 @@ uint64_t morton3(uint32_t a, uint32_t b, uint32_t c)
     return spread(a) | (spread(b) << 1) | (spread(c) << 2);
 }
 
+struct KeyX {
+    uint64_t a, b, c;
+    uint32_t x, y, z;
+    bool operator==(const KeyX &o) const { return a == o.a && b == o.b && c == o.c && x == o.x && y == o.y && z == o.z; }
+    bool operator<(const KeyX &o) const
+    {
+        if (a != o.a) return a < o.a;
+        if (b != o.b) return b < o.b;
+        if (c != o.c) return c < o.c;
+        if (x != o.x) return x < o.x;
+        return y != o.y ? y < o.y : z < o.z;
+    }
+};
+struct KeyXHash {
+    size_t operator()(const KeyX &k) const
+    {
+        uint64_t h = k.a * 0x9E3779B97F4A7C15ull ^ (k.b + 0x632BE59BD9B4E019ull) * 0xBF58476D1CE4E5B9ull;
+        h ^= (k.c + 0x94D049BB133111EBull) * 0xD6E8FEB86659FD93ull;
+        h ^= ((uint64_t)k.x << 32 | k.y) * 0xA24BAED4963EE407ull ^ (uint64_t)k.z * 0x9FB21C651E98DF25ull;
+        return (size_t)(h ^ (h >> 29));
+    }
+};
+
+inline uint32_t fbits(float x)
+{
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    return u;
+}
+
 struct Key3 {
     uint64_t a, b, c;
     bool operator==(const Key3 &o) const { return a == o.a && b == o.b && c == o.c; }
@@ -762,6 +907,25 @@ DictEntry make_entry(double l0, double vcf, double bs)
 
 // Coordinates for which the shared-divisor division is exact: +0, or a
 // magnitude in [2^-100, 2^100].
+// Per-node FP32 (high, low) record of a node-major displacement array u
+// (x of node p at [p], y at [p + nN], z at [p + 2 nN]): [2p] = high parts,
+// [2p + 1] = low parts, matching what the kernels write after each step.
+std::vector<float4> split_record(const double *u, int64_t nN)
+{
+    std::vector<float4> r(2 * nN);
+    for (int64_t p = 0; p < nN; p++) {
+        float h[3], l[3];
+        for (int c = 0; c < 3; c++) {
+            const double v = u[p + c * nN];
+            h[c] = (float)v;
+            l[c] = (float)(v - (double)h[c]);
+        }
+        r[2 * p] = make_float4(h[0], h[1], h[2], 0.f);
+        r[2 * p + 1] = make_float4(l[0], l[1], l[2], 0.f);
+    }
+    return r;
+}
+
 inline bool coord_safe(double x)
 {
     const double a = std::fabs(x);
@@ -782,6 +946,7 @@ struct bbpd_solver {
     bbpd_params prm{};
     int64_t nN = 0, nB = 0, ns = 0, ne = 0, ndict = 0;
     bool wide = false;
+    int prec = kP64;                    // kernel variant (kP64, kP32D, kP32X)
     int64_t step = 1;
     double cn = 0;
     std::vector<int32_t> perm;          // device position -> input node
@@ -914,10 +1079,74 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     for (int64_t p = 0; p < nN; p++) S->inv[S->perm[p]] = (int32_t)p;
     const int32_t *inv = S->inv.data();
 
-    // dictionary of (L0, VCF, BONDSTIFFNESS) triples
-    std::vector<uint32_t> bond_cid(nB);
+    // FP32 form: a dictionary of (L0, VCF, BONDSTIFFNESS, bond vector in FP32)
+    // with one id per directed entry; kept when it fits 16-bit ids
+    std::vector<uint32_t> bond_cid(nB), cid_j;
     std::vector<DictEntry> dict;
-    {
+    std::vector<float4> dictx;
+    S->prec = kP64;
+    if (prm->precision == BBPD_PREC_FP32) {
+        S->prec = kP32D;
+        const double *X = pb->undeformed_coordinates;
+        auto keyx = [&](int64_t k, int side) {
+            int64_t a = (int64_t)bl[k] - 1, b = (int64_t)bl[nB + k] - 1;
+            if (side) std::swap(a, b);   // bond vector X[other] - X[me]
+            const float fx = (float)(X[b] - X[a]), fy = (float)(X[b + nN] - X[a + nN]),
+                        fz = (float)(X[b + 2 * nN] - X[a + 2 * nN]);
+            return KeyX{bits_of(pb->undeformed_length[k]), bits_of(pb->volume_correction[k]),
+                        bits_of(pb->bond_stiffness[k]), fbits(fx), fbits(fy), fbits(fz)};
+        };
+        const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
+        std::vector<std::unordered_map<KeyX, uint32_t, KeyXHash>> local(HT);
+        host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
+            auto &m = local[t];
+            for (int64_t k = lo; k < hi && m.size() <= 70000; k++) {
+                m.emplace(keyx(k, 0), 0u);
+                m.emplace(keyx(k, 1), 0u);
+            }
+        });
+        std::unordered_map<KeyX, uint32_t, KeyXHash> all;
+        bool overflow = false;
+        for (auto &m : local) {
+            if (m.size() > 70000) overflow = true;
+            for (auto &kv : m) all.emplace(kv.first, 0u);
+        }
+        if (all.size() > 65535) overflow = true;
+        if (!overflow) {
+            std::vector<KeyX> keys;
+            keys.reserve(all.size());
+            for (auto &kv : all) keys.push_back(kv.first);
+            std::sort(keys.begin(), keys.end());
+            for (size_t q = 0; q < keys.size(); q++) all[keys[q]] = (uint32_t)q;
+            cid_j.resize(nB);
+            host_ranges(nB, HT, [&](int, int64_t lo, int64_t hi) {
+                for (int64_t k = lo; k < hi; k++) {
+                    bond_cid[k] = all.find(keyx(k, 0))->second;
+                    cid_j[k] = all.find(keyx(k, 1))->second;
+                }
+            });
+            dict.resize(keys.size());
+            dictx.resize(2 * keys.size());
+            for (size_t q = 0; q < keys.size(); q++) {
+                double l0, vcf, bs;
+                std::memcpy(&l0, &keys[q].a, 8);
+                std::memcpy(&vcf, &keys[q].b, 8);
+                std::memcpy(&bs, &keys[q].c, 8);
+                dict[q] = make_entry(l0, vcf, bs);
+                float xf, yf, zf;
+                std::memcpy(&xf, &keys[q].x, 4);
+                std::memcpy(&yf, &keys[q].y, 4);
+                std::memcpy(&zf, &keys[q].z, 4);
+                const double c0 = ((double)xf * xf + (double)yf * yf + (double)zf * zf) - l0 * l0;
+                dictx[2 * q] = make_float4(xf, yf, zf, (float)l0);
+                dictx[2 * q + 1] = make_float4((float)(bs * prm->cell_volume * vcf), (float)c0,
+                                               dict[q].rl0 > 0 ? 1.f : 0.f, 0.f);
+            }
+            S->prec = kP32X;
+            S->ndict = (int64_t)dict.size();
+        }
+    }
+    if (S->prec != kP32X) {
         const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
         std::vector<std::unordered_map<Key3, uint32_t, Key3Hash>> local(HT);
         host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
@@ -1030,8 +1259,9 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
                 const int64_t pos = entry_pos(sptr[me / 32], rank[me], (int)(me % 32));
                 rank[me]++;
                 colw[pos] = (uint32_t)other | bt;
-                if (S->wide) cid32[pos] = bond_cid[k];
-                else cid16[pos] = (uint16_t)bond_cid[k];
+                const uint32_t cidv = (side && S->prec == kP32X) ? cid_j[k] : bond_cid[k];
+                if (S->wide) cid32[pos] = cidv;
+                else cid16[pos] = (uint16_t)cidv;
                 st[pos] = st0;
                 bond_of[pos] = (int32_t)k;
                 if (pb->s0) s0e[pos] = pb->s0[k];
@@ -1107,6 +1337,14 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     TRY(S->alloc(&d.bsf, (size_t)ne));
     BBPD_CUDA_TRY(cudaMemset(d.bsf, 0, sizeof(double) * std::max<int64_t>(ne, 1)));
     TRY(S->put((DictEntry **)&d.dict, dict));
+    d.dictx = nullptr;
+    d.ur0 = d.ur1 = nullptr;
+    if (S->prec == kP32X) {
+        TRY(S->put((float4 **)&d.dictx, dictx));
+        const std::vector<float4> ur = split_record(u0.data(), nN);
+        TRY(S->put(&d.ur0, ur));
+        TRY(S->put(&d.ur1, ur));
+    }
     {
         std::vector<float> k32(dict.size());
         for (size_t q = 0; q < dict.size(); q++) k32[q] = (float)(dict[q].bs * prm->cell_volume * dict[q].vcf);
@@ -1188,7 +1426,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     d.timeout_ns = (unsigned long long)(to * 1e9);
 
     // kernel and grid
-    S->kernel = pick_kernel(prm->law, prm->scheme, prm->precision, S->wide, pb->sc != nullptr);
+    S->kernel = pick_kernel(prm->law, prm->scheme, S->prec, S->wide, pb->sc != nullptr);
     int nsm = 0, occ = 0, coop = 0;
     BBPD_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     BBPD_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
@@ -1360,6 +1598,12 @@ extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
         for (int c = 0; c < 3; c++)
             for (int64_t p = 0; p < nN; p++) h[p + c * nN] = in[S->perm[p] + c * nN];
         BBPD_CUDA_TRY(cudaMemcpy(dst, h.data(), sizeof(double) * 3 * nN, cudaMemcpyHostToDevice));
+        if (field == BBPD_FIELD_DISPLACEMENT && S->prec == kP32X) {
+            // the FP32 form gathers an FP32 record of the displacement
+            const std::vector<float4> ur = split_record(h.data(), nN);
+            BBPD_CUDA_TRY(cudaMemcpy(S->d.ur0, ur.data(), sizeof(float4) * 2 * nN, cudaMemcpyHostToDevice));
+            BBPD_CUDA_TRY(cudaMemcpy(S->d.ur1, ur.data(), sizeof(float4) * 2 * nN, cudaMemcpyHostToDevice));
+        }
         if (field == BBPD_FIELD_DEFORMED) {
             // both position buffers: the next step reads the one of its parity
             BBPD_CUDA_TRY(cudaMemcpy(dst == S->d.xb0 ? S->d.xb1 : S->d.xb0, h.data(), sizeof(double) * 3 * nN, cudaMemcpyHostToDevice));
@@ -1419,6 +1663,7 @@ extern "C" int bbpd_set_step(bbpd_solver *S, int64_t step, double cn)
     if (((step - S->step) & 1) != 0) {
         std::swap(S->d.F0, S->d.F1);
         std::swap(S->d.xb0, S->d.xb1);
+        std::swap(S->d.ur0, S->d.ur1);
     }
     S->step = step;
     S->cn = cn;
@@ -1459,7 +1704,7 @@ extern "C" int bbpd_get_info(bbpd_solver *S, bbpd_info *info)
     info->block_threads = kBlock;
     info->device_bytes = S->device_bytes;
     info->bytes_per_step = S->bytes_per_step;
-    info->layout = S->wide ? 2 : 1;
+    info->layout = S->wide ? 2 : (S->prec == kP32X ? 3 : 1);
     info->reserved = (int32_t)std::min<int64_t>(S->ndict, INT32_MAX);
     return BBPD_OK;
 }
