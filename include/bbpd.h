@@ -174,6 +174,23 @@ int bbpd_calculatedampingcoefficient(const double *nodalForce,
         const double *nodalVelocityPreviousHalf, const double *nodalDisplacement,
         int64_t nNodes, double *cn);
 
+/* No counterpart in the reference. The damping coefficient above without any
+ * device allocation, for callers that must not allocate device memory per call
+ * (a time loop that has handed the device's memory to its own fixed pool, or
+ * one held to a fixed HBM budget, where a per-step allocation could fail or grow
+ * the pool mid-run). Same sums in the same tree order; the result is written to
+ * *cn in DEVICE memory (one double), stream-ordered, with no host
+ * synchronisation. Scratch is a fixed 256 KiB array per device inside the
+ * library, so nNodes <= BBPD_DAMPING_NOALLOC_MAX_NODES (larger: BBPD_ERR_ARG).
+ * The first call on each device looks up that array's address: make it before
+ * any stream capture. Nothing needs zeroing beforehand. Calls that overlap on
+ * one device (unordered streams or host threads) race on the shared scratch. */
+#define BBPD_DAMPING_NOALLOC_MAX_NODES 16777216
+int bbpd_dev_calculatedampingcoefficient_noalloc(const double *nodalForce,
+        const double *massVector, const double *nodalForcePrevious, double DT,
+        const double *nodalVelocityPreviousHalf, const double *nodalDisplacement,
+        int64_t nNodes, double *cn, void *stream);
+
 /* Free the device mirrors and cached plan of the host-pointer entry points
  * (the gateways register it with mexAtExit). */
 int bbpd_release_mirrors(void);
