@@ -104,7 +104,8 @@ struct Dev {
     const DictEntry *dict;
     const float *dict32;             // BONDSTIFFNESS * cellVolume * VCF per dictionary entry (FP32 form)
     const float4 *dictx;             // FP32 form, 2 per entry: (xi_x, xi_y, xi_z, L0), (k32, |xi|^2-L0^2, regular, 0)
-    float4 *ur0, *ur1;               // FP32 form: per node (uh, ul) FP32 split of the displacement, 32 B, ping-pong like positions
+    float4 *urh0, *urh1;             // FP32 form: per node (uh_x, uh_y, uh_z, ul_x), ping-pong like positions
+    float2 *url0, *url1;             // FP32 form: per node (ul_y, ul_z); uh + ul is the FP32 split of u
     const double *s0e, *s1e, *sce;   // per-entry law stretches or null
     const double *X;
     double *xb0, *xb1;               // positions: step n reads xb[(n-1)&1], writes xb[n&1]
@@ -120,8 +121,8 @@ struct Dev {
     int n_levels;
     double *scal;                    // [0] = cn
     unsigned *bar;                   // [0] arrivals, [1] generation
+    unsigned long long *work;        // slice counter of phase A, zeroed before each launch
     unsigned *sticky;                // bit 0: a coordinate left the range of the fast division
-    const int64_t *wrange;           // slices [wrange[w], wrange[w+1]) belong to warp w
     int *err;
     LawScalars P;
     double V, dt, damping;
@@ -223,6 +224,15 @@ __device__ void tree_publish(const Dev &d, int64_t sl, int lane, double c1, doub
         L++;
         idx = g;
     }
+}
+
+// Next slice for this warp from the phase-A counter (lane 0 takes it, all
+// lanes receive it).
+__device__ __forceinline__ int64_t grab_slice(const Dev &d, int lane)
+{
+    unsigned long long v = 0;
+    if (lane == 0) v = atomicAdd(d.work, 1ull);
+    return (int64_t)__shfl_sync(0xffffffffu, v, 0);
 }
 
 // Grid-wide barrier with a time limit. False on timeout.
@@ -520,11 +530,10 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
     tx = tx + ax; ty = ty + ay; tz = tz + az;
 }
 
-// General path of the FP32 dictionary-vector form, out of line so that the
-// fast path keeps its registers: FP64 positions of both nodes, then the
-// general entry in difference form.
+// General path of the FP32 dictionary-vector form: FP64 positions of both
+// nodes, then the general entry in difference form.
 template <int LAW>
-__device__ __noinline__ double3 entry_general_x(const Dev &d, int64_t e, uint32_t w, uint32_t sv,
+__device__ __forceinline__ double3 entry_general_x(const Dev &d, int64_t e, uint32_t w, uint32_t sv,
                                                 uint32_t c, double scd, int64_t i, const double *xs)
 {
     const int64_t nN = d.n_nodes;
@@ -535,9 +544,10 @@ __device__ __noinline__ double3 entry_general_x(const Dev &d, int64_t e, uint32_
 
 // FP32 form, dictionary bond vectors (kP32X). Lane `lane` owns node sl*32+lane.
 // The deformed bond vector is e = xi + eta: xi = X_j - X_i from the dictionary
-// (FP32), eta = (uh_j - uh_i) + (ul_j - ul_i) from a 32-byte record per node
-// holding the displacement split into FP32 high and low parts (one sector per
-// gather; eta keeps close to FP64 accuracy under rigid translation), and
+// (FP32), eta = (uh_j - uh_i) + (ul_j - ul_i) from the displacement split into
+// FP32 high and low parts, stored as a 16-byte and an 8-byte array per node so
+// that a warp's gathers of consecutive nodes read whole sectors (eta keeps close
+// to FP64 accuracy under rigid translation), and
 //   L^2 - L0^2 = eta . (2 xi + eta) + (|xi|^2 - L0^2),  s = (L^2 - L0^2) / (L0 (L + L0))
 // is computed without cancellation; force = BS V VCF s e / L in FP32, summed in
 // FP64 in the reference's order. Bonds whose stretch lies within the guard band
@@ -545,15 +555,17 @@ __device__ __noinline__ double3 entry_general_x(const Dev &d, int64_t e, uint32_
 // take the general path with FP64 positions.
 template <int LAW, class CID, bool SCE>
 __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lane, const double *xs,
-                                               const float4 *ur, double &tx, double &ty, double &tz)
+                                               const float4 *urh, const float2 *url, double &tx,
+                                               double &ty, double &tz)
 {
     const int64_t nN = d.n_nodes;
     const int64_t i = sl * 32 + lane;
     const int dg = (i < nN) ? d.deg[i] : 0;
     const int64_t sb = d.slice_ptr[sl];
 
-    float4 ui = make_float4(0.f, 0.f, 0.f, 0.f), li = ui;
-    if (i < nN) { ui = ur[2 * i]; li = ur[2 * i + 1]; }
+    float4 ui = make_float4(0.f, 0.f, 0.f, 0.f);
+    float2 li = make_float2(0.f, 0.f);
+    if (i < nN) { ui = urh[i]; li = url[i]; }
     tx = 0.0; ty = 0.0; tz = 0.0;
     double ax = 0.0, ay = 0.0, az = 0.0;
     const float s0f = (float)d.P.s0, guardf = (float)d.guard;
@@ -565,13 +577,14 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
     for (int g = 0; g < ng; g++, e0 += 128) {
         if (g + 1 < ng) load_group<CID>(d, e0 + 128, Gn);
         const int nq = min(4, dg - 4 * g);
-        float4 uj[4], lj[4];
+        float4 uj[4];
+        float2 lj[4];
 #pragma unroll
         for (int q = 0; q < 4; q++)
             if (q < nq) {
                 const uint32_t j = group_w(Gc, q) & COL_MASK;
-                uj[q] = ur[2 * j];
-                lj[q] = ur[2 * j + 1];
+                uj[q] = urh[j];
+                lj[q] = url[j];
             }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
@@ -581,9 +594,9 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
                 const double scd = SCE ? __ldcs(d.sce + e) : d.P.sc;
                 const int bt = (w >> BT_SHIFT) & 3;
                 const float4 A = __ldg(&d.dictx[2 * c]), Bv = __ldg(&d.dictx[2 * c + 1]);
-                const float etx = (uj[q].x - ui.x) + (lj[q].x - li.x);
-                const float ety = (uj[q].y - ui.y) + (lj[q].y - li.y);
-                const float etz = (uj[q].z - ui.z) + (lj[q].z - li.z);
+                const float etx = (uj[q].x - ui.x) + (uj[q].w - ui.w);
+                const float ety = (uj[q].y - ui.y) + (lj[q].x - li.x);
+                const float etz = (uj[q].z - ui.z) + (lj[q].y - li.y);
                 const float ex = A.x + etx, ey = A.y + ety, ez = A.z + etz;
                 const float L2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
                 const float rL = rsqrtf(L2);
@@ -630,9 +643,8 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
 {
     const int lane = threadIdx.x & 31;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nN = d.n_nodes;
-    // contiguous slice range of this warp, balanced by entry count on the host
-    const int64_t sl0 = d.wrange[gwarp], sl1 = d.wrange[gwarp + 1];
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nN = d.n_nodes, nsl = d.n_slices;
 
     for (int64_t it = 0; it < nsteps; it++) {
         const int64_t n = step0 + it;
@@ -640,17 +652,27 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
         const double *Fp = (n & 1) ? d.F0 : d.F1;
         const double *xs = ((n - 1) & 1) ? d.xb1 : d.xb0;
         double *xn = (n & 1) ? d.xb1 : d.xb0;
-        const float4 *urs = ((n - 1) & 1) ? d.ur1 : d.ur0;
-        float4 *urn = (n & 1) ? d.ur1 : d.ur0;
+        const float4 *urhs = ((n - 1) & 1) ? d.urh1 : d.urh0;
+        const float2 *urls = ((n - 1) & 1) ? d.url1 : d.url0;
+        float4 *urhn = (n & 1) ? d.urh1 : d.urh0;
+        float2 *urln = (n & 1) ? d.url1 : d.url0;
         const double Un1 = prescribed_value(d, n + 1);
         const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
 
         // ---- phase A: bond forces (+ Euler-Cromer / ADR terms) ----
-        for (int64_t sl = sl0; sl < sl1; sl++) {
+        // Warps take slices from a shared counter, so warps that finish early
+        // take more. Each warp stops at its first grab past the last slice,
+        // so a step uses exactly nsl + nwarps counter values and the base of
+        // step `it` of this launch is it * (nsl + nwarps). Results depend on
+        // slice indices only, not on which warp computes a slice.
+        const int64_t base = it * (nsl + nwarps);
+        int64_t sl = grab_slice(d, lane) - base;
+        while (sl < nsl) {
+            const int64_t sl_next = grab_slice(d, lane) - base;
             const int64_t i = sl * 32 + lane;
             const bool valid = i < nN;
             double tx, ty, tz;
-            if (PREC == kP32X) slice_forces_x<LAW, CID, SCE>(d, sl, lane, xs, urs, tx, ty, tz);
+            if (PREC == kP32X) slice_forces_x<LAW, CID, SCE>(d, sl, lane, xs, urhs, urls, tx, ty, tz);
             else slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, xs, tx, ty, tz);
             if (SCHEME == BBPD_SCHEME_EULERCROMER) {
                 if (valid) {
@@ -676,8 +698,8 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
                         far |= coord_out_of_range(xe);
                     }
                     if (PREC == kP32X) {
-                        urn[2 * i] = make_float4(uh[0], uh[1], uh[2], 0.f);
-                        urn[2 * i + 1] = make_float4(ul[0], ul[1], ul[2], 0.f);
+                        urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
+                        urln[i] = make_float2(ul[1], ul[2]);
                     }
                     if (bad) atomicOr(d.err, ERR_NONFINITE);
                     if (far) atomicOr(d.sticky, 1u);
@@ -709,13 +731,14 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
                 }
                 tree_publish(d, sl, lane, c1, c2);
             }
+            sl = sl_next;
         }
         if (SCHEME == BBPD_SCHEME_ADR) {
             if (!grid_barrier(d)) return;
             // ---- phase B: timeintegrationADR.m:168-197 ----
             const double cn = __ldcg(&d.scal[0]);
-            for (int64_t sl = sl0; sl < sl1; sl++) {
-                const int64_t i = sl * 32 + lane;
+            for (int64_t sb = gwarp; sb < nsl; sb += nwarps) {
+                const int64_t i = sb * 32 + lane;
                 if (i >= nN) continue;
                 const uint8_t fl = d.nflag[i];
                 const double minv = 1.0 / d.mass[i];
@@ -738,8 +761,8 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
                     far |= coord_out_of_range(xe);
                 }
                 if (PREC == kP32X) {
-                    urn[2 * i] = make_float4(uh[0], uh[1], uh[2], 0.f);
-                    urn[2 * i + 1] = make_float4(ul[0], ul[1], ul[2], 0.f);
+                    urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
+                    urln[i] = make_float2(ul[1], ul[2]);
                 }
                 if (bad) atomicOr(d.err, ERR_NONFINITE);
                 if (far) atomicOr(d.sticky, 1u);
@@ -905,27 +928,28 @@ DictEntry make_entry(double l0, double vcf, double bs)
     return e;
 }
 
-// Coordinates for which the shared-divisor division is exact: +0, or a
-// magnitude in [2^-100, 2^100].
-// Per-node FP32 (high, low) record of a node-major displacement array u
-// (x of node p at [p], y at [p + nN], z at [p + 2 nN]): [2p] = high parts,
-// [2p + 1] = low parts, matching what the kernels write after each step.
-std::vector<float4> split_record(const double *u, int64_t nN)
+// FP32 (high, low) split of a node-major displacement array u (x of node p
+// at [p], y at [p + nN], z at [p + 2 nN]) in the two per-node arrays the
+// kernels gather and write after each step: h[p] = (uh_x, uh_y, uh_z, ul_x),
+// l[p] = (ul_y, ul_z), uh = RN32(u), ul = RN32(u - uh).
+void split_record(const double *u, int64_t nN, std::vector<float4> &h, std::vector<float2> &l)
 {
-    std::vector<float4> r(2 * nN);
+    h.resize(nN);
+    l.resize(nN);
     for (int64_t p = 0; p < nN; p++) {
-        float h[3], l[3];
+        float hi[3], lo[3];
         for (int c = 0; c < 3; c++) {
             const double v = u[p + c * nN];
-            h[c] = (float)v;
-            l[c] = (float)(v - (double)h[c]);
+            hi[c] = (float)v;
+            lo[c] = (float)(v - (double)hi[c]);
         }
-        r[2 * p] = make_float4(h[0], h[1], h[2], 0.f);
-        r[2 * p + 1] = make_float4(l[0], l[1], l[2], 0.f);
+        h[p] = make_float4(hi[0], hi[1], hi[2], lo[0]);
+        l[p] = make_float2(lo[1], lo[2]);
     }
-    return r;
 }
 
+// Coordinates for which the shared-divisor division is exact: +0, or a
+// magnitude in [2^-100, 2^100].
 inline bool coord_safe(double x)
 {
     const double a = std::fabs(x);
@@ -1338,12 +1362,17 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     BBPD_CUDA_TRY(cudaMemset(d.bsf, 0, sizeof(double) * std::max<int64_t>(ne, 1)));
     TRY(S->put((DictEntry **)&d.dict, dict));
     d.dictx = nullptr;
-    d.ur0 = d.ur1 = nullptr;
+    d.urh0 = d.urh1 = nullptr;
+    d.url0 = d.url1 = nullptr;
     if (S->prec == kP32X) {
         TRY(S->put((float4 **)&d.dictx, dictx));
-        const std::vector<float4> ur = split_record(u0.data(), nN);
-        TRY(S->put(&d.ur0, ur));
-        TRY(S->put(&d.ur1, ur));
+        std::vector<float4> uh;
+        std::vector<float2> ul;
+        split_record(u0.data(), nN, uh, ul);
+        TRY(S->put(&d.urh0, uh));
+        TRY(S->put(&d.urh1, uh));
+        TRY(S->put(&d.url0, ul));
+        TRY(S->put(&d.url1, ul));
     }
     {
         std::vector<float> k32(dict.size());
@@ -1395,6 +1424,8 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     TRY(S->put(&d.scal, sc4));
     std::vector<unsigned> bar(2, 0u);
     TRY(S->put(&d.bar, bar));
+    std::vector<unsigned long long> work(1, 0ull);
+    TRY(S->put(&d.work, work));
     std::vector<int> err(1, 0);
     TRY(S->put(&d.err, err));
     std::vector<unsigned> sticky(1, 0u);
@@ -1435,23 +1466,6 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     if (occ < 1) return fail(BBPD_ERR_CUDA, "kernel cannot be resident");
     int64_t want = (ns * 32 + kBlock - 1) / kBlock;   // one warp per slice at most
     S->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * occ, want));
-    {
-        // contiguous slice ranges per warp with equal work: a slice costs its
-        // longest list (the warp's trip count) plus a few trips of node work
-        const int64_t nw = (int64_t)S->grid * (kBlock / 32);
-        std::vector<double> pre(ns + 1, 0.0);
-        for (int64_t s = 0; s < ns; s++) pre[s + 1] = pre[s] + (double)slen[s] + 4.0;
-        std::vector<int64_t> wr(nw + 1, 0);
-        int64_t s = 0;
-        for (int64_t w = 1; w < nw; w++) {
-            const double target = pre[ns] * (double)w / (double)nw;
-            while (s < ns && pre[s + 1] <= target) s++;
-            if (s < ns && target - pre[s] > pre[s + 1] - target) s++;  // nearer boundary
-            wr[w] = std::max(s, wr[w - 1]);
-        }
-        wr[nw] = ns;
-        TRY(S->put((int64_t **)&d.wrange, wr));
-    }
     BBPD_CUDA_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
     BBPD_CUDA_TRY(cudaEventCreate(&S->ev0));
     BBPD_CUDA_TRY(cudaEventCreate(&S->ev1));
@@ -1492,6 +1506,7 @@ extern "C" int bbpd_step_async(bbpd_solver *S, int64_t nsteps)
     BBPD_CUDA_TRY(cudaSetDevice(S->device));
     int64_t step0 = S->step;
     void *args[] = {(void *)&S->d, (void *)&step0, (void *)&nsteps};
+    BBPD_CUDA_TRY(cudaMemsetAsync(S->d.work, 0, sizeof(unsigned long long), S->stream));
     BBPD_CUDA_TRY(cudaEventRecord(S->ev0, S->stream));
     BBPD_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)S->kernel, dim3(S->grid), dim3(kBlock), args, 0, S->stream));
     BBPD_CUDA_TRY(cudaEventRecord(S->ev1, S->stream));
@@ -1600,9 +1615,13 @@ extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
         BBPD_CUDA_TRY(cudaMemcpy(dst, h.data(), sizeof(double) * 3 * nN, cudaMemcpyHostToDevice));
         if (field == BBPD_FIELD_DISPLACEMENT && S->prec == kP32X) {
             // the FP32 form gathers an FP32 record of the displacement
-            const std::vector<float4> ur = split_record(h.data(), nN);
-            BBPD_CUDA_TRY(cudaMemcpy(S->d.ur0, ur.data(), sizeof(float4) * 2 * nN, cudaMemcpyHostToDevice));
-            BBPD_CUDA_TRY(cudaMemcpy(S->d.ur1, ur.data(), sizeof(float4) * 2 * nN, cudaMemcpyHostToDevice));
+            std::vector<float4> uh;
+            std::vector<float2> ul;
+            split_record(h.data(), nN, uh, ul);
+            BBPD_CUDA_TRY(cudaMemcpy(S->d.urh0, uh.data(), sizeof(float4) * nN, cudaMemcpyHostToDevice));
+            BBPD_CUDA_TRY(cudaMemcpy(S->d.urh1, uh.data(), sizeof(float4) * nN, cudaMemcpyHostToDevice));
+            BBPD_CUDA_TRY(cudaMemcpy(S->d.url0, ul.data(), sizeof(float2) * nN, cudaMemcpyHostToDevice));
+            BBPD_CUDA_TRY(cudaMemcpy(S->d.url1, ul.data(), sizeof(float2) * nN, cudaMemcpyHostToDevice));
         }
         if (field == BBPD_FIELD_DEFORMED) {
             // both position buffers: the next step reads the one of its parity
@@ -1663,7 +1682,8 @@ extern "C" int bbpd_set_step(bbpd_solver *S, int64_t step, double cn)
     if (((step - S->step) & 1) != 0) {
         std::swap(S->d.F0, S->d.F1);
         std::swap(S->d.xb0, S->d.xb1);
-        std::swap(S->d.ur0, S->d.ur1);
+        std::swap(S->d.urh0, S->d.urh1);
+        std::swap(S->d.url0, S->d.url1);
     }
     S->step = step;
     S->cn = cn;
