@@ -2,12 +2,15 @@
 //
 // Layout in HBM (built on the host at bbpd_create):
 //   nodes   SoA float64 (x of all nodes, then y, then z), in input order or
-//           Morton order; one flags byte per node (held / prescribed DOFs).
+//           Morton order; one flags byte per node (held / prescribed DOFs). The
+//           FP32 form adds the displacement split into FP32 high and low parts
+//           (16 + 8 bytes per node).
 //   bonds   every undirected bond is stored twice, once in the list of each
 //           end node ("directed entries"). Lists keep bond order and are laid
-//           out as 32-node slices (SELL-32): entry k of the node in lane l of
-//           slice s sits at slice_ptr[s] + 32 k + l, so a warp walking its 32
-//           nodes' lists in step reads every per-entry stream coalesced.
+//           out as 32-node slices (SELL-32) in groups of 4: entries 4g..4g+3
+//           of the node in lane l of slice s sit contiguously at
+//           slice_ptr[s] + 4 (32 g + l), so one vector load gives a lane 4
+//           entries of a stream and a warp reads 32 such groups contiguously.
 //           Per entry, read every step:
 //             colw  u32  neighbour index (24 bits), chunk-start bit, BONDTYPE
 //             cid   u16  (u32 for irregular inputs) index into a dictionary of
@@ -18,10 +21,12 @@
 //           critical stretch (float64) when the law takes per-bond sc.
 //
 // One time step (a launch runs any number of steps):
-//   phase A  each warp takes a 32-node slice; each lane walks its node's
-//            entries with loads issued two entries ahead, computes stretch,
-//            law, damage and bond force, and sums the forces in the reference's
-//            OpenMP order (chunk partials in bond order, added in chunk order).
+//   phase A  warps take 32-node slices from a shared counter; each lane walks
+//            its node's entries a group of 4 at a time (the next group's
+//            streams load while the current group's neighbour gathers are in
+//            flight), computes stretch, law, damage and bond force, and sums the
+//            forces in the reference's OpenMP order (chunk partials in bond
+//            order, added in chunk order).
 //            Both copies of a bond see bit-identical stretch (the squared
 //            components do not depend on direction), so both copies of the
 //            damage state evolve identically: no atomics, no cross-warp traffic.
