@@ -76,6 +76,16 @@ constexpr int kBlock = 256;
 #endif
 constexpr int kMaxLevels = 8;     // 32-ary reduction tree over the slices
 
+// Tiled kernel: nodes per tile, and the local neighbour word of an entry
+// (12-bit index into the tile's staged nodes, chunk-start bit, BONDTYPE).
+constexpr int kTile = 512;
+constexpr int kTileSlices = kTile / 32;
+constexpr uint32_t TJ_MASK = 0x0FFFu;
+constexpr uint32_t TF_CHUNK = 1u << 12;
+constexpr int TBT_SHIFT = 13;
+constexpr int kTileCapMax = 4096;        // staged nodes per tile (12-bit local index)
+constexpr int kDictCache = 1024;         // dictionary entries kept in shared memory
+
 // Kernel precision variants. The FP32 form runs as kP32X when the bond vectors
 // compress into the dictionary and as kP32D (FP64 differences) otherwise.
 constexpr int kP64 = 0, kP32D = 1, kP32X = 2;
@@ -102,7 +112,13 @@ struct Dev {
     const int64_t *slice_ptr;
     const int32_t *deg;
     const int32_t *slice_len;        // longest list of each slice
-    const uint32_t *colw;
+    const uint32_t *colw;            // global-gather kernels: neighbour word per entry
+    const uint16_t *jw;              // tiled kernel: local neighbour word per entry
+    int64_t n_tiles;
+    const int64_t *halo_ptr;         // halo of tile t: halo[halo_ptr[t] .. halo_ptr[t+1])
+    const uint32_t *halo;            // device ids of the nodes outside a tile that it reads
+    int tile_cap;                    // largest tile + halo (staged nodes per block)
+    int ncache;                      // dictionary entries cached in shared memory
     const void *cid;
     uint8_t *st;
     double *bsf;
@@ -267,6 +283,18 @@ __device__ bool grid_barrier(const Dev &d)
     return s_ok != 0;
 }
 
+// L2 prefetch of one line: no register is written, so a warp can keep many
+// groups of its streams in flight ahead of the loads that consume them.
+__device__ __forceinline__ void prefetch_l2(const void *p)
+{
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+#ifndef BBPD_PREFETCH_GROUPS
+#define BBPD_PREFETCH_GROUPS 8   // groups of 4 entries prefetched ahead of the loads
+#endif
+constexpr int kPrefetch = BBPD_PREFETCH_GROUPS;
+
 __device__ __forceinline__ DictEntry ldg_dict(const DictEntry *t, uint32_t c)
 {
     const double2 *p = reinterpret_cast<const double2 *>(t + c);
@@ -327,6 +355,26 @@ __device__ __forceinline__ void load_group(const Dev &d, int64_t e0, Group<CID> 
     else
         G.c = __ldcs(reinterpret_cast<const uint4 *>(reinterpret_cast<const uint32_t *>(d.cid) + e0));
     G.s = __ldcs(reinterpret_cast<const uint32_t *>(d.st + e0));
+}
+
+template <class CID, bool SCE>
+__device__ __forceinline__ void prefetch_group(const Dev &d, int64_t e0)
+{
+    prefetch_l2(d.colw + e0);
+    prefetch_l2(reinterpret_cast<const CID *>(d.cid) + e0);
+    prefetch_l2(d.st + e0);
+    if (SCE) prefetch_l2(d.sce + e0);
+}
+
+// First groups of slice sl, prefetched before its turn (within the slice's
+// padded length).
+template <class CID, bool SCE>
+__device__ __forceinline__ void prefetch_slice_head(const Dev &d, int64_t sl, int lane)
+{
+    if (sl >= d.n_slices) return;
+    const int64_t sb = d.slice_ptr[sl];
+    const int ng = min(kPrefetch, d.slice_len[sl] >> 2);
+    for (int g = 0; g < ng; g++) prefetch_group<CID, SCE>(d, entry_pos(sb, 4 * g, lane));
 }
 
 // Critical stretch whose crossing breaks a bond under the brittle law
@@ -502,6 +550,7 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
     int64_t e0 = entry_pos(sb, 0, lane);
     if (ng > 0) load_group<CID>(d, e0, Gc);
     for (int g = 0; g < ng; g++, e0 += 128) {
+        if (g + kPrefetch < ng) prefetch_group<CID, SCE>(d, e0 + 128 * kPrefetch);
         if (g + 1 < ng) load_group<CID>(d, e0 + 128, Gn);
         const int nq = min(4, dg - 4 * g);
         double xj[4], yj[4], zj[4];
@@ -580,6 +629,7 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
     int64_t e0 = entry_pos(sb, 0, lane);
     if (ng > 0) load_group<CID>(d, e0, Gc);
     for (int g = 0; g < ng; g++, e0 += 128) {
+        if (g + kPrefetch < ng) prefetch_group<CID, SCE>(d, e0 + 128 * kPrefetch);
         if (g + 1 < ng) load_group<CID>(d, e0 + 128, Gn);
         const int nq = min(4, dg - 4 * g);
         float4 uj[4];
@@ -643,25 +693,158 @@ __device__ __forceinline__ bool coord_out_of_range(double x)
     return (a != 0 || signbit(x)) && !(a >= 0x1p-100 && a <= 0x1p100);
 }
 
+// Buffers of step n: forces of this and the previous step, positions read and
+// written (double-buffered), FP32 displacement split read and written, and the
+// prescribed displacement of step n + 1.
+struct StepBufs {
+    int64_t n;
+    double *Fc;
+    const double *Fp, *xs;
+    double *xn;
+    const float4 *urhs;
+    const float2 *urls;
+    float4 *urhn;
+    float2 *urln;
+    double Un1;
+};
+
+__device__ __forceinline__ StepBufs step_bufs(const Dev &d, int64_t n)
+{
+    StepBufs b;
+    b.n = n;
+    b.Fc = (n & 1) ? d.F1 : d.F0;
+    b.Fp = (n & 1) ? d.F0 : d.F1;
+    b.xs = ((n - 1) & 1) ? d.xb1 : d.xb0;
+    b.xn = (n & 1) ? d.xb1 : d.xb0;
+    b.urhs = ((n - 1) & 1) ? d.urh1 : d.urh0;
+    b.urls = ((n - 1) & 1) ? d.url1 : d.url0;
+    b.urhn = (n & 1) ? d.urh1 : d.urh0;
+    b.urln = (n & 1) ? d.url1 : d.url0;
+    b.Un1 = prescribed_value(d, n + 1);
+    return b;
+}
+
+// Work on one slice after its nodal forces (tx, ty, tz of lane's node) are
+// summed: Euler-Cromer integrates the node; ADR stores F, forms the node's
+// Rayleigh-quotient terms, folds them over the slice and enters the tree.
+template <int SCHEME, int PREC>
+__device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, int64_t sl, int lane,
+                                             double tx, double ty, double tz)
+{
+    const int64_t nN = d.n_nodes;
+    const int64_t i = sl * 32 + lane;
+    const bool valid = i < nN;
+    if (SCHEME == BBPD_SCHEME_EULERCROMER) {
+        if (valid) {
+            // timeintegrationeulercromerMex.c:33-50 on the node just summed
+            const uint8_t fl = d.nflag[i];
+            const double Fv[3] = {tx, ty, tz};
+            float uh[3], ul[3];
+            bool bad = false, far = false;
+#pragma unroll
+            for (int dof = 0; dof < 3; dof++) {
+                const int64_t e = i + nN * dof;
+                b.Fc[e] = Fv[dof];
+                double ae = (Fv[dof] - d.damping * d.v[e]) / d.rho[i];
+                if (fl & (1 << dof)) ae = 0;
+                double ve = d.v[e] + (ae * d.dt);
+                double ue = d.u[e] + (ve * d.dt);
+                double xe = d.X[e] + ue;
+                if (fl & (8 << dof)) { ue = b.Un1; xe = d.X[e] + ue; }
+                if (d.a) d.a[e] = ae;
+                d.v[e] = ve; d.u[e] = ue; b.xn[e] = xe;
+                uh[dof] = (float)ue; ul[dof] = (float)(ue - (double)uh[dof]);
+                bad |= !isfinite(ue) || !isfinite(ve);
+                far |= coord_out_of_range(xe);
+            }
+            if (PREC == kP32X) {
+                b.urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
+                b.urln[i] = make_float2(ul[1], ul[2]);
+            }
+            if (bad) atomicOr(d.err, ERR_NONFINITE);
+            if (far) atomicOr(d.sticky, 1u);
+        }
+    } else {
+        // calculatedampingcoefficient.m:61-85 terms of this node, then the
+        // xor butterfly over the slice's 32 lanes
+        double c1 = 0, c2 = 0;
+        if (valid) {
+            b.Fc[i] = tx; b.Fc[i + nN] = ty; b.Fc[i + 2 * nN] = tz;
+            const double m = d.mass[i];
+            const double Fv[3] = {tx, ty, tz};
+#pragma unroll
+            for (int dof = 0; dof < 3; dof++) {
+                const int64_t e = i + nN * dof;
+                const double vhp = d.v[e], ue = d.u[e];
+                if (vhp != 0) c1 = c1 - ue * ue * ((Fv[dof] / m - b.Fp[e] / m) / (d.dt * vhp));
+            }
+#pragma unroll
+            for (int dof = 0; dof < 3; dof++) {
+                const double ue = d.u[i + nN * dof];
+                c2 = c2 + ue * ue;
+            }
+        }
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
+            c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
+        }
+        tree_publish(d, sl, lane, c1, c2);
+    }
+}
+
+// ADR phase B (timeintegrationADR.m:168-197) on slices gwarp, gwarp + nwarps, ...
+template <int PREC>
+__device__ __forceinline__ void adr_update(const Dev &d, const StepBufs &b, int lane, int64_t gwarp,
+                                           int64_t nwarps)
+{
+    const int64_t nN = d.n_nodes, nsl = d.n_slices;
+    const double cn = __ldcg(&d.scal[0]);
+    for (int64_t sb = gwarp; sb < nsl; sb += nwarps) {
+        const int64_t i = sb * 32 + lane;
+        if (i >= nN) continue;
+        const uint8_t fl = d.nflag[i];
+        const double minv = 1.0 / d.mass[i];
+        float uh[3], ul[3];
+        bool bad = false, far = false;
+#pragma unroll
+        for (int dof = 0; dof < 3; dof++) {
+            const int64_t e = i + nN * dof;
+            const double F = b.Fc[e];
+            double vh;
+            if (b.n == 1) vh = 0.5 * d.dt * minv * F;
+            else vh = (((2 - cn * d.dt) * d.v[e]) + (2 * d.dt * minv * F)) / (2 + cn * d.dt);
+            double ue = d.u[e] + (d.dt * vh);
+            if (fl & (1 << dof)) { ue = 0; vh = 0; }
+            if (fl & (8 << dof)) { ue = b.Un1; vh = 0; }
+            const double xe = d.X[e] + ue;
+            d.v[e] = vh; d.u[e] = ue; b.xn[e] = xe;
+            uh[dof] = (float)ue; ul[dof] = (float)(ue - (double)uh[dof]);
+            bad |= !isfinite(ue) || !isfinite(vh);
+            far |= coord_out_of_range(xe);
+        }
+        if (PREC == kP32X) {
+            b.urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
+            b.urln[i] = make_float2(ul[1], ul[2]);
+        }
+        if (bad) atomicOr(d.err, ERR_NONFINITE);
+        if (far) atomicOr(d.sticky, 1u);
+    }
+}
+
+// Global-gather kernel: neighbour data read from HBM/L2 per entry. Used for
+// inputs whose tiles do not fit shared memory, and for input or plain Morton
+// node order.
 template <int LAW, int SCHEME, int PREC, class CID, bool SCE>
 __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : BBPD_MIN_BLOCKS) step_kernel(Dev d, int64_t step0, int64_t nsteps)
 {
     const int lane = threadIdx.x & 31;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t nN = d.n_nodes, nsl = d.n_slices;
+    const int64_t nsl = d.n_slices;
 
     for (int64_t it = 0; it < nsteps; it++) {
-        const int64_t n = step0 + it;
-        double *Fc = (n & 1) ? d.F1 : d.F0;
-        const double *Fp = (n & 1) ? d.F0 : d.F1;
-        const double *xs = ((n - 1) & 1) ? d.xb1 : d.xb0;
-        double *xn = (n & 1) ? d.xb1 : d.xb0;
-        const float4 *urhs = ((n - 1) & 1) ? d.urh1 : d.urh0;
-        const float2 *urls = ((n - 1) & 1) ? d.url1 : d.url0;
-        float4 *urhn = (n & 1) ? d.urh1 : d.urh0;
-        float2 *urln = (n & 1) ? d.url1 : d.url0;
-        const double Un1 = prescribed_value(d, n + 1);
+        const StepBufs b = step_bufs(d, step0 + it);
         const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
 
         // ---- phase A: bond forces (+ Euler-Cromer / ADR terms) ----
@@ -672,106 +855,294 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
         // slice indices only, not on which warp computes a slice.
         const int64_t base = it * (nsl + nwarps);
         int64_t sl = grab_slice(d, lane) - base;
+        prefetch_slice_head<CID, SCE>(d, sl, lane);
         while (sl < nsl) {
             const int64_t sl_next = grab_slice(d, lane) - base;
-            const int64_t i = sl * 32 + lane;
-            const bool valid = i < nN;
+            prefetch_slice_head<CID, SCE>(d, sl_next, lane);
             double tx, ty, tz;
-            if (PREC == kP32X) slice_forces_x<LAW, CID, SCE>(d, sl, lane, xs, urhs, urls, tx, ty, tz);
-            else slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, xs, tx, ty, tz);
-            if (SCHEME == BBPD_SCHEME_EULERCROMER) {
-                if (valid) {
-                    // timeintegrationeulercromerMex.c:33-50 on the node just summed
-                    const uint8_t fl = d.nflag[i];
-                    const double Fv[3] = {tx, ty, tz};
-                    float uh[3], ul[3];
-                    bool bad = false, far = false;
-#pragma unroll
-                    for (int dof = 0; dof < 3; dof++) {
-                        const int64_t e = i + nN * dof;
-                        Fc[e] = Fv[dof];
-                        double ae = (Fv[dof] - d.damping * d.v[e]) / d.rho[i];
-                        if (fl & (1 << dof)) ae = 0;
-                        double ve = d.v[e] + (ae * d.dt);
-                        double ue = d.u[e] + (ve * d.dt);
-                        double xe = d.X[e] + ue;
-                        if (fl & (8 << dof)) { ue = Un1; xe = d.X[e] + ue; }
-                        if (d.a) d.a[e] = ae;
-                        d.v[e] = ve; d.u[e] = ue; xn[e] = xe;
-                        uh[dof] = (float)ue; ul[dof] = (float)(ue - (double)uh[dof]);
-                        bad |= !isfinite(ue) || !isfinite(ve);
-                        far |= coord_out_of_range(xe);
-                    }
-                    if (PREC == kP32X) {
-                        urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
-                        urln[i] = make_float2(ul[1], ul[2]);
-                    }
-                    if (bad) atomicOr(d.err, ERR_NONFINITE);
-                    if (far) atomicOr(d.sticky, 1u);
-                }
-            } else {
-                // calculatedampingcoefficient.m:61-85 terms of this node, then the
-                // xor butterfly over the slice's 32 lanes
-                double c1 = 0, c2 = 0;
-                if (valid) {
-                    Fc[i] = tx; Fc[i + nN] = ty; Fc[i + 2 * nN] = tz;
-                    const double m = d.mass[i];
-                    const double Fv[3] = {tx, ty, tz};
-#pragma unroll
-                    for (int dof = 0; dof < 3; dof++) {
-                        const int64_t e = i + nN * dof;
-                        const double vhp = d.v[e], ue = d.u[e];
-                        if (vhp != 0) c1 = c1 - ue * ue * ((Fv[dof] / m - Fp[e] / m) / (d.dt * vhp));
-                    }
-#pragma unroll
-                    for (int dof = 0; dof < 3; dof++) {
-                        const double ue = d.u[i + nN * dof];
-                        c2 = c2 + ue * ue;
-                    }
-                }
-#pragma unroll
-                for (int off = 16; off >= 1; off >>= 1) {
-                    c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
-                    c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
-                }
-                tree_publish(d, sl, lane, c1, c2);
-            }
+            if (PREC == kP32X) slice_forces_x<LAW, CID, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
+            else slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, b.xs, tx, ty, tz);
+            finish_slice<SCHEME, PREC>(d, b, sl, lane, tx, ty, tz);
             sl = sl_next;
         }
         if (SCHEME == BBPD_SCHEME_ADR) {
             if (!grid_barrier(d)) return;
-            // ---- phase B: timeintegrationADR.m:168-197 ----
-            const double cn = __ldcg(&d.scal[0]);
-            for (int64_t sb = gwarp; sb < nsl; sb += nwarps) {
-                const int64_t i = sb * 32 + lane;
-                if (i >= nN) continue;
-                const uint8_t fl = d.nflag[i];
-                const double minv = 1.0 / d.mass[i];
-                float uh[3], ul[3];
-                bool bad = false, far = false;
+            adr_update<PREC>(d, b, lane, gwarp, nwarps);
+        }
+        if (!grid_barrier(d)) return;
+    }
+}
+
+// ---------------------------------------------------------------- tiled kernel
+//
+// Nodes in Morton order are cut into tiles of kTile consecutive nodes (16
+// slices; an 8 x 8 x 8 brick on a regular lattice). For every tile the host
+// lists the nodes outside it that its entries reference (its halo); entries
+// name their neighbour by a 12-bit index into [tile nodes, halo nodes]. A block
+// takes a tile, stages the positions (FP64 form) or the displacement split
+// (FP32 form) of the tile and its halo into shared memory with independent
+// loads, then its warps take the tile's slices and read every neighbour from
+// shared memory. The most used dictionary entries stay in shared memory for the
+// whole launch.
+
+// Streams of one group of 4 entries: local neighbour words, dictionary ids, states.
+struct TGroup {
+    uint2 j, c;
+    uint32_t s;
+    __device__ __forceinline__ uint32_t jw(int q) const
+    {
+        const uint32_t h = (q < 2) ? j.x : j.y;
+        return (q & 1) ? (h >> 16) : (h & 0xFFFFu);
+    }
+    __device__ __forceinline__ uint32_t cid(int q) const
+    {
+        const uint32_t h = (q < 2) ? c.x : c.y;
+        return (q & 1) ? (h >> 16) : (h & 0xFFFFu);
+    }
+};
+
+template <bool SCE>
+__device__ __forceinline__ void prefetch_tgroup(const Dev &d, int64_t e0)
+{
+    prefetch_l2(d.jw + e0);
+    prefetch_l2(reinterpret_cast<const uint16_t *>(d.cid) + e0);
+    prefetch_l2(d.st + e0);
+    if (SCE) prefetch_l2(d.sce + e0);
+}
+
+template <bool SCE>
+__device__ __forceinline__ void prefetch_tslice_head(const Dev &d, int64_t sl, int lane)
+{
+    const int64_t sb = d.slice_ptr[sl];
+    const int ng = min(kPrefetch, d.slice_len[sl] >> 2);
+    for (int g = 0; g < ng; g++) prefetch_tgroup<SCE>(d, entry_pos(sb, 4 * g, lane));
+}
+
+__device__ __forceinline__ void load_tgroup(const Dev &d, int64_t e0, TGroup &G)
+{
+    G.j = __ldcs(reinterpret_cast<const uint2 *>(d.jw + e0));
+    G.c = __ldcs(reinterpret_cast<const uint2 *>(reinterpret_cast<const uint16_t *>(d.cid) + e0));
+    G.s = __ldcs(reinterpret_cast<const uint32_t *>(d.st + e0));
+}
+
+// Bond-type bits of a local neighbour word, placed where entry_force and
+// entry_general expect them.
+__device__ __forceinline__ uint32_t tword(uint32_t jw)
+{
+    return ((jw >> TBT_SHIFT) & 3u) << BT_SHIFT;
+}
+
+// FP64 form: forces of the 32 nodes of slice sl, lane's node at local index li.
+template <int LAW, bool SCE>
+__device__ __forceinline__ void tslice_forces(const Dev &d, int64_t sl, int li, int lane, bool safe,
+                                              const double *sx, const double *sy, const double *sz,
+                                              const DictEntry *sdict, int ncache, double &tx,
+                                              double &ty, double &tz)
+{
+    const int64_t i = sl * 32 + lane;
+    const int dg = (i < d.n_nodes) ? d.deg[i] : 0;
+    const int64_t sb = d.slice_ptr[sl];
+    double xi = 0, yi = 0, zi = 0;
+    if (dg > 0) { xi = sx[li]; yi = sy[li]; zi = sz[li]; }
+    tx = 0.0; ty = 0.0; tz = 0.0;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    const int ng = (dg + 3) >> 2;
+    TGroup Gc, Gn;
+    int64_t e0 = entry_pos(sb, 0, lane);
+    if (ng > 0) load_tgroup(d, e0, Gc);
+    for (int g = 0; g < ng; g++, e0 += 128) {
+        if (g + kPrefetch < ng) prefetch_tgroup<SCE>(d, e0 + 128 * kPrefetch);
+        if (g + 1 < ng) load_tgroup(d, e0 + 128, Gn);
+        const int nq = min(4, dg - 4 * g);
 #pragma unroll
-                for (int dof = 0; dof < 3; dof++) {
-                    const int64_t e = i + nN * dof;
-                    const double F = Fc[e];
-                    double vh;
-                    if (n == 1) vh = 0.5 * d.dt * minv * F;
-                    else vh = (((2 - cn * d.dt) * d.v[e]) + (2 * d.dt * minv * F)) / (2 + cn * d.dt);
-                    double ue = d.u[e] + (d.dt * vh);
-                    if (fl & (1 << dof)) { ue = 0; vh = 0; }
-                    if (fl & (8 << dof)) { ue = Un1; vh = 0; }
-                    const double xe = d.X[e] + ue;
-                    d.v[e] = vh; d.u[e] = ue; xn[e] = xe;
-                    uh[dof] = (float)ue; ul[dof] = (float)(ue - (double)uh[dof]);
-                    bad |= !isfinite(ue) || !isfinite(vh);
-                    far |= coord_out_of_range(xe);
+        for (int q = 0; q < 4; q++) {
+            if (q < nq) {
+                const uint32_t jw = Gc.jw(q), jl = jw & TJ_MASK;
+                Fetch f;
+                f.w = tword(jw);
+                f.c = Gc.cid(q);
+                f.sv = (Gc.s >> (8 * q)) & 0xFFu;
+                f.sc = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
+                f.xj = sx[jl]; f.yj = sy[jl]; f.zj = sz[jl];
+                f.g = ((int)f.c < ncache) ? sdict[f.c] : ldg_dict(d.dict, f.c);
+                const double3 r = entry_force<LAW, kP64>(d, e0 + q, f, safe, xi, yi, zi);
+                if (jw & TF_CHUNK) {  // partial of the previous OpenMP thread is complete
+                    tx = tx + ax; ty = ty + ay; tz = tz + az;
+                    ax = 0.0; ay = 0.0; az = 0.0;
                 }
-                if (PREC == kP32X) {
-                    urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
-                    urln[i] = make_float2(ul[1], ul[2]);
-                }
-                if (bad) atomicOr(d.err, ERR_NONFINITE);
-                if (far) atomicOr(d.sticky, 1u);
+                ax = ax + r.x; ay = ay + r.y; az = az + r.z;
             }
+        }
+        Gc = Gn;
+    }
+    tx = tx + ax; ty = ty + ay; tz = tz + az;
+}
+
+// FP32 dictionary-vector form on staged displacement splits (see slice_forces_x
+// for the arithmetic). Neighbours outside the fast path read FP64 positions
+// from HBM through the tile's halo list.
+template <int LAW, bool SCE>
+__device__ __forceinline__ void tslice_forces_x(const Dev &d, int64_t sl, int li, int lane,
+                                                int64_t n0, int nt, int64_t hp,
+                                                const float4 *suh, const float2 *sul,
+                                                const float4 *sdx, int ncache, const double *xs,
+                                                double &tx, double &ty, double &tz)
+{
+    const int64_t nN = d.n_nodes;
+    const int64_t i = sl * 32 + lane;
+    const int dg = (i < nN) ? d.deg[i] : 0;
+    const int64_t sb = d.slice_ptr[sl];
+    float4 ui = make_float4(0.f, 0.f, 0.f, 0.f);
+    float2 vi = make_float2(0.f, 0.f);
+    if (dg > 0) { ui = suh[li]; vi = sul[li]; }
+    tx = 0.0; ty = 0.0; tz = 0.0;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    const float s0f = (float)d.P.s0, guardf = (float)d.guard;
+    const int ng = (dg + 3) >> 2;
+    TGroup Gc, Gn;
+    int64_t e0 = entry_pos(sb, 0, lane);
+    if (ng > 0) load_tgroup(d, e0, Gc);
+    for (int g = 0; g < ng; g++, e0 += 128) {
+        if (g + kPrefetch < ng) prefetch_tgroup<SCE>(d, e0 + 128 * kPrefetch);
+        if (g + 1 < ng) load_tgroup(d, e0 + 128, Gn);
+        const int nq = min(4, dg - 4 * g);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (q < nq) {
+                const int64_t e = e0 + q;
+                const uint32_t jw = Gc.jw(q), jl = jw & TJ_MASK, c = Gc.cid(q);
+                const uint32_t sv = (Gc.s >> (8 * q)) & 0xFFu, w = tword(jw);
+                const double scd = SCE ? __ldcs(d.sce + e) : d.P.sc;
+                const int bt = (w >> BT_SHIFT) & 3;
+                const bool hit = (int)c < ncache;
+                const float4 A = hit ? sdx[2 * c] : __ldg(&d.dictx[2 * c]);
+                const float4 Bv = hit ? sdx[2 * c + 1] : __ldg(&d.dictx[2 * c + 1]);
+                const float4 uj = suh[jl];
+                const float2 vj = sul[jl];
+                const float etx = (uj.x - ui.x) + (uj.w - ui.w);
+                const float ety = (uj.y - ui.y) + (vj.x - vi.x);
+                const float etz = (uj.z - ui.z) + (vj.y - vi.y);
+                const float ex = A.x + etx, ey = A.y + ety, ez = A.z + etz;
+                const float L2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
+                const float rL = rsqrtf(L2);
+                const float L = L2 * rL;
+                const float num = __fmaf_rn(etz, A.z + ez, __fmaf_rn(ety, A.y + ey, __fmaf_rn(etx, A.x + ex, Bv.y)));
+                const float sf = __fdividef(num, A.w * (L + A.w));
+                const float crit = (float)((LAW == BBPD_LAW_LINEAR) ? linear_crit(d.P, bt, scd) : scd);
+                const float s0b = d.s0e ? (float)__ldg(d.s0e + e) : s0f;
+                const bool quiet = (LAW == BBPD_LAW_LINEAR) ? !(sf > crit) : !(bt == 0 && sf > s0b);
+                double3 r;
+                if (sv == 0 && Bv.z != 0.f && L2 > 0.f && L2 < INFINITY && !(fabsf(sf - crit) < guardf) && quiet) {
+                    const float qf = Bv.x * sf * rL;
+                    r.x = (double)(qf * ex);
+                    r.y = (double)(qf * ey);
+                    r.z = (double)(qf * ez);
+                } else {
+                    const int64_t gj = ((int)jl < nt) ? n0 + jl : (int64_t)d.halo[hp + jl - nt];
+                    r = entry_general<LAW, kP32D>(d, e, w, sv, ldg_dict(d.dict, c), scd, xs[i], xs[i + nN],
+                                                  xs[i + 2 * nN], xs[gj], xs[gj + nN], xs[gj + 2 * nN]);
+                }
+                if (jw & TF_CHUNK) {  // partial of the previous OpenMP thread is complete
+                    tx = tx + ax; ty = ty + ay; tz = tz + az;
+                    ax = 0.0; ay = 0.0; az = 0.0;
+                }
+                ax = ax + r.x; ay = ay + r.y; az = az + r.z;
+            }
+        }
+        Gc = Gn;
+    }
+    tx = tx + ax; ty = ty + ay; tz = tz + az;
+}
+
+// Dynamic shared memory of the tiled kernel: the dictionary cache (ncache
+// entries of 32 bytes) followed by the staged node data of one tile (tile_cap
+// nodes of 24 bytes: x, y, z in FP64, or the FP32 split as float4 + float2).
+template <int LAW, int SCHEME, int PREC, bool SCE>
+__global__ void __launch_bounds__(kBlock, 2) tstep_kernel(Dev d, int64_t step0, int64_t nsteps)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int64_t s_tile;
+    __shared__ int s_next;
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nN = d.n_nodes, ntiles = d.n_tiles;
+    const int ncache = d.ncache, cap = d.tile_cap;
+
+    DictEntry *sdict = reinterpret_cast<DictEntry *>(smem);
+    float4 *sdx = reinterpret_cast<float4 *>(smem);
+    unsigned char *stage = smem + (size_t)32 * ncache;
+    double *sx = reinterpret_cast<double *>(stage), *sy = sx + cap, *sz = sy + cap;
+    float4 *suh = reinterpret_cast<float4 *>(stage);
+    float2 *sul = reinterpret_cast<float2 *>(suh + cap);
+
+    for (int c = threadIdx.x; c < ncache; c += blockDim.x) {
+        if (PREC == kP32X) {
+            sdx[2 * c] = __ldg(&d.dictx[2 * c]);
+            sdx[2 * c + 1] = __ldg(&d.dictx[2 * c + 1]);
+        } else {
+            sdict[c] = ldg_dict(d.dict, c);
+        }
+    }
+
+    for (int64_t it = 0; it < nsteps; it++) {
+        const StepBufs b = step_bufs(d, step0 + it);
+        const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
+        // Blocks take tiles from a shared counter; each block stops at its
+        // first grab past the last tile, so a step uses exactly
+        // ntiles + gridDim.x counter values.
+        const int64_t base = it * (ntiles + gridDim.x);
+        for (;;) {
+            if (threadIdx.x == 0) {
+                s_tile = (int64_t)atomicAdd(d.work, 1ull) - base;
+                s_next = 0;
+            }
+            __syncthreads();
+            const int64_t tile = s_tile;
+            if (tile >= ntiles) break;
+            const int64_t n0 = tile * kTile;
+            const int nt = (int)min((int64_t)kTile, nN - n0);
+            const int64_t hp = d.halo_ptr[tile];
+            const int nloc = nt + (int)(d.halo_ptr[tile + 1] - hp);
+            {
+                const int w = threadIdx.x >> 5;
+                if (w * 32 < nt) prefetch_tslice_head<SCE>(d, tile * kTileSlices + w, lane);
+            }
+            for (int l = threadIdx.x; l < nloc; l += blockDim.x) {
+                const int64_t g = (l < nt) ? n0 + l : (int64_t)d.halo[hp + l - nt];
+                if (PREC == kP32X) {
+                    suh[l] = b.urhs[g];
+                    sul[l] = b.urls[g];
+                } else {
+                    sx[l] = b.xs[g];
+                    sy[l] = b.xs[g + nN];
+                    sz[l] = b.xs[g + 2 * nN];
+                }
+            }
+            __syncthreads();
+            const int nslt = (nt + 31) / 32;
+            const int nwb = blockDim.x >> 5;
+            for (;;) {
+                int k = 0;
+                if (lane == 0) k = atomicAdd(&s_next, 1);
+                k = __shfl_sync(0xffffffffu, k, 0);
+                if (k >= nslt) break;
+                const int64_t sl = tile * kTileSlices + k;
+                if (k + nwb < nslt) prefetch_tslice_head<SCE>(d, sl + nwb, lane);
+                double tx, ty, tz;
+                if (PREC == kP32X)
+                    tslice_forces_x<LAW, SCE>(d, sl, k * 32 + lane, lane, n0, nt, hp, suh, sul, sdx, ncache,
+                                              b.xs, tx, ty, tz);
+                else
+                    tslice_forces<LAW, SCE>(d, sl, k * 32 + lane, lane, safe, sx, sy, sz, sdict, ncache,
+                                            tx, ty, tz);
+                finish_slice<SCHEME, PREC>(d, b, sl, lane, tx, ty, tz);
+            }
+            __syncthreads();
+        }
+        if (SCHEME == BBPD_SCHEME_ADR) {
+            if (!grid_barrier(d)) return;
+            adr_update<PREC>(d, b, lane, gwarp, nwarps);
         }
         if (!grid_barrier(d)) return;
     }
@@ -811,6 +1182,31 @@ kernel_t pick_scheme(int scheme, int prec, bool wide, bool sce)
 {
     return scheme == BBPD_SCHEME_ADR ? pick_prec<LAW, BBPD_SCHEME_ADR>(prec, wide, sce)
                                      : pick_prec<LAW, BBPD_SCHEME_EULERCROMER>(prec, wide, sce);
+}
+
+template <int LAW, int SCHEME>
+kernel_t pick_tprec(int prec, bool sce)
+{
+    if (prec == kP32X) return sce ? tstep_kernel<LAW, SCHEME, kP32X, true> : tstep_kernel<LAW, SCHEME, kP32X, false>;
+    return sce ? tstep_kernel<LAW, SCHEME, kP64, true> : tstep_kernel<LAW, SCHEME, kP64, false>;
+}
+
+template <int LAW>
+kernel_t pick_tscheme(int scheme, int prec, bool sce)
+{
+    return scheme == BBPD_SCHEME_ADR ? pick_tprec<LAW, BBPD_SCHEME_ADR>(prec, sce)
+                                     : pick_tprec<LAW, BBPD_SCHEME_EULERCROMER>(prec, sce);
+}
+
+// Tiled kernels: 16-bit dictionary ids, FP64 or FP32 dictionary-vector form.
+kernel_t pick_tkernel(int law, int scheme, int prec, bool sce)
+{
+    switch (law) {
+    case BBPD_LAW_LINEAR: return pick_tscheme<BBPD_LAW_LINEAR>(scheme, prec, sce);
+    case BBPD_LAW_BILINEAR: return pick_tscheme<BBPD_LAW_BILINEAR>(scheme, prec, sce);
+    case BBPD_LAW_TRILINEAR: return pick_tscheme<BBPD_LAW_TRILINEAR>(scheme, prec, sce);
+    default: return pick_tscheme<BBPD_LAW_EXPONENTIAL>(scheme, prec, sce);
+    }
 }
 
 kernel_t pick_kernel(int law, int scheme, int prec, bool wide, bool sce)
@@ -987,6 +1383,8 @@ struct bbpd_solver {
     double bytes_per_step = 0;
     kernel_t kernel = nullptr;
     int grid = 0;
+    bool tiled = false;                 // tiled kernel with shared-memory staging
+    size_t smem = 0;                    // its dynamic shared memory per block
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -1087,19 +1485,31 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     S->perm.resize(nN);
     S->inv.resize(nN);
     std::iota(S->perm.begin(), S->perm.end(), 0);
-    if (prm->node_order == BBPD_ORDER_MORTON) {
+    if (prm->node_order == BBPD_ORDER_MORTON || prm->node_order == BBPD_ORDER_TILED) {
         const double *X = pb->undeformed_coordinates;
         double lo[3], hi[3];
         for (int c = 0; c < 3; c++) {
             lo[c] = *std::min_element(X + c * nN, X + (c + 1) * nN);
             hi[c] = *std::max_element(X + c * nN, X + (c + 1) * nN);
         }
+        // Quantize on the shortest bond length when that resolves the domain
+        // in 21 bits per axis: a regular lattice then maps to its integer
+        // indices and aligned Morton blocks are exact bricks (a 512-node tile
+        // is an 8 x 8 x 8 brick). Otherwise scale each axis to 21 bits.
+        double h = 0;
+        for (int64_t k = 0; k < nB; k++) {
+            const double l = pb->undeformed_length[k];
+            if (l > 0 && std::isfinite(l) && (h == 0 || l < h)) h = l;
+        }
+        bool lattice = h > 0;
+        for (int c = 0; c < 3 && lattice; c++) lattice = (hi[c] - lo[c]) / h < 2097000.0;
         std::vector<uint64_t> key(nN);
         for (int64_t i = 0; i < nN; i++) {
             uint32_t q[3];
             for (int c = 0; c < 3; c++) {
-                double span = hi[c] - lo[c];
-                q[c] = span > 0 ? (uint32_t)((X[i + c * nN] - lo[c]) / span * 2097151.0) : 0;
+                const double span = hi[c] - lo[c];
+                if (lattice) q[c] = (uint32_t)std::floor((X[i + c * nN] - lo[c]) / h + 0.5);
+                else q[c] = span > 0 ? (uint32_t)((X[i + c * nN] - lo[c]) / span * 2097151.0) : 0;
             }
             key[i] = morton3(q[0], q[1], q[2]);
         }
@@ -1314,6 +1724,94 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     std::vector<int32_t>().swap(bond_of);
     cnt.clear();
 
+    // Tiles for the tiled kernel: per tile the sorted list of outside nodes its
+    // entries read, and per entry a 12-bit index into [tile nodes, halo].
+    std::vector<uint16_t> jw;
+    std::vector<int64_t> hptr;
+    std::vector<uint32_t> halo;
+    int tile_cap = 0;
+    if (prm->node_order == BBPD_ORDER_TILED && !S->wide && S->prec != kP32D) {
+        const int64_t ntiles = (nN + kTile - 1) / kTile;
+        std::vector<std::vector<uint32_t>> hl(ntiles);
+        std::vector<int> over(HT, 0), capt(HT, 0);
+        host_ranges(ntiles, HT, [&](int th, int64_t lo, int64_t hi) {
+            for (int64_t t = lo; t < hi; t++) {
+                const int64_t n0 = t * kTile, n1 = std::min(nN, n0 + kTile);
+                std::vector<uint32_t> &h = hl[t];
+                for (int64_t me = n0; me < n1; me++)
+                    for (int32_t r = 0; r < deg[me]; r++) {
+                        const uint32_t j = colw[entry_pos(sptr[me / 32], r, (int)(me % 32))] & COL_MASK;
+                        if ((int64_t)j < n0 || (int64_t)j >= n1) h.push_back(j);
+                    }
+                std::sort(h.begin(), h.end());
+                h.erase(std::unique(h.begin(), h.end()), h.end());
+                const int loc = (int)(n1 - n0) + (int)h.size();
+                if (loc > kTileCapMax) over[th] = 1;
+                capt[th] = std::max(capt[th], loc);
+            }
+        });
+        bool fits = true;
+        for (int th = 0; th < HT; th++) {
+            fits = fits && !over[th];
+            tile_cap = std::max(tile_cap, capt[th]);
+        }
+        tile_cap = (tile_cap + 31) & ~31;
+        int optin = 0;
+        BBPD_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+        const int ncache = (int)std::min<int64_t>(kDictCache, (int64_t)dict.size());
+        const size_t smem = (size_t)32 * ncache + (size_t)24 * tile_cap;
+        if (fits && smem <= (size_t)optin) {
+            S->tiled = true;
+            S->smem = smem;
+            jw.assign(ne, 0);
+            hptr.assign(ntiles + 1, 0);
+            for (int64_t t = 0; t < ntiles; t++) hptr[t + 1] = hptr[t] + (int64_t)hl[t].size();
+            halo.resize(hptr[ntiles]);
+            host_ranges(ntiles, HT, [&](int, int64_t lo, int64_t hi) {
+                for (int64_t t = lo; t < hi; t++) {
+                    const int64_t n0 = t * kTile, n1 = std::min(nN, n0 + kTile);
+                    const std::vector<uint32_t> &h = hl[t];
+                    std::copy(h.begin(), h.end(), halo.begin() + hptr[t]);
+                    for (int64_t me = n0; me < n1; me++)
+                        for (int32_t r = 0; r < deg[me]; r++) {
+                            const int64_t pos = entry_pos(sptr[me / 32], r, (int)(me % 32));
+                            const uint32_t w = colw[pos], j = w & COL_MASK;
+                            uint32_t l;
+                            if ((int64_t)j >= n0 && (int64_t)j < n1) l = (uint32_t)(j - n0);
+                            else l = (uint32_t)(n1 - n0) + (uint32_t)(std::lower_bound(h.begin(), h.end(), j) - h.begin());
+                            jw[pos] = (uint16_t)(l | ((w & F_CHUNK) ? TF_CHUNK : 0u) |
+                                                 (((w >> BT_SHIFT) & 3u) << TBT_SHIFT));
+                        }
+                }
+            });
+            // dictionary ordered by use, so that the entries kept in shared
+            // memory are the most used ones
+            std::vector<int64_t> uses(dict.size(), 0);
+            for (int64_t me = 0; me < nN; me++)
+                for (int32_t r = 0; r < deg[me]; r++) uses[cid16[entry_pos(sptr[me / 32], r, (int)(me % 32))]]++;
+            std::vector<uint32_t> order(dict.size());
+            std::iota(order.begin(), order.end(), 0u);
+            std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return uses[a] > uses[b]; });
+            std::vector<uint32_t> rank(dict.size());
+            for (size_t q = 0; q < order.size(); q++) rank[order[q]] = (uint32_t)q;
+            for (int64_t e = 0; e < ne; e++) cid16[e] = (uint16_t)rank[cid16[e]];
+            std::vector<DictEntry> dict2(dict.size());
+            for (size_t q = 0; q < order.size(); q++) dict2[q] = dict[order[q]];
+            dict.swap(dict2);
+            if (S->prec == kP32X) {
+                std::vector<float4> dx2(dictx.size());
+                for (size_t q = 0; q < order.size(); q++) {
+                    dx2[2 * q] = dictx[2 * order[q]];
+                    dx2[2 * q + 1] = dictx[2 * order[q] + 1];
+                }
+                dictx.swap(dx2);
+            }
+            S->d.ncache = ncache;
+            S->d.tile_cap = tile_cap;
+            S->d.n_tiles = ntiles;
+        }
+    }
+
     // node arrays in device order
     auto perm3 = [&](const double *src, std::vector<double> &dst) {
         dst.assign(3 * nN, 0.0);
@@ -1359,7 +1857,19 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     TRY(S->put((int64_t **)&d.slice_ptr, sptr));
     TRY(S->put((int32_t **)&d.deg, deg));
     TRY(S->put((int32_t **)&d.slice_len, slen));
-    TRY(S->put((uint32_t **)&d.colw, colw));
+    d.colw = nullptr;
+    d.jw = nullptr;
+    d.halo_ptr = nullptr;
+    d.halo = nullptr;
+    if (S->tiled) {
+        TRY(S->put((uint16_t **)&d.jw, jw));
+        TRY(S->put((int64_t **)&d.halo_ptr, hptr));
+        TRY(S->put((uint32_t **)&d.halo, halo));
+    } else {
+        TRY(S->put((uint32_t **)&d.colw, colw));
+    }
+    std::vector<uint32_t>().swap(colw);
+    std::vector<uint16_t>().swap(jw);
     if (S->wide) TRY(S->put((uint32_t **)&d.cid, cid32));
     else TRY(S->put((uint16_t **)&d.cid, cid16));
     TRY(S->put(&d.st, st));
@@ -1462,12 +1972,18 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     d.timeout_ns = (unsigned long long)(to * 1e9);
 
     // kernel and grid
-    S->kernel = pick_kernel(prm->law, prm->scheme, S->prec, S->wide, pb->sc != nullptr);
+    if (S->tiled) {
+        S->kernel = pick_tkernel(prm->law, prm->scheme, S->prec, pb->sc != nullptr);
+        BBPD_CUDA_TRY(cudaFuncSetAttribute((const void *)S->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)S->smem));
+    } else {
+        S->kernel = pick_kernel(prm->law, prm->scheme, S->prec, S->wide, pb->sc != nullptr);
+    }
     int nsm = 0, occ = 0, coop = 0;
     BBPD_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     BBPD_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
     if (!coop) return fail(BBPD_ERR_UNSUPPORTED, "device lacks cooperative launch");
-    BBPD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)S->kernel, kBlock, 0));
+    BBPD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)S->kernel, kBlock, S->smem));
     if (occ < 1) return fail(BBPD_ERR_CUDA, "kernel cannot be resident");
     int64_t want = (ns * 32 + kBlock - 1) / kBlock;   // one warp per slice at most
     S->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * occ, want));
@@ -1478,7 +1994,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     // DRAM bytes one step moves with this layout (streams of the live entries,
     // node arrays; dictionary and damaged-bond BSF reads excluded)
     {
-        double per_entry = 4 + (S->wide ? 4 : 2) + 1 + (pb->s0 ? 8 : 0) + (pb->s1 ? 8 : 0) + (pb->sc ? 8 : 0);
+        double per_entry = (S->tiled ? 2 : 4) + (S->wide ? 4 : 2) + 1 + (pb->s0 ? 8 : 0) + (pb->s1 ? 8 : 0) + (pb->sc ? 8 : 0);
         double node = prm->scheme == BBPD_SCHEME_ADR
                           ? (24 /*x*/ + 4 /*deg*/ + 24 * 3 + 8 /*u v Fp m*/ + 24 /*F w*/ +
                              24 * 4 + 8 + 1 /*F u v X m flag*/ + 72 /*v u x w*/)
@@ -1513,7 +2029,7 @@ extern "C" int bbpd_step_async(bbpd_solver *S, int64_t nsteps)
     void *args[] = {(void *)&S->d, (void *)&step0, (void *)&nsteps};
     BBPD_CUDA_TRY(cudaMemsetAsync(S->d.work, 0, sizeof(unsigned long long), S->stream));
     BBPD_CUDA_TRY(cudaEventRecord(S->ev0, S->stream));
-    BBPD_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)S->kernel, dim3(S->grid), dim3(kBlock), args, 0, S->stream));
+    BBPD_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)S->kernel, dim3(S->grid), dim3(kBlock), args, S->smem, S->stream));
     BBPD_CUDA_TRY(cudaEventRecord(S->ev1, S->stream));
     S->step += nsteps;
     return BBPD_OK;
@@ -1729,7 +2245,7 @@ extern "C" int bbpd_get_info(bbpd_solver *S, bbpd_info *info)
     info->block_threads = kBlock;
     info->device_bytes = S->device_bytes;
     info->bytes_per_step = S->bytes_per_step;
-    info->layout = S->wide ? 2 : (S->prec == kP32X ? 3 : 1);
+    info->layout = (S->wide ? 2 : (S->prec == kP32X ? 3 : 1)) + (S->tiled ? 16 : 0);
     info->reserved = (int32_t)std::min<int64_t>(S->ndict, INT32_MAX);
     return BBPD_OK;
 }

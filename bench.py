@@ -55,6 +55,17 @@ def peak_hbm():
         return 6650.0, "fallback"
 
 
+def measured_traffic(cfg, form):
+    """DRAM bytes (read + write) per time step of the step kernel from an ncu
+    capture of this workload (profiles/step_kernel_traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "step_kernel_traffic.json")) as f:
+            t = json.load(f)[cfg][form]
+        return float(t["dram_bytes_per_step"]), t.get("source")
+    except Exception:
+        return None, None
+
+
 def algorithmic_bytes(nN, nB, per_bond_sc):
     """Bytes one time step must move: per directed bond entry 4 B of neighbour
     index + 8 B of damage state (+ 8 B of per-bond critical stretch), per node
@@ -144,7 +155,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=list(CONFIGS))
     ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--node-order", default="input", choices=["input", "morton"])
+    ap.add_argument("--node-order", default="input", choices=["input", "morton", "tiled"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -254,8 +265,9 @@ def main():
     peak, peak_kind = peak_hbm()
     alg = algorithmic_bytes(nN, nB, per_bond_sc)
     achieved = alg / (ms_step / 1e3) / 1e9
+    traffic, tsrc = measured_traffic(args.config, args.form)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_kind": peak_kind, "traffic": None,
+                "peak_kind": peak_kind, "traffic": traffic, "traffic_source": tsrc, "per": "time step",
                 "algorithmic_bytes_per_step": alg, "layout_bytes_per_step": info["bytes_per_step"]}
 
     cpu = None

@@ -50,7 +50,12 @@ enum { BBPD_PREC_FP64 = 0,        /* plain form: bit-identical to the reference 
        BBPD_PREC_FP32 = 1         /* FP32 stretch/force, FP64 sums, FP64 guard band */ };
 enum { BBPD_AMP_LINEAR = 0,       /* U(n) = rate * n */
        BBPD_AMP_SMOOTHSTEP = 1    /* smoothstepdata.m:40-42 from step 1 to nTimeSteps */ };
-enum { BBPD_ORDER_INPUT = 0, BBPD_ORDER_MORTON = 1 };
+enum { BBPD_ORDER_INPUT = 0,      /* input node order, neighbours gathered from HBM/L2
+                                     with L2 prefetch of the bond streams; the default */
+       BBPD_ORDER_MORTON = 1,     /* Morton node order, neighbours gathered from HBM/L2 */
+       BBPD_ORDER_TILED = 2       /* Morton order in 512-node tiles whose neighbours are
+                                     staged in shared memory (falls back to MORTON when a
+                                     tile's neighbourhood does not fit) */ };
 
 /* Message of the last failing call on this thread ("" if none). */
 const char *bbpd_last_error(void);
@@ -297,8 +302,10 @@ typedef struct bbpd_info {
     int32_t grid_blocks, block_threads;
     int64_t device_bytes;                 /* device memory held by the solver */
     double bytes_per_step;                /* algorithmic DRAM bytes of one step */
-    int32_t layout;                       /* 0 = wide per-entry constants, 1 = compact */
-    int32_t reserved;
+    int32_t layout;                       /* 1 = 16-bit dictionary ids, 2 = 32-bit ids
+                                             (irregular input), 3 = FP32 dictionary of bond
+                                             vectors; +16 when the tiled kernel runs */
+    int32_t reserved;                     /* dictionary entries */
 } bbpd_info;
 int bbpd_get_info(bbpd_solver *s, bbpd_info *info);
 
