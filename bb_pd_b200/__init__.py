@@ -5,10 +5,14 @@ This package is the host-side mirror of the reference's MATLAB calls:
 
     routines   the reference MEX routines under their own names (in place)
     Solver     the fused time loop, state resident on the GPU
+    Batch      many solvers stepped by one persistent launch (batching form)
+    serving    continuous batching of beam solves under an HBM budget
     beam       synthetic beams like the reference's input scripts
 """
-from . import _native, beam, routines
+from . import _native, beam, routines, serving
 from ._native import BBPDError, device_count
+from .batch import Batch
 from .solver import Solver, make_params
 
-__all__ = ["Solver", "make_params", "beam", "routines", "BBPDError", "device_count", "_native"]
+__all__ = ["Solver", "Batch", "make_params", "beam", "routines", "serving", "BBPDError", "device_count",
+           "_native"]

@@ -71,6 +71,13 @@ class Info(C.Structure):
     ]
 
 
+class BatchInfo(C.Structure):
+    _fields_ = [
+        ("n_members", C.c_int32), ("blocks_per_sm", C.c_int32), ("grab", C.c_int32),
+        ("graph", C.c_int32), ("total_slices", C.c_int64), ("device_bytes", C.c_int64),
+    ]
+
+
 class BeamSpec(C.Structure):
     _fields_ = [
         ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("dx", C.c_double),
@@ -117,6 +124,17 @@ def lib() -> C.CDLL:
         L.bbpd_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
         L.bbpd_selftest_wait_timeout.argtypes = [C.c_double]
         L.bbpd_selftest_division.argtypes = [C.c_int64, C.c_uint64] + [C.POINTER(C.c_int64)] * 3 + [_P]
+        L.bbpd_get_reaction.argtypes = [C.c_void_p, C.c_int64, _P]
+        L.bbpd_batch_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        for name in ("bbpd_batch_destroy",):
+            getattr(L, name).argtypes = [C.c_void_p]
+        for name in ("bbpd_batch_add", "bbpd_batch_remove"):
+            getattr(L, name).argtypes = [C.c_void_p, C.c_void_p]
+        L.bbpd_batch_step.argtypes = [C.c_void_p, C.c_int64]
+        L.bbpd_batch_tune.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.bbpd_batch_set_schedule.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.bbpd_batch_get_info.argtypes = [C.c_void_p, C.POINTER(BatchInfo)]
+        L.bbpd_batch_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
         L.bbpd_beam_count.argtypes = [C.POINTER(BeamSpec), C.POINTER(BeamScalars)]
         L.bbpd_beam_build.argtypes = [C.POINTER(BeamSpec)] + [_P] * 11
         _lib = L

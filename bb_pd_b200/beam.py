@@ -89,3 +89,51 @@ def small(nx: int = 24, ny: int = 5, nz: int = 6, dx: float = 5e-3, **kw) -> N.B
     """A small beam for parity tests (supports at 2 dx from each end)."""
     kw.setdefault("supports", (3 * dx, (nx - 2) * dx))
     return spec(nx, ny, nz, dx, **kw)
+
+
+def geometric_beam(depth: float, dx: float, *, span_to_depth: float = 5.0, width: float = 0.05,
+                   **kw) -> N.BeamSpec:
+    """A 3-point-bending beam of the given depth: span = span_to_depth x depth,
+    half a depth of overhang at each end, supports on the bottom layer at the
+    span ends, midspan top nodes under prescribed displacement."""
+    span = span_to_depth * depth
+    length = span + depth
+    nx = max(4, int(round(length / dx)))
+    nz = max(3, int(round(depth / dx)))
+    ny = max(2, int(round(width / dx)))
+    # support lines on node planes (nodes sit at dx * (k + 1))
+    x0 = dx * (int(round(0.5 * depth / dx)) + 1)
+    x1 = dx * (int(round((0.5 * depth + span) / dx)) + 1)
+    return spec(nx, ny, nz, dx, supports=(x0 - 0.25 * dx, x1 - 0.25 * dx), **kw)
+
+
+def size_effect_series(n: int = 64, seed: int = 20261203, depth_range=(0.05, 0.4), dx: float = 2.5e-3,
+                       sc_mean: float = 2e-3, sc_cov: float = 0.1) -> list[tuple[N.BeamSpec, str]]:
+    """Geometrically similar beams with log-uniform depths, span/depth 5, width
+    50 mm, seeded lognormal critical stretch; laws alternate linear/trilinear.
+    Returns (spec, law) pairs."""
+    rng = np.random.default_rng(seed)
+    depths = np.exp(rng.uniform(np.log(depth_range[0]), np.log(depth_range[1]), n))
+    laws = rng.choice(["linear", "trilinear"], n)
+    return [(geometric_beam(float(d), dx, sc_lognormal=(sc_mean, sc_cov), seed=seed + k), str(l))
+            for k, (d, l) in enumerate(zip(depths, laws))]
+
+
+def serving_stream(n: int = 200, seed: int = 20261203, nodes_range=(1e4, 1e6), rate_hz: float = 2.0,
+                   dx_choices=(1.25e-3, 2.5e-3, 5e-3)) -> list[dict]:
+    """Poisson arrivals of beam solves: node counts log-uniform in nodes_range,
+    dx drawn from dx_choices, law uniform over the four laws. A beam of depth d
+    is 6d long and d/2 wide, so nodes ~ 3 (d/dx)^3. Returns dicts with
+    arrival (s), spec, law and nodes (estimate)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_hz, n))
+    laws = rng.choice(["linear", "bilinear", "trilinear", "exponential"], n)
+    out = []
+    for k in range(n):
+        target = float(np.exp(rng.uniform(np.log(nodes_range[0]), np.log(nodes_range[1]))))
+        dx = float(rng.choice(dx_choices))
+        cells = (target / 3.0) ** (1.0 / 3.0)
+        depth = cells * dx
+        s = geometric_beam(depth, dx, width=0.5 * depth)
+        out.append(dict(arrival=float(t[k]), spec=s, law=str(laws[k]), nodes=int(s.nx) * int(s.ny) * int(s.nz)))
+    return out

@@ -75,6 +75,7 @@ constexpr int kBlock = 256;
 #define BBPD_MIN_BLOCKS_F32 2   // resident blocks per SM, FP32 dictionary-vector kernels
 #endif
 constexpr int kMaxLevels = 8;     // 32-ary reduction tree over the slices
+constexpr int64_t kReactCap = 4096;  // per-step reactions kept from one launch
 
 // Tiled kernel: nodes per tile, and the local neighbour word of an entry
 // (12-bit index into the tile's staged nodes, chunk-start bit, BONDTYPE).
@@ -135,6 +136,10 @@ struct Dev {
     const double *mass, *rho;
     const uint8_t *nflag;            // bit d: held (constrained or prescribed); bit 3+d: prescribed
     double2 *tree;                   // partial sums (cn1, cn2) of every tree level
+    double *tree3;                   // partial sums of the reaction, same tree
+    double *react;                   // reaction of step `it` of the last launch at [it]
+    int64_t react_cap;               // entries of react[]
+    int law;                         // BBPD_LAW_* (read by the batch kernel)
     unsigned *tcnt;                  // arrival counters of the groups of levels >= 2
     int64_t lvl_cnt[kMaxLevels];     // values at level L (level 1: one per slice)
     int64_t lvl_off[kMaxLevels];     // offset of level L in tree[]
@@ -209,18 +214,26 @@ __device__ __forceinline__ double cn_from_sums(double cn1, double cn2)
 // (arrival counter, fence) folds the group with the xor butterfly and carries
 // the result one level up, until the root yields cn. The order of every
 // addition depends on slice indices only, never on timing or launch shape.
-__device__ void tree_publish(const Dev &d, int64_t sl, int lane, double c1, double c2)
+// A third sum, the reaction (internal force summed over the prescribed DOFs),
+// rides the same tree; the root stores it for step `it` of the launch.
+__device__ void tree_publish(const Dev &d, int64_t sl, int lane, double c1, double c2, double c3,
+                             int64_t it)
 {
     int L = 1;
     int64_t idx = sl;
     for (;;) {
-        if (lane == 0) d.tree[d.lvl_off[L] + idx] = make_double2(c1, c2);
+        if (lane == 0) {
+            d.tree[d.lvl_off[L] + idx] = make_double2(c1, c2);
+            d.tree3[d.lvl_off[L] + idx] = c3;
+        }
         const int64_t cnt = d.lvl_cnt[L];
         if (cnt == 1) {   // root
             if (lane == 0) {
                 d.scal[0] = cn_from_sums(c1, c2);
                 d.scal[1] = c1;
                 d.scal[2] = c2;
+                d.scal[3] = c3;
+                if (it < d.react_cap) d.react[it] = c3;
             }
             return;
         }
@@ -234,54 +247,65 @@ __device__ void tree_publish(const Dev &d, int64_t sl, int lane, double c1, doub
         if (lane == 0) d.tcnt[d.cnt_off[L + 1] + g] = 0u;
         __threadfence();
         double2 v = make_double2(0.0, 0.0);
-        if (lane < gsize) v = __ldcg(&d.tree[d.lvl_off[L] + g * 32 + lane]);
+        double v3 = 0.0;
+        if (lane < gsize) {
+            v = __ldcg(&d.tree[d.lvl_off[L] + g * 32 + lane]);
+            v3 = __ldcg(&d.tree3[d.lvl_off[L] + g * 32 + lane]);
+        }
         c1 = v.x;
         c2 = v.y;
+        c3 = v3;
 #pragma unroll
         for (int off = 16; off >= 1; off >>= 1) {
             c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
             c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
+            c3 = c3 + __shfl_xor_sync(0xffffffffu, c3, off);
         }
         L++;
         idx = g;
     }
 }
 
-// Next slice for this warp from the phase-A counter (lane 0 takes it, all
-// lanes receive it).
-__device__ __forceinline__ int64_t grab_slice(const Dev &d, int lane)
+// Next value of a work counter for this warp (lane 0 takes it, all lanes
+// receive it).
+__device__ __forceinline__ int64_t grab_counter(unsigned long long *ctr, int lane)
 {
     unsigned long long v = 0;
-    if (lane == 0) v = atomicAdd(d.work, 1ull);
+    if (lane == 0) v = atomicAdd(ctr, 1ull);
     return (int64_t)__shfl_sync(0xffffffffu, v, 0);
 }
 
-// Grid-wide barrier with a time limit. False on timeout.
-__device__ bool grid_barrier(const Dev &d)
+__device__ __forceinline__ int64_t grab_slice(const Dev &d, int lane) { return grab_counter(d.work, lane); }
+
+// Grid-wide barrier with a time limit on bar[0] (arrivals) and bar[1]
+// (generation). False on timeout (ERR_TIMEOUT set in *err).
+__device__ bool grid_barrier_raw(unsigned *bar, int *err, unsigned long long timeout_ns)
 {
     __shared__ int s_last, s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *gen = d.bar + 1;
+        volatile unsigned *gen = bar + 1;
         unsigned g = *gen;
         __threadfence();
-        unsigned prev = atomicAdd(d.bar, 1u);
+        unsigned prev = atomicAdd(bar, 1u);
         s_last = (prev == gridDim.x - 1);
         s_ok = 1;
-        if (!s_last) s_ok = bounded_wait_change(gen, g, d.err, d.timeout_ns) ? 1 : 0;
+        if (!s_last) s_ok = bounded_wait_change(gen, g, err, timeout_ns) ? 1 : 0;
     }
     __syncthreads();
     if (s_last) {
         if (threadIdx.x == 0) {
-            d.bar[0] = 0;
+            bar[0] = 0;
             __threadfence();
-            atomicAdd(d.bar + 1, 1u);
+            atomicAdd(bar + 1, 1u);
         }
     }
     __threadfence();
     __syncthreads();
     return s_ok != 0;
 }
+
+__device__ __forceinline__ bool grid_barrier(const Dev &d) { return grid_barrier_raw(d.bar, d.err, d.timeout_ns); }
 
 // L2 prefetch of one line: no register is written, so a warp can keep many
 // groups of its streams in flight ahead of the loads that consume them.
@@ -729,7 +753,7 @@ __device__ __forceinline__ StepBufs step_bufs(const Dev &d, int64_t n)
 // Rayleigh-quotient terms, folds them over the slice and enters the tree.
 template <int SCHEME, int PREC>
 __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, int64_t sl, int lane,
-                                             double tx, double ty, double tz)
+                                             double tx, double ty, double tz, int64_t it)
 {
     const int64_t nN = d.n_nodes;
     const int64_t i = sl * 32 + lane;
@@ -765,13 +789,18 @@ __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, in
             if (far) atomicOr(d.sticky, 1u);
         }
     } else {
-        // calculatedampingcoefficient.m:61-85 terms of this node, then the
-        // xor butterfly over the slice's 32 lanes
-        double c1 = 0, c2 = 0;
+        // calculatedampingcoefficient.m:61-85 terms of this node and its share
+        // of the reaction (force on its prescribed DOFs), then the xor
+        // butterfly over the slice's 32 lanes
+        double c1 = 0, c2 = 0, c3 = 0;
         if (valid) {
             b.Fc[i] = tx; b.Fc[i + nN] = ty; b.Fc[i + 2 * nN] = tz;
             const double m = d.mass[i];
             const double Fv[3] = {tx, ty, tz};
+            const uint8_t fl = d.nflag[i];
+#pragma unroll
+            for (int dof = 0; dof < 3; dof++)
+                if (fl & (8 << dof)) c3 = c3 + Fv[dof];
 #pragma unroll
             for (int dof = 0; dof < 3; dof++) {
                 const int64_t e = i + nN * dof;
@@ -788,21 +817,21 @@ __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, in
         for (int off = 16; off >= 1; off >>= 1) {
             c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
             c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
+            c3 = c3 + __shfl_xor_sync(0xffffffffu, c3, off);
         }
-        tree_publish(d, sl, lane, c1, c2);
+        tree_publish(d, sl, lane, c1, c2, c3, it);
     }
 }
 
-// ADR phase B (timeintegrationADR.m:168-197) on slices gwarp, gwarp + nwarps, ...
+// ADR phase B (timeintegrationADR.m:168-197) on the nodes of slice sb.
 template <int PREC>
-__device__ __forceinline__ void adr_update(const Dev &d, const StepBufs &b, int lane, int64_t gwarp,
-                                           int64_t nwarps)
+__device__ __forceinline__ void adr_update_slice(const Dev &d, const StepBufs &b, int64_t sb, int lane)
 {
-    const int64_t nN = d.n_nodes, nsl = d.n_slices;
+    const int64_t nN = d.n_nodes;
     const double cn = __ldcg(&d.scal[0]);
-    for (int64_t sb = gwarp; sb < nsl; sb += nwarps) {
+    {
         const int64_t i = sb * 32 + lane;
-        if (i >= nN) continue;
+        if (i >= nN) return;
         const uint8_t fl = d.nflag[i];
         const double minv = 1.0 / d.mass[i];
         float uh[3], ul[3];
@@ -830,6 +859,14 @@ __device__ __forceinline__ void adr_update(const Dev &d, const StepBufs &b, int 
         if (bad) atomicOr(d.err, ERR_NONFINITE);
         if (far) atomicOr(d.sticky, 1u);
     }
+}
+
+// ADR phase B on slices gwarp, gwarp + nwarps, ...
+template <int PREC>
+__device__ __forceinline__ void adr_update(const Dev &d, const StepBufs &b, int lane, int64_t gwarp,
+                                           int64_t nwarps)
+{
+    for (int64_t sb = gwarp; sb < d.n_slices; sb += nwarps) adr_update_slice<PREC>(d, b, sb, lane);
 }
 
 // Global-gather kernel: neighbour data read from HBM/L2 per entry. Used for
@@ -862,7 +899,7 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
             double tx, ty, tz;
             if (PREC == kP32X) slice_forces_x<LAW, CID, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
             else slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, b.xs, tx, ty, tz);
-            finish_slice<SCHEME, PREC>(d, b, sl, lane, tx, ty, tz);
+            finish_slice<SCHEME, PREC>(d, b, sl, lane, tx, ty, tz, it);
             sl = sl_next;
         }
         if (SCHEME == BBPD_SCHEME_ADR) {
@@ -1136,7 +1173,7 @@ __global__ void __launch_bounds__(kBlock, 2) tstep_kernel(Dev d, int64_t step0, 
                 else
                     tslice_forces<LAW, SCE>(d, sl, k * 32 + lane, lane, safe, sx, sy, sz, sdict, ncache,
                                             tx, ty, tz);
-                finish_slice<SCHEME, PREC>(d, b, sl, lane, tx, ty, tz);
+                finish_slice<SCHEME, PREC>(d, b, sl, lane, tx, ty, tz, it);
             }
             __syncthreads();
         }
@@ -1147,6 +1184,102 @@ __global__ void __launch_bounds__(kBlock, 2) tstep_kernel(Dev d, int64_t step0, 
         if (!grid_barrier(d)) return;
     }
 }
+
+// ---------------------------------------------------------------- batch kernel
+//
+// Many solver states ("members") of any sizes and laws stepped by one
+// persistent launch: phase A takes slices from one counter over the
+// concatenation of all members' slices (prefix[m] = first global slice of
+// member m), so the SMs stay busy however uneven the members are; every
+// member keeps its own step number, ADR tree, damping coefficient and
+// reaction history, and its arithmetic is that of a launch of its own.
+struct BatchCtl {
+    const Dev *members;        // device copies of the members' descriptors
+    const int64_t *prefix;     // S + 1 entries
+    int64_t *mstep;            // next step of each member; advanced at the end of a launch
+    int S;
+    int grab;                  // consecutive slices per counter grab
+    int64_t total;             // prefix[S]
+    unsigned *bar;
+    unsigned long long *work;
+    int *err;
+    unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ int member_of(const BatchCtl &B, int64_t w)
+{
+    int lo = 0, hi = B.S;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(&B.prefix[mid]) <= w) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// One slice of one member, out of line so that each law instance gets its own
+// register allocation (the batch kernel dispatches on the member's law).
+template <int LAW, int PREC, bool SCE>
+__device__ __noinline__ void batch_slice(const Dev *dp, int64_t sl, int64_t n, int64_t it, int lane)
+{
+    const Dev &d = *dp;
+    const StepBufs b = step_bufs(d, n);
+    const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
+    double tx, ty, tz;
+    if (PREC == kP32X) slice_forces_x<LAW, uint16_t, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
+    else slice_forces<LAW, PREC, uint16_t, SCE>(d, sl, lane, safe, b.xs, tx, ty, tz);
+    finish_slice<BBPD_SCHEME_ADR, PREC>(d, b, sl, lane, tx, ty, tz, it);
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl B, int64_t nsteps)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t G = B.grab;
+    const int64_t ngrabs = (B.total + G - 1) / G;
+
+    for (int64_t it = 0; it < nsteps; it++) {
+        // one failing grab per warp and step: ngrabs + nwarps values per step
+        const int64_t base = it * (ngrabs + nwarps);
+        int64_t gi = grab_counter(B.work, lane) - base;
+        while (gi < ngrabs) {
+            const int64_t gnext = grab_counter(B.work, lane) - base;
+            const int64_t w1 = min(B.total, (gi + 1) * G);
+            for (int64_t w = gi * G; w < w1; w++) {
+                const int m = member_of(B, w);
+                const Dev *dp = B.members + m;
+                const int64_t sl = w - __ldg(&B.prefix[m]);
+                const int64_t n = __ldg(&B.mstep[m]) + it;
+                switch (dp->law * 2 + (dp->sce != nullptr)) {
+                case 0: batch_slice<BBPD_LAW_LINEAR, PREC, false>(dp, sl, n, it, lane); break;
+                case 1: batch_slice<BBPD_LAW_LINEAR, PREC, true>(dp, sl, n, it, lane); break;
+                case 2: batch_slice<BBPD_LAW_BILINEAR, PREC, false>(dp, sl, n, it, lane); break;
+                case 3: batch_slice<BBPD_LAW_BILINEAR, PREC, true>(dp, sl, n, it, lane); break;
+                case 4: batch_slice<BBPD_LAW_TRILINEAR, PREC, false>(dp, sl, n, it, lane); break;
+                case 5: batch_slice<BBPD_LAW_TRILINEAR, PREC, true>(dp, sl, n, it, lane); break;
+                case 6: batch_slice<BBPD_LAW_EXPONENTIAL, PREC, false>(dp, sl, n, it, lane); break;
+                default: batch_slice<BBPD_LAW_EXPONENTIAL, PREC, true>(dp, sl, n, it, lane); break;
+                }
+            }
+            gi = gnext;
+        }
+        if (!grid_barrier_raw(B.bar, B.err, B.timeout_ns)) return;
+        for (int64_t w = gwarp; w < B.total; w += nwarps) {
+            const int m = member_of(B, w);
+            const Dev &d = B.members[m];
+            const StepBufs b = step_bufs(d, __ldg(&B.mstep[m]) + it);
+            adr_update_slice<PREC>(d, b, w - __ldg(&B.prefix[m]), lane);
+        }
+        if (!grid_barrier_raw(B.bar, B.err, B.timeout_ns)) return;
+    }
+    // every block has read the step numbers of the last step (barrier above)
+    if (blockIdx.x == 0)
+        for (int m = threadIdx.x; m < B.S; m += blockDim.x) B.mstep[m] += nsteps;
+}
+
+typedef void (*batch_kernel_t)(BatchCtl, int64_t);
 
 // Self-test of the bounded wait: one thread waits on a word that nothing
 // writes, so the wait must expire and report ERR_TIMEOUT.
@@ -1385,6 +1518,8 @@ struct bbpd_solver {
     int grid = 0;
     bool tiled = false;                 // tiled kernel with shared-memory staging
     size_t smem = 0;                    // its dynamic shared memory per block
+    bbpd_batch *batch = nullptr;        // batch this solver is a member of
+    bool cn_stale = false;              // cn on the device is newer than S->cn
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -1417,6 +1552,10 @@ struct bbpd_solver {
 };
 
 #define TRY(x) do { int r_ = (x); if (r_) return r_; } while (0)
+
+// Wait for the batch's launches and rebuild its member table before the next
+// one (a member's descriptor or step changed on the host).
+static int batch_member_changed(bbpd_batch *B);
 
 static int validate_01(const double *a, int64_t n, const char *name)
 {
@@ -1932,9 +2071,14 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         }
         d.n_levels = L;
         TRY(S->alloc(&d.tree, (size_t)std::max<int64_t>(off, 1)));
+        TRY(S->alloc(&d.tree3, (size_t)std::max<int64_t>(off, 1)));
         std::vector<unsigned> tc((size_t)std::max<int64_t>(coff, 1), 0u);
         TRY(S->put(&d.tcnt, tc));
     }
+    d.react_cap = kReactCap;
+    TRY(S->alloc(&d.react, (size_t)kReactCap));
+    BBPD_CUDA_TRY(cudaMemset(d.react, 0, sizeof(double) * kReactCap));
+    d.law = prm->law;
     std::vector<double> sc4(4, 0.0);
     TRY(S->put(&d.scal, sc4));
     std::vector<unsigned> bar(2, 0u);
@@ -2023,6 +2167,7 @@ static int collect_status(bbpd_solver *S)
 extern "C" int bbpd_step_async(bbpd_solver *S, int64_t nsteps)
 {
     if (!S || nsteps < 0) return fail(BBPD_ERR_ARG, "bad argument");
+    if (S->batch) return fail(BBPD_ERR_ARG, "solver is a batch member: step it with bbpd_batch_step");
     if (nsteps == 0) return BBPD_OK;
     BBPD_CUDA_TRY(cudaSetDevice(S->device));
     int64_t step0 = S->step;
@@ -2061,9 +2206,12 @@ extern "C" int bbpd_last_kernel_ms(bbpd_solver *S, float *ms)
     return BBPD_OK;
 }
 
+extern "C" int bbpd_batch_remove(bbpd_batch *B, bbpd_solver *S);
+
 extern "C" int bbpd_destroy(bbpd_solver *S)
 {
     if (!S) return BBPD_OK;
+    if (S->batch) bbpd_batch_remove(S->batch, S);
     cudaSetDevice(S->device);
     if (S->stream) cudaStreamSynchronize(S->stream);
     delete S;
@@ -2123,6 +2271,7 @@ extern "C" int bbpd_get(bbpd_solver *S, int field, double *out)
 extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
 {
     if (!S || !in) return fail(BBPD_ERR_ARG, "null argument");
+    if (S->batch) TRY(batch_member_changed(S->batch));
     BBPD_CUDA_TRY(cudaSetDevice(S->device));
     BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
     const int64_t nN = S->nN, nB = S->nB;
@@ -2188,6 +2337,11 @@ extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
 extern "C" int bbpd_get_step(bbpd_solver *S, int64_t *step, double *cn)
 {
     if (!S) return fail(BBPD_ERR_ARG, "null solver");
+    if (S->cn_stale) {   // last stepped by a batch launch
+        BBPD_CUDA_TRY(cudaSetDevice(S->device));
+        BBPD_CUDA_TRY(cudaMemcpy(&S->cn, S->d.scal, sizeof(double), cudaMemcpyDeviceToHost));
+        S->cn_stale = false;
+    }
     if (step) *step = S->step;
     if (cn) *cn = S->cn;
     return BBPD_OK;
@@ -2208,6 +2362,8 @@ extern "C" int bbpd_set_step(bbpd_solver *S, int64_t step, double cn)
     }
     S->step = step;
     S->cn = cn;
+    S->cn_stale = false;
+    if (S->batch) TRY(batch_member_changed(S->batch));
     BBPD_CUDA_TRY(cudaMemcpy(S->d.scal, &cn, sizeof(double), cudaMemcpyHostToDevice));
     return BBPD_OK;
 }
@@ -2247,5 +2403,341 @@ extern "C" int bbpd_get_info(bbpd_solver *S, bbpd_info *info)
     info->bytes_per_step = S->bytes_per_step;
     info->layout = (S->wide ? 2 : (S->prec == kP32X ? 3 : 1)) + (S->tiled ? 16 : 0);
     info->reserved = (int32_t)std::min<int64_t>(S->ndict, INT32_MAX);
+    return BBPD_OK;
+}
+
+// ------------------------------------------------------------------ batches
+
+struct bbpd_batch {
+    int device = 0;
+    int prec = kP64;                       // kernel precision shared by all members
+    std::vector<bbpd_solver *> members;
+    bool dirty = true;                     // member table must be rebuilt before the next launch
+    Dev *d_members = nullptr;
+    int64_t *d_prefix = nullptr, *d_mstep = nullptr;
+    size_t cap = 0;                        // members the device tables hold
+    unsigned *bar = nullptr;
+    unsigned long long *work = nullptr;
+    int *err = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    batch_kernel_t kernel = nullptr;
+    int nsm = 0, occ = 0;                  // SMs, resident blocks per SM
+    int blocks_per_sm = 0;                 // schedule: resident blocks used per SM
+    int grab = 1;                          // schedule: slices per counter grab
+    bool tuned = false;
+    int64_t total = 0;
+    BatchCtl ctl{};
+    bool use_graph = true;                 // replay the launch from a captured CUDA graph
+    cudaGraphExec_t gexec = nullptr;
+    int64_t g_nsteps = -1;
+    int g_grid = 0, g_grab = 0;
+    bool last_graph = false;
+
+    void drop_graph()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+        g_nsteps = -1;
+    }
+    ~bbpd_batch()
+    {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        drop_graph();
+        for (void *p : {(void *)d_members, (void *)d_prefix, (void *)d_mstep, (void *)bar, (void *)work, (void *)err})
+            if (p) cudaFree(p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+        for (bbpd_solver *S : members) S->batch = nullptr;
+    }
+};
+
+static int batch_member_changed(bbpd_batch *B)
+{
+    BBPD_CUDA_TRY(cudaSetDevice(B->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(B->stream));
+    B->dirty = true;
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_batch_create(int device, int precision, bbpd_batch **out)
+{
+    clear_error();
+    if (!out || (precision != BBPD_PREC_FP64 && precision != BBPD_PREC_FP32)) return fail(BBPD_ERR_ARG, "bad argument");
+    *out = nullptr;
+    TRY(require_device());
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(BBPD_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+    }
+    auto *B = new bbpd_batch;
+    std::unique_ptr<bbpd_batch> guard_(B);
+    B->device = device;
+    B->prec = precision == BBPD_PREC_FP32 ? kP32X : kP64;
+    B->kernel = B->prec == kP32X ? batch_kernel<kP32X> : batch_kernel<kP64>;
+    BBPD_CUDA_TRY(cudaMalloc((void **)&B->bar, 2 * sizeof(unsigned)));
+    BBPD_CUDA_TRY(cudaMemset(B->bar, 0, 2 * sizeof(unsigned)));
+    BBPD_CUDA_TRY(cudaMalloc((void **)&B->work, sizeof(unsigned long long)));
+    BBPD_CUDA_TRY(cudaMalloc((void **)&B->err, sizeof(int)));
+    BBPD_CUDA_TRY(cudaMemset(B->err, 0, sizeof(int)));
+    BBPD_CUDA_TRY(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+    BBPD_CUDA_TRY(cudaEventCreate(&B->ev0));
+    BBPD_CUDA_TRY(cudaEventCreate(&B->ev1));
+    int coop = 0;
+    BBPD_CUDA_TRY(cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, device));
+    BBPD_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+    if (!coop) return fail(BBPD_ERR_UNSUPPORTED, "device lacks cooperative launch");
+    BBPD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B->occ, (const void *)B->kernel, kBlock, 0));
+    if (B->occ < 1) return fail(BBPD_ERR_CUDA, "batch kernel cannot be resident");
+    B->blocks_per_sm = B->occ;
+    *out = guard_.release();
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_batch_destroy(bbpd_batch *B)
+{
+    delete B;
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_batch_add(bbpd_batch *B, bbpd_solver *S)
+{
+    if (!B || !S) return fail(BBPD_ERR_ARG, "null argument");
+    if (S->batch) return fail(BBPD_ERR_ARG, "solver already belongs to a batch");
+    if (S->device != B->device) return fail(BBPD_ERR_ARG, "solver and batch live on different devices");
+    if (S->prm.scheme != BBPD_SCHEME_ADR) return fail(BBPD_ERR_UNSUPPORTED, "batches run the ADR scheme");
+    if (S->prec != B->prec)
+        return fail(BBPD_ERR_UNSUPPORTED, "solver precision form differs from the batch's (an FP32 batch takes "
+                                          "solvers whose bond vectors fit the FP32 dictionary)");
+    if (S->wide || S->tiled)
+        return fail(BBPD_ERR_UNSUPPORTED, "batch members need 16-bit dictionary ids and input or Morton node order");
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    B->members.push_back(S);
+    S->batch = B;
+    B->dirty = true;
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_batch_remove(bbpd_batch *B, bbpd_solver *S)
+{
+    if (!B || !S) return fail(BBPD_ERR_ARG, "null argument");
+    auto it = std::find(B->members.begin(), B->members.end(), S);
+    if (it == B->members.end()) return fail(BBPD_ERR_ARG, "solver is not a member of this batch");
+    BBPD_CUDA_TRY(cudaSetDevice(B->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(B->stream));
+    B->members.erase(it);
+    S->batch = nullptr;
+    B->dirty = true;
+    return BBPD_OK;
+}
+
+// Device copies of the member descriptors, slice prefix and step numbers.
+static int batch_rebuild(bbpd_batch *B)
+{
+    const size_t S = B->members.size();
+    if (S > B->cap) {
+        for (void *p : {(void *)B->d_members, (void *)B->d_prefix, (void *)B->d_mstep})
+            if (p) cudaFree(p);
+        B->d_members = nullptr;
+        B->d_prefix = B->d_mstep = nullptr;
+        const size_t c = std::max<size_t>(S, 2 * B->cap);
+        BBPD_CUDA_TRY(cudaMalloc((void **)&B->d_members, sizeof(Dev) * c));
+        BBPD_CUDA_TRY(cudaMalloc((void **)&B->d_prefix, sizeof(int64_t) * (c + 1)));
+        BBPD_CUDA_TRY(cudaMalloc((void **)&B->d_mstep, sizeof(int64_t) * c));
+        B->cap = c;
+    }
+    std::vector<Dev> devs(S);
+    std::vector<int64_t> prefix(S + 1, 0), mstep(S);
+    for (size_t m = 0; m < S; m++) {
+        devs[m] = B->members[m]->d;
+        prefix[m + 1] = prefix[m] + B->members[m]->ns;
+        mstep[m] = B->members[m]->step;
+    }
+    if (S) {
+        BBPD_CUDA_TRY(cudaMemcpy(B->d_members, devs.data(), sizeof(Dev) * S, cudaMemcpyHostToDevice));
+        BBPD_CUDA_TRY(cudaMemcpy(B->d_mstep, mstep.data(), sizeof(int64_t) * S, cudaMemcpyHostToDevice));
+    }
+    BBPD_CUDA_TRY(cudaMemcpy(B->d_prefix, prefix.data(), sizeof(int64_t) * (S + 1), cudaMemcpyHostToDevice));
+    B->total = prefix[S];
+    BatchCtl &c = B->ctl;
+    c.members = B->d_members;
+    c.prefix = B->d_prefix;
+    c.mstep = B->d_mstep;
+    c.S = (int)S;
+    c.total = B->total;
+    c.bar = B->bar;
+    c.work = B->work;
+    c.err = B->err;
+    double to = 0;
+    for (bbpd_solver *M : B->members) to = std::max(to, M->prm.barrier_timeout_s > 0 ? M->prm.barrier_timeout_s : 2.0);
+    c.timeout_ns = (unsigned long long)((to > 0 ? to : 2.0) * 1e9);
+    B->drop_graph();
+    B->dirty = false;
+    return BBPD_OK;
+}
+
+// Enqueue one launch of nsteps steps with the given schedule (graph replay
+// when enabled and the capture succeeds, a direct launch otherwise).
+static int batch_launch(bbpd_batch *B, int64_t nsteps, int blocks_per_sm, int grab, bool graph)
+{
+    int64_t want = (B->total * 32 + kBlock - 1) / kBlock;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)B->nsm * blocks_per_sm, want));
+    B->ctl.grab = grab;
+    void *args[] = {(void *)&B->ctl, (void *)&nsteps};
+    B->last_graph = false;
+    if (graph && B->use_graph) {
+        if (!B->gexec || B->g_nsteps != nsteps || B->g_grid != grid || B->g_grab != grab) {
+            B->drop_graph();
+            cudaGraph_t g = nullptr;
+            bool ok = cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                cudaMemsetAsync(B->work, 0, sizeof(unsigned long long), B->stream);
+                cudaLaunchCooperativeKernel((const void *)B->kernel, dim3(grid), dim3(kBlock), args, 0, B->stream);
+                ok = cudaStreamEndCapture(B->stream, &g) == cudaSuccess && g;
+            }
+            if (ok) ok = cudaGraphInstantiate(&B->gexec, g, 0) == cudaSuccess;
+            if (g) cudaGraphDestroy(g);
+            if (!ok) {   // capture of this launch is not available here: launch directly from now on
+                cudaGetLastError();
+                B->drop_graph();
+                B->use_graph = false;
+            } else {
+                B->g_nsteps = nsteps;
+                B->g_grid = grid;
+                B->g_grab = grab;
+            }
+        }
+        if (B->gexec) {
+            BBPD_CUDA_TRY(cudaEventRecord(B->ev0, B->stream));
+            BBPD_CUDA_TRY(cudaGraphLaunch(B->gexec, B->stream));
+            BBPD_CUDA_TRY(cudaEventRecord(B->ev1, B->stream));
+            B->last_graph = true;
+            return BBPD_OK;
+        }
+    }
+    BBPD_CUDA_TRY(cudaMemsetAsync(B->work, 0, sizeof(unsigned long long), B->stream));
+    BBPD_CUDA_TRY(cudaEventRecord(B->ev0, B->stream));
+    BBPD_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)B->kernel, dim3(grid), dim3(kBlock), args, 0, B->stream));
+    BBPD_CUDA_TRY(cudaEventRecord(B->ev1, B->stream));
+    return BBPD_OK;
+}
+
+// Wait for the launch, then account it to every member: step numbers, and
+// error flags (the batch's barrier flag and each member's own flag).
+static int batch_finish(bbpd_batch *B, int64_t nsteps)
+{
+    BBPD_CUDA_TRY(cudaStreamSynchronize(B->stream));
+    int h = 0;
+    BBPD_CUDA_TRY(cudaMemcpy(&h, B->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        int z = 0;
+        BBPD_CUDA_TRY(cudaMemcpy(B->err, &z, sizeof(int), cudaMemcpyHostToDevice));
+        B->dirty = true;   // step numbers on the device were not advanced
+        return fail(BBPD_ERR_TIMEOUT, "batch grid barrier wait exceeded its limit; kernel returned early");
+    }
+    int bad = -1;
+    for (size_t m = 0; m < B->members.size(); m++) {
+        bbpd_solver *S = B->members[m];
+        S->step += nsteps;
+        S->cn_stale = true;
+        int e = 0;
+        BBPD_CUDA_TRY(cudaMemcpy(&e, S->d.err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e && bad < 0) bad = (int)m;
+        if (e) {
+            int z = 0;
+            BBPD_CUDA_TRY(cudaMemcpy(S->d.err, &z, sizeof(int), cudaMemcpyHostToDevice));
+        }
+    }
+    if (bad >= 0) return fail(BBPD_ERR_NONFINITE, "non-finite displacement or velocity in batch member %d", bad);
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_batch_step(bbpd_batch *B, int64_t nsteps)
+{
+    if (!B || nsteps < 0) return fail(BBPD_ERR_ARG, "bad argument");
+    if (nsteps == 0 || B->members.empty()) return BBPD_OK;
+    BBPD_CUDA_TRY(cudaSetDevice(B->device));
+    if (B->dirty) TRY(batch_rebuild(B));
+    TRY(batch_launch(B, nsteps, B->blocks_per_sm, B->grab, true));
+    return batch_finish(B, nsteps);
+}
+
+extern "C" int bbpd_batch_tune(bbpd_batch *B, int64_t nsteps_per_trial, int *blocks_per_sm, int *grab)
+{
+    if (!B || nsteps_per_trial < 1) return fail(BBPD_ERR_ARG, "bad argument");
+    if (B->members.empty()) return fail(BBPD_ERR_ARG, "empty batch");
+    BBPD_CUDA_TRY(cudaSetDevice(B->device));
+    if (B->dirty) TRY(batch_rebuild(B));
+    // Candidate schedules: resident blocks per SM x slices per grab. Every
+    // trial runs real steps of the members, so tuning costs no extra work.
+    float best = 0;
+    int bb = B->occ, bg = 1;
+    bool first = true;
+    for (int bps = 1; bps <= B->occ; bps++)
+        for (int g : {1, 2, 4}) {
+            TRY(batch_launch(B, nsteps_per_trial, bps, g, false));
+            TRY(batch_finish(B, nsteps_per_trial));
+            TRY(batch_rebuild(B));   // step numbers on the host are authoritative
+            float ms = 0;
+            BBPD_CUDA_TRY(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
+            if (first || ms < best) {
+                best = ms;
+                bb = bps;
+                bg = g;
+                first = false;
+            }
+        }
+    B->blocks_per_sm = bb;
+    B->grab = bg;
+    B->tuned = true;
+    if (blocks_per_sm) *blocks_per_sm = bb;
+    if (grab) *grab = bg;
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_batch_set_schedule(bbpd_batch *B, int blocks_per_sm, int grab, int use_graph)
+{
+    if (!B || blocks_per_sm < 1 || grab < 1 || grab > 64) return fail(BBPD_ERR_ARG, "bad argument");
+    B->blocks_per_sm = std::min(blocks_per_sm, B->occ);
+    B->grab = grab;
+    B->use_graph = use_graph != 0;
+    B->drop_graph();
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_batch_get_info(bbpd_batch *B, bbpd_batch_info *info)
+{
+    if (!B || !info) return fail(BBPD_ERR_ARG, "null argument");
+    std::memset(info, 0, sizeof(*info));
+    info->n_members = (int32_t)B->members.size();
+    info->blocks_per_sm = B->blocks_per_sm;
+    info->grab = B->grab;
+    info->graph = B->last_graph ? 1 : 0;
+    info->total_slices = B->total;
+    int64_t bytes = 0;
+    for (bbpd_solver *S : B->members) bytes += S->device_bytes;
+    info->device_bytes = bytes;
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_batch_last_kernel_ms(bbpd_batch *B, float *ms)
+{
+    if (!B || !ms) return fail(BBPD_ERR_ARG, "null argument");
+    BBPD_CUDA_TRY(cudaEventElapsedTime(ms, B->ev0, B->ev1));
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_get_reaction(bbpd_solver *S, int64_t n, double *out)
+{
+    if (!S || !out || n < 0) return fail(BBPD_ERR_ARG, "bad argument");
+    if (S->prm.scheme != BBPD_SCHEME_ADR) return fail(BBPD_ERR_UNSUPPORTED, "the reaction is summed by the ADR scheme");
+    if (n > kReactCap) return fail(BBPD_ERR_ARG, "at most %lld per-step reactions are kept", (long long)kReactCap);
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    if (S->batch) TRY(batch_member_changed(S->batch));
+    if (n) BBPD_CUDA_TRY(cudaMemcpy(out, S->d.react, sizeof(double) * n, cudaMemcpyDeviceToHost));
     return BBPD_OK;
 }

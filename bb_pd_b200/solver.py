@@ -134,6 +134,17 @@ class Solver:
     def set_step(self, step: int, cn: float = 0.0) -> None:
         N.check(N.lib().bbpd_set_step(self._h, step, cn))
 
+    def reaction(self, n: int) -> np.ndarray:
+        """Reaction of the first n steps of the last launch (ADR): the internal
+        force summed over the prescribed DOFs; the applied load is its negative."""
+        out = np.zeros(n, dtype=np.float64)
+        N.check(N.lib().bbpd_get_reaction(self._h, n, N.ptr(out)))
+        return out
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
     def info(self) -> dict:
         i = N.Info()
         N.check(N.lib().bbpd_get_info(self._h, C.byref(i)))

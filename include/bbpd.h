@@ -309,6 +309,46 @@ typedef struct bbpd_info {
 } bbpd_info;
 int bbpd_get_info(bbpd_solver *s, bbpd_info *info);
 
+/* Reaction of each step of the last launch (ADR only): the internal nodal
+ * force summed over the prescribed DOFs, in the fixed tree order of the damping
+ * sums; out[k] belongs to the k-th step of that launch (at most 4096 kept).
+ * The applied load is its negative. The reference reads its load from the
+ * platen contact (dynamicsolverdisplacementcontrolled.m:115); with prescribed
+ * displacements this is the equivalent quantity. */
+int bbpd_get_reaction(bbpd_solver *s, int64_t n, double *host_out);
+
+/* ---- batches: many solver states stepped by one persistent launch ----
+ * Serving and batching form. Members keep their own state, step number,
+ * damping coefficient and reaction history, and compute exactly what a solo
+ * launch computes (results are bit-identical alone and in a batch); the batch
+ * only shares the SMs: slices of all members are taken from one work counter.
+ * Members: ADR solvers of the batch's precision form, 16-bit dictionary ids,
+ * input or Morton node order. Membership may change between launches
+ * (continuous batching); a launch is captured into a CUDA graph and replayed
+ * while the membership and step count stay the same. */
+typedef struct bbpd_batch bbpd_batch;
+typedef struct bbpd_batch_info {
+    int32_t n_members;
+    int32_t blocks_per_sm;     /* schedule in use */
+    int32_t grab;              /* slices taken per work-counter grab */
+    int32_t graph;             /* 1 if the last launch replayed a CUDA graph */
+    int64_t total_slices;
+    int64_t device_bytes;      /* device memory held by the members */
+} bbpd_batch_info;
+int bbpd_batch_create(int device, int precision, bbpd_batch **out);
+int bbpd_batch_destroy(bbpd_batch *b);          /* members stay valid */
+int bbpd_batch_add(bbpd_batch *b, bbpd_solver *s);
+int bbpd_batch_remove(bbpd_batch *b, bbpd_solver *s);
+/* Advance every member by nsteps in one launch, then synchronize. */
+int bbpd_batch_step(bbpd_batch *b, int64_t nsteps);
+/* Autotuner: time candidate schedules (resident blocks per SM x slices per
+ * grab), each on nsteps_per_trial real steps of the members, and keep the
+ * fastest. */
+int bbpd_batch_tune(bbpd_batch *b, int64_t nsteps_per_trial, int *blocks_per_sm, int *grab);
+int bbpd_batch_set_schedule(bbpd_batch *b, int blocks_per_sm, int grab, int use_graph);
+int bbpd_batch_get_info(bbpd_batch *b, bbpd_batch_info *info);
+int bbpd_batch_last_kernel_ms(bbpd_batch *b, float *ms);
+
 /* Elapsed device time of the last bbpd_step / bbpd_step_async launch (ms). */
 int bbpd_last_kernel_ms(bbpd_solver *s, float *ms);
 
