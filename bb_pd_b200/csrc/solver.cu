@@ -140,6 +140,7 @@ struct Dev {
     double *react;                   // reaction of step `it` of the last launch at [it]
     int64_t react_cap;               // entries of react[]
     int law;                         // BBPD_LAW_* (read by the batch kernel)
+    int prec;                        // kernel precision variant (read by the batch kernel)
     unsigned *tcnt;                  // arrival counters of the groups of levels >= 2
     int64_t lvl_cnt[kMaxLevels];     // values at level L (level 1: one per slice)
     int64_t lvl_off[kMaxLevels];     // offset of level L in tree[]
@@ -1231,7 +1232,8 @@ __device__ __noinline__ void batch_slice(const Dev *dp, int64_t sl, int64_t n, i
     finish_slice<BBPD_SCHEME_ADR, PREC>(d, b, sl, lane, tx, ty, tz, it);
 }
 
-template <int PREC>
+// FAM 0: FP64 members; FAM 1: FP32 members (dictionary-vector or difference form).
+template <int FAM>
 __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl B, int64_t nsteps)
 {
     const int lane = threadIdx.x & 31;
@@ -1239,6 +1241,8 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t G = B.grab;
     const int64_t ngrabs = (B.total + G - 1) / G;
+    constexpr int P1 = FAM ? kP32X : kP64;
+    constexpr int P2 = FAM ? kP32D : kP64;
 
     for (int64_t it = 0; it < nsteps; it++) {
         // one failing grab per warp and step: ngrabs + nwarps values per step
@@ -1252,15 +1256,24 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
                 const Dev *dp = B.members + m;
                 const int64_t sl = w - __ldg(&B.prefix[m]);
                 const int64_t n = __ldg(&B.mstep[m]) + it;
-                switch (dp->law * 2 + (dp->sce != nullptr)) {
-                case 0: batch_slice<BBPD_LAW_LINEAR, PREC, false>(dp, sl, n, it, lane); break;
-                case 1: batch_slice<BBPD_LAW_LINEAR, PREC, true>(dp, sl, n, it, lane); break;
-                case 2: batch_slice<BBPD_LAW_BILINEAR, PREC, false>(dp, sl, n, it, lane); break;
-                case 3: batch_slice<BBPD_LAW_BILINEAR, PREC, true>(dp, sl, n, it, lane); break;
-                case 4: batch_slice<BBPD_LAW_TRILINEAR, PREC, false>(dp, sl, n, it, lane); break;
-                case 5: batch_slice<BBPD_LAW_TRILINEAR, PREC, true>(dp, sl, n, it, lane); break;
-                case 6: batch_slice<BBPD_LAW_EXPONENTIAL, PREC, false>(dp, sl, n, it, lane); break;
-                default: batch_slice<BBPD_LAW_EXPONENTIAL, PREC, true>(dp, sl, n, it, lane); break;
+                const int key = (FAM && dp->prec != kP32X ? 8 : 0) + dp->law * 2 + (dp->sce != nullptr);
+                switch (key) {
+                case 0: batch_slice<BBPD_LAW_LINEAR, P1, false>(dp, sl, n, it, lane); break;
+                case 1: batch_slice<BBPD_LAW_LINEAR, P1, true>(dp, sl, n, it, lane); break;
+                case 2: batch_slice<BBPD_LAW_BILINEAR, P1, false>(dp, sl, n, it, lane); break;
+                case 3: batch_slice<BBPD_LAW_BILINEAR, P1, true>(dp, sl, n, it, lane); break;
+                case 4: batch_slice<BBPD_LAW_TRILINEAR, P1, false>(dp, sl, n, it, lane); break;
+                case 5: batch_slice<BBPD_LAW_TRILINEAR, P1, true>(dp, sl, n, it, lane); break;
+                case 6: batch_slice<BBPD_LAW_EXPONENTIAL, P1, false>(dp, sl, n, it, lane); break;
+                case 7: batch_slice<BBPD_LAW_EXPONENTIAL, P1, true>(dp, sl, n, it, lane); break;
+                case 8: batch_slice<BBPD_LAW_LINEAR, P2, false>(dp, sl, n, it, lane); break;
+                case 9: batch_slice<BBPD_LAW_LINEAR, P2, true>(dp, sl, n, it, lane); break;
+                case 10: batch_slice<BBPD_LAW_BILINEAR, P2, false>(dp, sl, n, it, lane); break;
+                case 11: batch_slice<BBPD_LAW_BILINEAR, P2, true>(dp, sl, n, it, lane); break;
+                case 12: batch_slice<BBPD_LAW_TRILINEAR, P2, false>(dp, sl, n, it, lane); break;
+                case 13: batch_slice<BBPD_LAW_TRILINEAR, P2, true>(dp, sl, n, it, lane); break;
+                case 14: batch_slice<BBPD_LAW_EXPONENTIAL, P2, false>(dp, sl, n, it, lane); break;
+                default: batch_slice<BBPD_LAW_EXPONENTIAL, P2, true>(dp, sl, n, it, lane); break;
                 }
             }
             gi = gnext;
@@ -1270,7 +1283,8 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
             const int m = member_of(B, w);
             const Dev &d = B.members[m];
             const StepBufs b = step_bufs(d, __ldg(&B.mstep[m]) + it);
-            adr_update_slice<PREC>(d, b, w - __ldg(&B.prefix[m]), lane);
+            if (FAM && d.prec == kP32X) adr_update_slice<kP32X>(d, b, w - __ldg(&B.prefix[m]), lane);
+            else adr_update_slice<kP64>(d, b, w - __ldg(&B.prefix[m]), lane);
         }
         if (!grid_barrier_raw(B.bar, B.err, B.timeout_ns)) return;
     }
@@ -2079,6 +2093,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     TRY(S->alloc(&d.react, (size_t)kReactCap));
     BBPD_CUDA_TRY(cudaMemset(d.react, 0, sizeof(double) * kReactCap));
     d.law = prm->law;
+    d.prec = S->prec;
     std::vector<double> sc4(4, 0.0);
     TRY(S->put(&d.scal, sc4));
     std::vector<unsigned> bar(2, 0u);
@@ -2145,7 +2160,9 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
                           : (24 + 4 + 24 * 3 + 8 + 1 /*x v u X rho flag*/ + 24 * 5 /*F a v u x w*/);
         S->bytes_per_step = 2.0 * (double)nB * per_entry + (double)nN * node;
     }
-    BBPD_CUDA_TRY(cudaDeviceSynchronize());
+    // the uploads above ran on the legacy default stream; wait for them only,
+    // not for other solvers' launches on their own streams
+    BBPD_CUDA_TRY(cudaStreamSynchronize(0));
     *out = guard_.release();
     return BBPD_OK;
 }
@@ -2410,7 +2427,7 @@ extern "C" int bbpd_get_info(bbpd_solver *S, bbpd_info *info)
 
 struct bbpd_batch {
     int device = 0;
-    int prec = kP64;                       // kernel precision shared by all members
+    int prec = kP64;                       // kP64: FP64 members; kP32X: FP32 members (either FP32 variant)
     std::vector<bbpd_solver *> members;
     bool dirty = true;                     // member table must be rebuilt before the next launch
     Dev *d_members = nullptr;
@@ -2476,7 +2493,7 @@ extern "C" int bbpd_batch_create(int device, int precision, bbpd_batch **out)
     std::unique_ptr<bbpd_batch> guard_(B);
     B->device = device;
     B->prec = precision == BBPD_PREC_FP32 ? kP32X : kP64;
-    B->kernel = B->prec == kP32X ? batch_kernel<kP32X> : batch_kernel<kP64>;
+    B->kernel = B->prec == kP32X ? batch_kernel<1> : batch_kernel<0>;
     BBPD_CUDA_TRY(cudaMalloc((void **)&B->bar, 2 * sizeof(unsigned)));
     BBPD_CUDA_TRY(cudaMemset(B->bar, 0, 2 * sizeof(unsigned)));
     BBPD_CUDA_TRY(cudaMalloc((void **)&B->work, sizeof(unsigned long long)));
@@ -2508,9 +2525,8 @@ extern "C" int bbpd_batch_add(bbpd_batch *B, bbpd_solver *S)
     if (S->batch) return fail(BBPD_ERR_ARG, "solver already belongs to a batch");
     if (S->device != B->device) return fail(BBPD_ERR_ARG, "solver and batch live on different devices");
     if (S->prm.scheme != BBPD_SCHEME_ADR) return fail(BBPD_ERR_UNSUPPORTED, "batches run the ADR scheme");
-    if (S->prec != B->prec)
-        return fail(BBPD_ERR_UNSUPPORTED, "solver precision form differs from the batch's (an FP32 batch takes "
-                                          "solvers whose bond vectors fit the FP32 dictionary)");
+    if ((S->prec == kP64) != (B->prec == kP64))
+        return fail(BBPD_ERR_UNSUPPORTED, "solver precision form differs from the batch's");
     if (S->wide || S->tiled)
         return fail(BBPD_ERR_UNSUPPORTED, "batch members need 16-bit dictionary ids and input or Morton node order");
     BBPD_CUDA_TRY(cudaSetDevice(S->device));

@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import dataclasses
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -104,57 +105,72 @@ def _new_solver(req: Request, precision: str, device: int) -> Solver:
 
 def run_batched(requests: list[Request], *, hbm_budget: float = 150e9, precision: str = "fp64",
                 chunk: int = 100, device: int = 0, tune: bool = True) -> tuple[list[Result], dict]:
-    """Continuous batching. Returns the results and run statistics."""
+    """Continuous batching. Solvers of arrived requests are built by a worker
+    thread (host layout and upload) while the GPU steps the batch; a request
+    is admitted when its estimated device memory fits the budget. Returns the
+    results and run statistics."""
     pending = sorted(requests, key=lambda r: r.arrival)
     batch = Batch(precision, device)
-    active: list[tuple[Request, Solver, _Track, float, int]] = []
+    pool = ThreadPoolExecutor(max_workers=1)
+    creating: list = []                 # (request, future, estimate)
+    active: list = []                   # (request, solver, track, admitted, bytes)
     results: list[Result] = []
-    used = 0
+    used = reserved = 0
     launches = 0
     peak_members = 0
     tuned = False
     t0 = time.perf_counter()
-    while pending or active:
-        now = time.perf_counter() - t0
-        while pending and pending[0].arrival <= now:
-            r = pending[0]
-            est = device_bytes_estimate(r.inp, "sc" in r.inp)
-            if active and used + est > hbm_budget:
-                break                       # wait for a solve to finish
-            s = _new_solver(r, precision, device)
-            nbytes = int(s.info()["device_bytes"])
-            batch.add(s)
-            used += nbytes
-            active.append((r, s, _Track(r), time.perf_counter() - t0, nbytes))
-            pending.pop(0)
+    try:
+        while pending or active or creating:
             now = time.perf_counter() - t0
-        if not active:
-            time.sleep(max(0.0, min(pending[0].arrival - now, 0.05)))
-            continue
-        peak_members = max(peak_members, len(active))
-        if tune and not tuned and len(active) > 1:
-            batch.tune(max(1, chunk // 16))    # trials run real steps of every member
-            tuned = True
-        batch.step(chunk)
-        launches += 1
-        done = []
-        for item in active:
-            r, s, tr, ta, nbytes = item
-            got = (s.next_step - 1) - tr.steps
-            if got > chunk:
-                tr.skip(got - chunk)
-            if tr.update(s.reaction(chunk)):
-                done.append(item)
-        tnow = time.perf_counter() - t0
-        for item in done:
-            r, s, tr, ta, nbytes = item
-            batch.remove(s)
-            s.close()
-            used -= nbytes
-            active.remove(item)
-            results.append(Result(r.id, r.arrival, ta, tnow, tr.steps, tr.peak, tr.peak_step,
-                                  float(r.inp["nBonds"]) * tr.steps, np.concatenate(tr.hist)))
-    batch.close()
+            while pending and pending[0].arrival <= now:
+                r = pending[0]
+                est = device_bytes_estimate(r.inp, "sc" in r.inp)
+                if (active or creating) and used + reserved + est > hbm_budget:
+                    break                   # wait for a solve to finish
+                creating.append((r, pool.submit(_new_solver, r, precision, device), est))
+                reserved += est
+                pending.pop(0)
+            for item in list(creating):
+                r, fut, est = item
+                if fut.done() or not active:
+                    s = fut.result()
+                    nbytes = int(s.info()["device_bytes"])
+                    batch.add(s)
+                    used += nbytes
+                    reserved -= est
+                    active.append((r, s, _Track(r), time.perf_counter() - t0, nbytes))
+                    creating.remove(item)
+            if not active:
+                if pending:
+                    time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 0.05)))
+                continue
+            peak_members = max(peak_members, len(active))
+            if tune and not tuned and len(active) > 1:
+                batch.tune(max(1, chunk // 16))   # trials run real steps of every member
+                tuned = True
+            batch.step(chunk)
+            launches += 1
+            done = []
+            for item in active:
+                r, s, tr, ta, nbytes = item
+                got = (s.next_step - 1) - tr.steps
+                if got > chunk:
+                    tr.skip(got - chunk)
+                if tr.update(s.reaction(chunk)):
+                    done.append(item)
+            tnow = time.perf_counter() - t0
+            for item in done:
+                r, s, tr, ta, nbytes = item
+                batch.remove(s)
+                s.close()
+                used -= nbytes
+                active.remove(item)
+                results.append(Result(r.id, r.arrival, ta, tnow, tr.steps, tr.peak, tr.peak_step,
+                                      float(r.inp["nBonds"]) * tr.steps, np.concatenate(tr.hist)))
+    finally:
+        pool.shutdown(wait=True)
+        batch.close()
     wall = time.perf_counter() - t0
     return results, dict(wall=wall, launches=launches, peak_members=peak_members)
 

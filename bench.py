@@ -147,6 +147,108 @@ def cpu_reference_rate(inp, lawkw, budget_s, warmup, max_steps, kernels="referen
     return inp["nBonds"] * n / dt, n, dt, kind, threads
 
 
+def _batch_line(args, metric, unit, value, ms_step, config, extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+f64", "data": "synthetic",
+            "config": config}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args):
+    """The size-effect series (geometrically similar beams, log-uniform depths
+    50-400 mm, span/depth 5, width 50 mm, seeded lognormal sc, laws alternating
+    linear/trilinear) stepped together by one persistent batch launch replayed
+    from a CUDA graph, against the same beams stepped one at a time in plain
+    FP64."""
+    import bb_pd_b200 as bb
+    from bb_pd_b200 import serving
+    series = bb.beam.size_effect_series(args.members, dx=args.dx)
+    inps = [(bb.beam.build(sp), law) for sp, law in series]
+    nodes = [i["nNodes"] for i, _ in inps]
+    bonds = [i["nBonds"] for i, _ in inps]
+    tot_b = float(sum(bonds))
+    mk = lambda i, law, prec: bb.Solver(i, scheme="adr", rate=RATE, precision=prec, **serving.LAWKW[law])
+    sol = [mk(i, law, args.form) for i, law in inps]
+    batch = bb.Batch(args.form)
+    for s in sol:
+        batch.add(s)
+    bps, grab = batch.tune(max(1, args.warmup // 3))
+    batch.step(args.warmup)
+    clocks = Clocks(0)
+    clocks.start()
+    time.sleep(0.15)
+    batch.step(args.steps)          # graph replays from the second launch of this length on
+    batch.step(args.steps)
+    clk = clocks.stop()
+    ms = batch.last_kernel_ms()
+    info = batch.info()
+    batch.close()
+    value = tot_b * args.steps / (ms / 1e3)
+    # plain FP64, one beam at a time, same steps
+    seq_ms = 0.0
+    for s in sol:
+        s.close()
+    for i, law in inps:
+        s = mk(i, law, "fp64")
+        s.step(args.warmup)
+        s.step(args.steps)
+        seq_ms += s.last_kernel_ms()
+        s.close()
+    seq = tot_b * args.steps / (seq_ms / 1e3)
+    peak, kind = peak_hbm()
+    alg = sum(algorithmic_bytes(n, b, True) for n, b in zip(nodes, bonds))
+    ach = alg / (ms / args.steps / 1e3) / 1e9
+    config = {"workload": f"size-effect series: {args.members} beams, depth 50-400 mm log-uniform, span/depth 5, "
+                          f"width 50 mm, dx {args.dx * 1e3:g} mm, linear/trilinear, lognormal sc, ADR, "
+                          f"1e-7 mm/step", "nodes": int(sum(nodes)), "bonds": int(tot_b),
+              "min_nodes": int(min(nodes)), "max_nodes": int(max(nodes)), "form": args.form,
+              "l2": "inputs larger than L2", "parallelism": "1 GPU, one persistent batch launch"}
+    _batch_line(args, "bond-updates/s", "bond-updates/s", value, ms / args.steps, config, {
+        "sequential_plain_fp64": {"value": seq, "unit": "bond-updates/s", "ms_per_step": seq_ms / args.steps},
+        "speedup_vs_sequential_fp64": value / seq,
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                     "peak_kind": peak_kind_str(kind), "traffic": None},
+        "schedule": {"blocks_per_sm": bps, "grab": grab, "graph": bool(info["graph"])},
+        "gpu_launches": 1, "clocks": clk, "cpu_baseline": None, "e2e": None})
+
+
+def peak_kind_str(kind):
+    return f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else kind
+
+
+def run_serve(args):
+    """A Poisson stream of beam solves (node counts log-uniform, dx from
+    1.25/2.5/5 mm, law uniform over the four laws), each run until its load has
+    dropped to 80 % of its peak or the step cap; continuous batching under a
+    150 GB HBM budget against one plain FP64 solve at a time."""
+    import bb_pd_b200 as bb
+    from bb_pd_b200 import serving
+    stream = bb.beam.serving_stream(args.requests, nodes_range=(1e4, args.max_nodes), rate_hz=args.arrival_hz)
+    reqs = [serving.Request(k, r["arrival"], bb.beam.build(r["spec"]), r["law"], args.serve_rate, args.max_steps)
+            for k, r in enumerate(stream)]
+    clocks = Clocks(0)
+    clocks.start()
+    res, st = serving.run_batched(reqs, precision=args.form, chunk=100)
+    clk = clocks.stop()
+    seq, sst = serving.run_sequential(reqs, precision="fp64", chunk=100)
+    a, b = serving.summary(res, st), serving.summary(seq, sst)
+    peaks = {r.id: r for r in res}
+    peak_err = max((abs(peaks[r.id].peak - r.peak) / r.peak for r in seq if r.peak > 0), default=0.0)
+    reached = sum(1 for r in res if r.steps < args.max_steps)
+    config = {"workload": f"serving stream: {args.requests} Poisson arrivals at {args.arrival_hz} /s, nodes "
+                          f"log-uniform 1e4-{args.max_nodes:.0e}, dx 1.25/2.5/5 mm, four laws, to 80 % post-peak "
+                          f"load or {args.max_steps} steps, {abs(args.serve_rate) * 1e3:g} mm/step, HBM budget 150 GB",
+              "form": args.form, "parallelism": "1 GPU, continuous batching"}
+    _batch_line(args, "solves/h", "solves/h", a["solves_per_hour"], None, config, {
+        "batched": a, "sequential_plain_fp64": b,
+        "speedup_solves_per_hour": a["solves_per_hour"] / b["solves_per_hour"],
+        "p50_latency_s": a["p50_latency_s"], "p99_latency_s": a["p99_latency_s"],
+        "peak_load_rel_diff_vs_fp64_max": peak_err, "solves_past_peak": reached,
+        "gpu_launches": st["launches"], "clocks": clk, "cpu_baseline": None, "e2e": None})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -158,8 +260,22 @@ def main():
     ap.add_argument("--node-order", default="input", choices=["input", "morton", "tiled"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve"],
+                    help="single: one beam (--config); batch: the size-effect series in one "
+                         "persistent batch launch; serve: a Poisson stream of solves, continuous batching")
+    ap.add_argument("--members", type=int, default=64, help="batch: beams in the size-effect series")
+    ap.add_argument("--dx", type=float, default=5e-3, help="batch: lattice spacing of the series (m)")
+    ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")
+    ap.add_argument("--max-nodes", type=float, default=3e5, help="serve: largest beam (nodes)")
+    ap.add_argument("--arrival-hz", type=float, default=4.0, help="serve: Poisson arrival rate")
+    ap.add_argument("--max-steps", type=int, default=6000, help="serve: step cap per solve")
+    ap.add_argument("--serve-rate", type=float, default=-1e-7, help="serve: displacement per step (m)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload != "single" and args.impl == "ours":
+        if int(os.environ.get("RANK", "0")) == 0:
+            (run_batch if args.workload == "batch" else run_serve)(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

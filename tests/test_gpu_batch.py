@@ -144,9 +144,9 @@ def test_batch_rejections(beams):
 def test_serving_results_same_alone_and_in_mix(beams):
     """Requests arriving while others run are admitted into the running
     batch; each result (every per-step reaction) equals its solo run."""
-    reqs = [serving.Request(k, 0.02 * k, inp, law, rate=-3e-6, max_steps=steps)
-            for k, (inp, law, steps) in enumerate(zip(beams, ["trilinear", "bilinear", "exponential"],
-                                                        (120, 80, 100)))]
+    reqs = [serving.Request(k, arr, inp, law, rate=-3e-6, max_steps=steps)
+            for k, (inp, law, steps, arr) in enumerate(zip(beams, ["trilinear", "bilinear", "exponential"],
+                                                             (1200, 600, 800), (0.0, 0.0, 0.005)))]
     res, stats = serving.run_batched(reqs, chunk=20, tune=False)
     assert len(res) == 3
     seq, _ = serving.run_sequential(reqs, chunk=20)
