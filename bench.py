@@ -66,6 +66,23 @@ def measured_traffic(cfg, form):
         return None, None
 
 
+def max_over_ranks(x, dist, device=None):
+    """The largest of every rank's x (every rank gets it); x itself without a
+    process group. Timings of a multi-GPU run are the slowest rank's."""
+    if not dist:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(bonds_per_rank, steps, world, seconds):
+    """Whole-job bond-updates/s of `world` independent replicas, each evaluating
+    bonds_per_rank bonds for `steps` steps, timed by the slowest rank."""
+    return bonds_per_rank * steps * world / seconds
+
+
 def algorithmic_bytes(nN, nB, per_bond_sc):
     """Bytes one time step must move: per directed bond entry 4 B of neighbour
     index + 8 B of damage state (+ 8 B of per-bond critical stretch), per node
@@ -281,7 +298,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
-    if world > 1:
+    if args.impl == "reference" and rank != 0:
+        return                      # the CPU reference runs on rank 0 only
+    if world > 1 and args.impl == "ours":
         import torch
         import torch.distributed as dist
         import datetime
@@ -337,14 +356,11 @@ def main():
     s.sync()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = s.last_kernel_ms()
+    ms = max_over_ranks(s.last_kernel_ms(), dist, "cuda")
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     ms_step = ms / args.steps
-    value = nB * args.steps * world / (ms / 1e3)
+    value = replica_rate(nB, args.steps, world, ms / 1e3)
     s.close()
     del s
 
@@ -361,15 +377,12 @@ def main():
         torch.cuda.synchronize()
         te = time.perf_counter() - t0
         s2.close()
-        if dist:
-            t = torch.tensor([te], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+        te = max_over_ranks(te, dist, "cuda")
         h2d = sum(inp[k].nbytes for k in ("undeformedCoordinates", "BONDLIST", "UNDEFORMEDLENGTH",
                                            "BONDSTIFFNESS", "VOLUMECORRECTIONFACTORS", "massVector",
                                            "CONSTRAINTFLAG", "BODYFORCEFLAG")) + (inp["sc"].nbytes if per_bond_sc else 0)
         d2h = sum(o.nbytes for o in outs)
-        e2e = {"value": nB * args.steps * world / te, "unit": unit,
+        e2e = {"value": replica_rate(nB, args.steps, world, te), "unit": unit,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "seconds": te, "includes": "upload of the reference arrays, layout build, K steps, download of state"}
 
