@@ -584,24 +584,72 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
             if (q < nq) {
                 const uint32_t j = group_w(Gc, q) & COL_MASK;
                 xj[q] = x0[j]; yj[q] = x1[j]; zj[q] = x2[j];
+            } else {   // unused slot: finite values for the branch-free pass
+                xj[q] = xi + 1.0; yj[q] = yi; zj[q] = zi;
             }
         }
+        if constexpr (PREC == kP64) {
+            // pass 1: the fast path of all entries of the group, without
+            // branches, so that the four dependency chains interleave
+            double fx[4], fy[4], fz[4];
+            unsigned slow = 0;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (q < nq) {
-                Fetch f;
-                f.w = group_w(Gc, q);
-                f.c = Gc.cid(q);
-                f.sv = (Gc.s >> (8 * q)) & 0xFFu;
-                f.sc = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
-                f.xj = xj[q]; f.yj = yj[q]; f.zj = zj[q];
-                f.g = ldg_dict(d.dict, f.c);
-                const double3 r = entry_force<LAW, PREC>(d, e0 + q, f, safe, xi, yi, zi);
-                if (f.w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
-                    tx = tx + ax; ty = ty + ay; tz = tz + az;
-                    ax = 0.0; ay = 0.0; az = 0.0;
+            for (int q = 0; q < 4; q++) {
+                const bool valid = q < nq;
+                const uint32_t w = group_w(Gc, q), c = valid ? Gc.cid(q) : 0u, sv = (Gc.s >> (8 * q)) & 0xFFu;
+                const DictEntry g = ldg_dict(d.dict, c);
+                const double scv = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
+                const double s0b = d.s0e ? __ldg(d.s0e + e0 + q) : d.P.s0;
+                const int bt = (w >> BT_SHIFT) & 3;
+                const double dX = xj[q] - xi, dY = yj[q] - yi, dZ = zj[q] - zi;
+                const double L = sqrt(dX * dX + dY * dY + dZ * dZ);
+                const double s = quot_rn(L - g.l0, g.l0, g.rl0);
+                bool okr;
+                const double rL = recip_rn(L, okr);
+                const bool fast = safe && okr && sv == 0 && g.rl0 > 0 && L > 0 && law_quiet<LAW>(d.P, bt, s, s0b, scv);
+                const double t = ((g.bs * s) * d.V) * g.vcf;
+                fx[q] = t * quot_rn(dX, L, rL);
+                fy[q] = t * quot_rn(dY, L, rL);
+                fz[q] = t * quot_rn(dZ, L, rL);
+                if (valid && !fast) slow |= 1u << q;
+            }
+            // pass 2: the rare general entries, and the sum in the reference's order
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (q < nq) {
+                    const uint32_t w = group_w(Gc, q);
+                    double3 r = make_double3(fx[q], fy[q], fz[q]);
+                    if (slow & (1u << q)) {
+                        const uint32_t j = w & COL_MASK;
+                        const double scv = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
+                        r = entry_general<LAW, PREC>(d, e0 + q, w, (Gc.s >> (8 * q)) & 0xFFu,
+                                                     ldg_dict(d.dict, Gc.cid(q)), scv, xi, yi, zi, x0[j], x1[j], x2[j]);
+                    }
+                    if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
+                        tx = tx + ax; ty = ty + ay; tz = tz + az;
+                        ax = 0.0; ay = 0.0; az = 0.0;
+                    }
+                    ax = ax + r.x; ay = ay + r.y; az = az + r.z;
                 }
-                ax = ax + r.x; ay = ay + r.y; az = az + r.z;
+            }
+        } else {
+    #pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (q < nq) {
+                    Fetch f;
+                    f.w = group_w(Gc, q);
+                    f.c = Gc.cid(q);
+                    f.sv = (Gc.s >> (8 * q)) & 0xFFu;
+                    f.sc = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
+                    f.xj = xj[q]; f.yj = yj[q]; f.zj = zj[q];
+                    f.g = ldg_dict(d.dict, f.c);
+                    const double3 r = entry_force<LAW, PREC>(d, e0 + q, f, safe, xi, yi, zi);
+                    if (f.w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
+                        tx = tx + ax; ty = ty + ay; tz = tz + az;
+                        ax = 0.0; ay = 0.0; az = 0.0;
+                    }
+                    ax = ax + r.x; ay = ay + r.y; az = az + r.z;
+                }
             }
         }
         Gc = Gn;
@@ -647,7 +695,8 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
     if (i < nN) { ui = urh[i]; li = url[i]; }
     tx = 0.0; ty = 0.0; tz = 0.0;
     double ax = 0.0, ay = 0.0, az = 0.0;
-    const float s0f = (float)d.P.s0, guardf = (float)d.guard;
+    const float s0f = (float)d.P.s0, guardf = (float)d.guard, scf0 = (float)d.P.sc;
+    const float steelf = (float)d.P.sc_steel;
 
     const int ng = (dg + 3) >> 2;
     Group<CID> Gc, Gn;
@@ -660,40 +709,66 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
         float4 uj[4];
         float2 lj[4];
 #pragma unroll
-        for (int q = 0; q < 4; q++)
+        for (int q = 0; q < 4; q++) {
             if (q < nq) {
                 const uint32_t j = group_w(Gc, q) & COL_MASK;
                 uj[q] = urh[j];
                 lj[q] = url[j];
+            } else {   // unused slot: finite values for the branch-free pass
+                uj[q] = ui;
+                lj[q] = li;
             }
+        }
+        // pass 1: the fast path of all entries of the group, without branches,
+        // so that the four dependency chains interleave
+        float fxq[4], fyq[4], fzq[4];
+        unsigned slow = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const bool valid = q < nq;
+            const int64_t e = e0 + q;
+            const uint32_t w = group_w(Gc, q), c = valid ? Gc.cid(q) : 0u, sv = (Gc.s >> (8 * q)) & 0xFFu;
+            const int bt = (w >> BT_SHIFT) & 3;
+            const float4 A = __ldg(&d.dictx[2 * c]), Bv = __ldg(&d.dictx[2 * c + 1]);
+            const float etx = (uj[q].x - ui.x) + (uj[q].w - ui.w);
+            const float ety = (uj[q].y - ui.y) + (lj[q].x - li.x);
+            const float etz = (uj[q].z - ui.z) + (lj[q].y - li.y);
+            const float ex = A.x + etx, ey = A.y + ety, ez = A.z + etz;
+            const float L2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
+            const float rL = rsqrtf(L2);
+            const float L = L2 * rL;
+            const float num = __fmaf_rn(etz, A.z + ez, __fmaf_rn(ety, A.y + ey, __fmaf_rn(etx, A.x + ex, Bv.y)));
+            const float sf = __fdividef(num, A.w * (L + A.w));
+            // Fast iff the law is quiet and sf is outside the guard band round
+            // the critical stretch (band edges rounded outwards); a NaN
+            // stretch (zero, infinite or NaN length) fails every comparison.
+            const float scf = SCE ? (float)__ldcs(d.sce + e) : scf0;
+            bool fast;
+            if (LAW == BBPD_LAW_LINEAR) {
+                const float critf = (bt == 0) ? scf : (bt == 1 ? 3.f * scf : steelf);
+                fast = sf <= __fsub_rd(critf, guardf);
+            } else {
+                const float top = (bt == 0) ? (d.s0e ? (float)__ldg(d.s0e + e) : s0f) : INFINITY;
+                fast = sf <= top && (sf <= __fsub_rd(scf, guardf) || sf >= __fadd_ru(scf, guardf));
+            }
+            fast = fast && sv == 0 && Bv.z != 0.f;
+            const float qf = Bv.x * sf * rL;
+            fxq[q] = qf * ex;
+            fyq[q] = qf * ey;
+            fzq[q] = qf * ez;
+            if (valid && !fast) slow |= 1u << q;
+        }
+        // pass 2: the rare general entries, and the sum in the reference's order
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             if (q < nq) {
-                const int64_t e = e0 + q;
-                const uint32_t w = group_w(Gc, q), c = Gc.cid(q), sv = (Gc.s >> (8 * q)) & 0xFFu;
-                const double scd = SCE ? __ldcs(d.sce + e) : d.P.sc;
-                const int bt = (w >> BT_SHIFT) & 3;
-                const float4 A = __ldg(&d.dictx[2 * c]), Bv = __ldg(&d.dictx[2 * c + 1]);
-                const float etx = (uj[q].x - ui.x) + (uj[q].w - ui.w);
-                const float ety = (uj[q].y - ui.y) + (lj[q].x - li.x);
-                const float etz = (uj[q].z - ui.z) + (lj[q].y - li.y);
-                const float ex = A.x + etx, ey = A.y + ety, ez = A.z + etz;
-                const float L2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
-                const float rL = rsqrtf(L2);
-                const float L = L2 * rL;
-                const float num = __fmaf_rn(etz, A.z + ez, __fmaf_rn(ety, A.y + ey, __fmaf_rn(etx, A.x + ex, Bv.y)));
-                const float sf = __fdividef(num, A.w * (L + A.w));
-                const float crit = (float)((LAW == BBPD_LAW_LINEAR) ? linear_crit(d.P, bt, scd) : scd);
-                const float s0b = d.s0e ? (float)__ldg(d.s0e + e) : s0f;
-                const bool quiet = (LAW == BBPD_LAW_LINEAR) ? !(sf > crit) : !(bt == 0 && sf > s0b);
+                const uint32_t w = group_w(Gc, q);
                 double3 r;
-                if (sv == 0 && Bv.z != 0.f && L2 > 0.f && L2 < INFINITY && !(fabsf(sf - crit) < guardf) && quiet) {
-                    const float qf = Bv.x * sf * rL;
-                    r.x = (double)(qf * ex);
-                    r.y = (double)(qf * ey);
-                    r.z = (double)(qf * ez);
+                if (slow & (1u << q)) {
+                    const double scd = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
+                    r = entry_general_x<LAW>(d, e0 + q, w, (Gc.s >> (8 * q)) & 0xFFu, Gc.cid(q), scd, i, xs);
                 } else {
-                    r = entry_general_x<LAW>(d, e, w, sv, c, scd, i, xs);
+                    r = make_double3((double)fxq[q], (double)fyq[q], (double)fzq[q]);
                 }
                 if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
                     tx = tx + ax; ty = ty + ay; tz = tz + az;
