@@ -266,6 +266,67 @@ def run_serve(args):
         "gpu_launches": st["launches"], "clocks": clk, "cpu_baseline": None, "e2e": None})
 
 
+def run_precision(args):
+    """Error of the FP32 form against plain FP64: (1) one step from the same
+    FP64 state of the --config beam after --warmup steps: nodal force error
+    relative to the largest nodal force, and whether the broken-bond set is
+    the same; (2) the 500 x 100 x 50 mm beam (dx 5 mm) loaded at 1e-4 mm/step
+    in both forms until its load has dropped to 80 % of the peak: peak load,
+    its step, the largest load difference along the curve, and the broken-bond
+    sets at the end."""
+    import numpy as np
+    import bb_pd_b200 as bb
+    from bb_pd_b200 import serving
+    fn, wname = CONFIGS[args.config]
+    lawname, lawkw = law_for(args.config)
+    inp = bb.beam.build(getattr(bb.beam, fn)())
+    kw = dict(lawkw, scheme="adr", rate=RATE)
+    a = bb.Solver(inp, precision="fp64", **kw)
+    b = bb.Solver(inp, precision="fp32", **kw)
+    a.step(args.warmup)
+    b.restore(a.checkpoint())
+    a.step(1)
+    b.step(1)
+    Fa, Fb = a.get("force"), b.get("force")
+    ferr = float(np.abs(Fa - Fb).max() / np.abs(Fa).max())
+    same_broken = bool(np.array_equal(a.get("bsf") == 1, b.get("bsf") == 1) and
+                       np.array_equal(a.get("fail") == 0, b.get("fail") == 0))
+    a.close()
+    b.close()
+    # load-displacement to 20 % post-peak on the 20 000-node beam
+    inp1 = bb.beam.build(bb.beam.config1())
+    curves, broken = {}, {}
+    for form in ("fp64", "fp32"):
+        s = bb.Solver(inp1, precision=form, scheme="adr", rate=-1e-7, **serving.LAWKW["trilinear"])
+        tr = serving._Track(serving.Request(0, 0.0, inp1, "trilinear", -1e-7, 20000))
+        while True:
+            s.step(100)
+            if tr.update(s.reaction(100)):
+                break
+        curves[form] = (np.concatenate(tr.hist), tr.peak, tr.peak_step)
+        broken[form] = (s.get("bsf") == 1) | (s.get("fail") == 0)
+        s.close()
+    (ra, pa, sa), (rb, pb, sb) = curves["fp64"], curves["fp32"]
+    n = min(len(ra), len(rb))
+    line = {"metric": "fp32 nodal-force error vs fp64", "value": ferr, "unit": "max |dF| / max |F|",
+            "n_gpus": 1, "steps": 1, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"{wname}, {lawname}, ADR: one step from the FP64 state after "
+                                   f"{args.warmup} steps; load-displacement: 500x100x50 mm beam, dx 5 mm, "
+                                   f"trilinear, 1e-4 mm/step, to 80 % post-peak load"},
+            "broken_set_identical_one_step": same_broken,
+            "load_displacement": {"peak_load_fp64": pa, "peak_load_fp32": pb,
+                                  "peak_load_rel_diff": abs(pb - pa) / pa, "peak_step_fp64": sa,
+                                  "peak_step_fp32": sb,
+                                  "max_load_diff_rel_to_peak": float(np.abs(ra[:n] - rb[:n]).max() / pa),
+                                  "steps_fp64": len(ra), "steps_fp32": len(rb),
+                                  "broken_bonds_fp64": int(broken["fp64"].sum()),
+                                  "broken_bonds_fp32": int(broken["fp32"].sum()),
+                                  "broken_set_identical_at_end": bool(np.array_equal(broken["fp64"], broken["fp32"]))},
+            "gpu_launches": None, "cpu_baseline": None, "e2e": None, "roofline": None}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -277,7 +338,7 @@ def main():
     ap.add_argument("--node-order", default="input", choices=["input", "morton", "tiled"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "precision"],
                     help="single: one beam (--config); batch: the size-effect series in one "
                          "persistent batch launch; serve: a Poisson stream of solves, continuous batching")
     ap.add_argument("--members", type=int, default=64, help="batch: beams in the size-effect series")
@@ -291,7 +352,7 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.workload != "single" and args.impl == "ours":
         if int(os.environ.get("RANK", "0")) == 0:
-            (run_batch if args.workload == "batch" else run_serve)(args)
+            {"batch": run_batch, "serve": run_serve, "precision": run_precision}[args.workload](args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
