@@ -74,7 +74,8 @@ class Info(C.Structure):
 class BatchInfo(C.Structure):
     _fields_ = [
         ("n_members", C.c_int32), ("blocks_per_sm", C.c_int32), ("grab", C.c_int32),
-        ("graph", C.c_int32), ("total_slices", C.c_int64), ("device_bytes", C.c_int64),
+        ("graph", C.c_int32), ("n_classes", C.c_int32), ("reserved", C.c_int32),
+        ("total_slices", C.c_int64), ("device_bytes", C.c_int64),
     ]
 
 

@@ -382,18 +382,26 @@ __device__ __forceinline__ void load_group(const Dev &d, int64_t e0, Group<CID> 
     G.s = __ldcs(reinterpret_cast<const uint32_t *>(d.st + e0));
 }
 
-template <class CID, bool SCE>
+// Per-entry critical stretch: SCE 1 reads the per-entry stream, 0 takes the
+// scalar, 2 decides from the descriptor at run time (batch members).
+template <int SCE>
+__device__ __forceinline__ bool has_sce(const Dev &d)
+{
+    return SCE == 1 || (SCE == 2 && d.sce != nullptr);
+}
+
+template <class CID, int SCE>
 __device__ __forceinline__ void prefetch_group(const Dev &d, int64_t e0)
 {
     prefetch_l2(d.colw + e0);
     prefetch_l2(reinterpret_cast<const CID *>(d.cid) + e0);
     prefetch_l2(d.st + e0);
-    if (SCE) prefetch_l2(d.sce + e0);
+    if (has_sce<SCE>(d)) prefetch_l2(d.sce + e0);
 }
 
 // First groups of slice sl, prefetched before its turn (within the slice's
 // padded length).
-template <class CID, bool SCE>
+template <class CID, int SCE>
 __device__ __forceinline__ void prefetch_slice_head(const Dev &d, int64_t sl, int lane)
 {
     if (sl >= d.n_slices) return;
@@ -554,7 +562,7 @@ __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fe
 // of 4 at a time: the next group's streams load while the current group's 12
 // coordinate gathers are issued together and its entries computed. Returns the
 // node's force summed in the reference's order.
-template <int LAW, int PREC, class CID, bool SCE>
+template <int LAW, int PREC, class CID, int SCE>
 __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane, bool safe,
                                              const double *xs, double &tx, double &ty,
                                              double &tz)
@@ -598,7 +606,7 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
                 const bool valid = q < nq;
                 const uint32_t w = group_w(Gc, q), c = valid ? Gc.cid(q) : 0u, sv = (Gc.s >> (8 * q)) & 0xFFu;
                 const DictEntry g = ldg_dict(d.dict, c);
-                const double scv = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
+                const double scv = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
                 const double s0b = d.s0e ? __ldg(d.s0e + e0 + q) : d.P.s0;
                 const int bt = (w >> BT_SHIFT) & 3;
                 const double dX = xj[q] - xi, dY = yj[q] - yi, dZ = zj[q] - zi;
@@ -621,7 +629,7 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
                     double3 r = make_double3(fx[q], fy[q], fz[q]);
                     if (slow & (1u << q)) {
                         const uint32_t j = w & COL_MASK;
-                        const double scv = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
+                        const double scv = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
                         r = entry_general<LAW, PREC>(d, e0 + q, w, (Gc.s >> (8 * q)) & 0xFFu,
                                                      ldg_dict(d.dict, Gc.cid(q)), scv, xi, yi, zi, x0[j], x1[j], x2[j]);
                     }
@@ -640,7 +648,7 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
                     f.w = group_w(Gc, q);
                     f.c = Gc.cid(q);
                     f.sv = (Gc.s >> (8 * q)) & 0xFFu;
-                    f.sc = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
+                    f.sc = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
                     f.xj = xj[q]; f.yj = yj[q]; f.zj = zj[q];
                     f.g = ldg_dict(d.dict, f.c);
                     const double3 r = entry_force<LAW, PREC>(d, e0 + q, f, safe, xi, yi, zi);
@@ -680,7 +688,7 @@ __device__ __forceinline__ double3 entry_general_x(const Dev &d, int64_t e, uint
 // FP64 in the reference's order. Bonds whose stretch lies within the guard band
 // of the critical stretch, damaged or broken bonds and bonds whose law is active
 // take the general path with FP64 positions.
-template <int LAW, class CID, bool SCE>
+template <int LAW, class CID, int SCE>
 __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lane, const double *xs,
                                                const float4 *urh, const float2 *url, double &tx,
                                                double &ty, double &tz)
@@ -742,7 +750,7 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
             // Fast iff the law is quiet and sf is outside the guard band round
             // the critical stretch (band edges rounded outwards); a NaN
             // stretch (zero, infinite or NaN length) fails every comparison.
-            const float scf = SCE ? (float)__ldcs(d.sce + e) : scf0;
+            const float scf = has_sce<SCE>(d) ? (float)__ldcs(d.sce + e) : scf0;
             bool fast;
             if (LAW == BBPD_LAW_LINEAR) {
                 const float critf = (bt == 0) ? scf : (bt == 1 ? 3.f * scf : steelf);
@@ -765,7 +773,7 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
                 const uint32_t w = group_w(Gc, q);
                 double3 r;
                 if (slow & (1u << q)) {
-                    const double scd = SCE ? __ldcs(d.sce + e0 + q) : d.P.sc;
+                    const double scd = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
                     r = entry_general_x<LAW>(d, e0 + q, w, (Gc.s >> (8 * q)) & 0xFFu, Gc.cid(q), scd, i, xs);
                 } else {
                     r = make_double3((double)fxq[q], (double)fyq[q], (double)fzq[q]);
@@ -1263,12 +1271,13 @@ __global__ void __launch_bounds__(kBlock, 2) tstep_kernel(Dev d, int64_t step0, 
 
 // ---------------------------------------------------------------- batch kernel
 //
-// Many solver states ("members") of any sizes and laws stepped by one
-// persistent launch: phase A takes slices from one counter over the
-// concatenation of all members' slices (prefix[m] = first global slice of
-// member m), so the SMs stay busy however uneven the members are; every
-// member keeps its own step number, ADR tree, damping coefficient and
-// reaction history, and its arithmetic is that of a launch of its own.
+// Many solver states ("members") of any sizes stepped together: the members
+// of one class (same law and kernel variant) share one persistent launch, in
+// which phase A takes slices from one counter over the concatenation of all
+// members' slices (prefix[m] = first global slice of member m), so the SMs
+// stay busy however uneven the members are; every member keeps its own step
+// number, ADR tree, damping coefficient and reaction history, and its
+// arithmetic is that of a launch of its own.
 struct BatchCtl {
     const Dev *members;        // device copies of the members' descriptors
     const int64_t *prefix;     // S + 1 entries
@@ -1293,31 +1302,39 @@ __device__ __forceinline__ int member_of(const BatchCtl &B, int64_t w)
     return lo;
 }
 
-// One slice of one member, out of line so that each law instance gets its own
-// register allocation (the batch kernel dispatches on the member's law).
-template <int LAW, int PREC, bool SCE>
-__device__ __noinline__ void batch_slice(const Dev *dp, int64_t sl, int64_t n, int64_t it, int lane)
+// Copy member m's descriptor into this warp's shared slot (when it holds
+// another member). Reads through the slot cannot alias the state the kernel
+// stores to global memory, so the compiler keeps descriptor fields in
+// registers as it does for a kernel parameter.
+__device__ __forceinline__ const Dev &warp_member(const BatchCtl &B, int m, Dev *slot, int *held, int lane)
 {
-    const Dev &d = *dp;
-    const StepBufs b = step_bufs(d, n);
-    const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
-    double tx, ty, tz;
-    if (PREC == kP32X) slice_forces_x<LAW, uint16_t, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
-    else slice_forces<LAW, PREC, uint16_t, SCE>(d, sl, lane, safe, b.xs, tx, ty, tz);
-    finish_slice<BBPD_SCHEME_ADR, PREC>(d, b, sl, lane, tx, ty, tz, it);
+    if (*held != m) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(B.members + m);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(slot);
+        for (int k = lane; k < (int)(sizeof(Dev) / 4); k += 32) dst[k] = __ldg(src + k);
+        __syncwarp();
+        if (lane == 0) *held = m;
+        __syncwarp();
+    }
+    return *slot;
 }
 
-// FAM 0: FP64 members; FAM 1: FP32 members (dictionary-vector or difference form).
-template <int FAM>
+// The members of one class (one law, one kernel precision variant) stepped by
+// one persistent launch; a batch of mixed classes replays one such launch per
+// class. Every instance is as specialised as the single-solver kernel; the
+// per-entry critical stretch is decided from each member's descriptor.
+template <int LAW, int PREC>
 __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl B, int64_t nsteps)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ Dev s_dev[kBlock / 32];
+    __shared__ int s_held[kBlock / 32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t G = B.grab;
     const int64_t ngrabs = (B.total + G - 1) / G;
-    constexpr int P1 = FAM ? kP32X : kP64;
-    constexpr int P2 = FAM ? kP32D : kP64;
+    if (lane == 0) s_held[wib] = -1;
+    __syncwarp();
 
     for (int64_t it = 0; it < nsteps; it++) {
         // one failing grab per warp and step: ngrabs + nwarps values per step
@@ -1328,38 +1345,23 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
             const int64_t w1 = min(B.total, (gi + 1) * G);
             for (int64_t w = gi * G; w < w1; w++) {
                 const int m = member_of(B, w);
-                const Dev *dp = B.members + m;
+                const Dev &d = warp_member(B, m, &s_dev[wib], &s_held[wib], lane);
                 const int64_t sl = w - __ldg(&B.prefix[m]);
-                const int64_t n = __ldg(&B.mstep[m]) + it;
-                const int key = (FAM && dp->prec != kP32X ? 8 : 0) + dp->law * 2 + (dp->sce != nullptr);
-                switch (key) {
-                case 0: batch_slice<BBPD_LAW_LINEAR, P1, false>(dp, sl, n, it, lane); break;
-                case 1: batch_slice<BBPD_LAW_LINEAR, P1, true>(dp, sl, n, it, lane); break;
-                case 2: batch_slice<BBPD_LAW_BILINEAR, P1, false>(dp, sl, n, it, lane); break;
-                case 3: batch_slice<BBPD_LAW_BILINEAR, P1, true>(dp, sl, n, it, lane); break;
-                case 4: batch_slice<BBPD_LAW_TRILINEAR, P1, false>(dp, sl, n, it, lane); break;
-                case 5: batch_slice<BBPD_LAW_TRILINEAR, P1, true>(dp, sl, n, it, lane); break;
-                case 6: batch_slice<BBPD_LAW_EXPONENTIAL, P1, false>(dp, sl, n, it, lane); break;
-                case 7: batch_slice<BBPD_LAW_EXPONENTIAL, P1, true>(dp, sl, n, it, lane); break;
-                case 8: batch_slice<BBPD_LAW_LINEAR, P2, false>(dp, sl, n, it, lane); break;
-                case 9: batch_slice<BBPD_LAW_LINEAR, P2, true>(dp, sl, n, it, lane); break;
-                case 10: batch_slice<BBPD_LAW_BILINEAR, P2, false>(dp, sl, n, it, lane); break;
-                case 11: batch_slice<BBPD_LAW_BILINEAR, P2, true>(dp, sl, n, it, lane); break;
-                case 12: batch_slice<BBPD_LAW_TRILINEAR, P2, false>(dp, sl, n, it, lane); break;
-                case 13: batch_slice<BBPD_LAW_TRILINEAR, P2, true>(dp, sl, n, it, lane); break;
-                case 14: batch_slice<BBPD_LAW_EXPONENTIAL, P2, false>(dp, sl, n, it, lane); break;
-                default: batch_slice<BBPD_LAW_EXPONENTIAL, P2, true>(dp, sl, n, it, lane); break;
-                }
+                const StepBufs b = step_bufs(d, __ldg(&B.mstep[m]) + it);
+                const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
+                double tx, ty, tz;
+                if (PREC == kP32X) slice_forces_x<LAW, uint16_t, 2>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
+                else slice_forces<LAW, PREC, uint16_t, 2>(d, sl, lane, safe, b.xs, tx, ty, tz);
+                finish_slice<BBPD_SCHEME_ADR, PREC>(d, b, sl, lane, tx, ty, tz, it);
             }
             gi = gnext;
         }
         if (!grid_barrier_raw(B.bar, B.err, B.timeout_ns)) return;
         for (int64_t w = gwarp; w < B.total; w += nwarps) {
             const int m = member_of(B, w);
-            const Dev &d = B.members[m];
+            const Dev &d = warp_member(B, m, &s_dev[wib], &s_held[wib], lane);
             const StepBufs b = step_bufs(d, __ldg(&B.mstep[m]) + it);
-            if (FAM && d.prec == kP32X) adr_update_slice<kP32X>(d, b, w - __ldg(&B.prefix[m]), lane);
-            else adr_update_slice<kP64>(d, b, w - __ldg(&B.prefix[m]), lane);
+            adr_update_slice<PREC>(d, b, w - __ldg(&B.prefix[m]), lane);
         }
         if (!grid_barrier_raw(B.bar, B.err, B.timeout_ns)) return;
     }
@@ -1369,6 +1371,24 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
 }
 
 typedef void (*batch_kernel_t)(BatchCtl, int64_t);
+
+template <int PREC>
+batch_kernel_t pick_batch_law(int law)
+{
+    switch (law) {
+    case BBPD_LAW_LINEAR: return batch_kernel<BBPD_LAW_LINEAR, PREC>;
+    case BBPD_LAW_BILINEAR: return batch_kernel<BBPD_LAW_BILINEAR, PREC>;
+    case BBPD_LAW_TRILINEAR: return batch_kernel<BBPD_LAW_TRILINEAR, PREC>;
+    default: return batch_kernel<BBPD_LAW_EXPONENTIAL, PREC>;
+    }
+}
+
+batch_kernel_t pick_batch_kernel(int law, int prec)
+{
+    if (prec == kP32X) return pick_batch_law<kP32X>(law);
+    if (prec == kP32D) return pick_batch_law<kP32D>(law);
+    return pick_batch_law<kP64>(law);
+}
 
 // Self-test of the bounded wait: one thread waits on a word that nothing
 // writes, so the wait must expire and report ERR_TIMEOUT.
@@ -2500,30 +2520,50 @@ extern "C" int bbpd_get_info(bbpd_solver *S, bbpd_info *info)
 
 // ------------------------------------------------------------------ batches
 
+// One class of batch members: same law and kernel precision variant, stepped
+// by one persistent launch of its own specialised kernel.
+struct BatchClass {
+    int law = 0, prec = kP64;
+    batch_kernel_t kernel = nullptr;
+    std::vector<bbpd_solver *> members;
+    Dev *d_members = nullptr;
+    int64_t *d_prefix = nullptr, *d_mstep = nullptr;
+    size_t cap = 0;
+    unsigned long long *work = nullptr;
+    int occ = 0;
+    BatchCtl ctl{};
+
+    void release()
+    {
+        for (void *p : {(void *)d_members, (void *)d_prefix, (void *)d_mstep, (void *)work})
+            if (p) cudaFree(p);
+        d_members = nullptr;
+        d_prefix = d_mstep = nullptr;
+        work = nullptr;
+        cap = 0;
+    }
+};
+
 struct bbpd_batch {
     int device = 0;
     int prec = kP64;                       // kP64: FP64 members; kP32X: FP32 members (either FP32 variant)
     std::vector<bbpd_solver *> members;
-    bool dirty = true;                     // member table must be rebuilt before the next launch
-    Dev *d_members = nullptr;
-    int64_t *d_prefix = nullptr, *d_mstep = nullptr;
-    size_t cap = 0;                        // members the device tables hold
+    bool dirty = true;                     // class tables must be rebuilt before the next launch
+    std::vector<BatchClass> classes;       // non-empty classes of the current membership
     unsigned *bar = nullptr;
-    unsigned long long *work = nullptr;
     int *err = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    batch_kernel_t kernel = nullptr;
-    int nsm = 0, occ = 0;                  // SMs, resident blocks per SM
+    int nsm = 0, occ = 0;                  // SMs, resident blocks per SM (smallest over the kernels)
     int blocks_per_sm = 0;                 // schedule: resident blocks used per SM
     int grab = 1;                          // schedule: slices per counter grab
     bool tuned = false;
     int64_t total = 0;
-    BatchCtl ctl{};
-    bool use_graph = true;                 // replay the launch from a captured CUDA graph
+    double timeout_s = 2.0;
+    bool use_graph = true;                 // replay the launches from a captured CUDA graph
     cudaGraphExec_t gexec = nullptr;
     int64_t g_nsteps = -1;
-    int g_grid = 0, g_grab = 0;
+    int g_bps = 0, g_grab = 0;
     bool last_graph = false;
 
     void drop_graph()
@@ -2537,7 +2577,8 @@ struct bbpd_batch {
         cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
         drop_graph();
-        for (void *p : {(void *)d_members, (void *)d_prefix, (void *)d_mstep, (void *)bar, (void *)work, (void *)err})
+        for (BatchClass &c : classes) c.release();
+        for (void *p : {(void *)bar, (void *)err})
             if (p) cudaFree(p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -2568,10 +2609,8 @@ extern "C" int bbpd_batch_create(int device, int precision, bbpd_batch **out)
     std::unique_ptr<bbpd_batch> guard_(B);
     B->device = device;
     B->prec = precision == BBPD_PREC_FP32 ? kP32X : kP64;
-    B->kernel = B->prec == kP32X ? batch_kernel<1> : batch_kernel<0>;
     BBPD_CUDA_TRY(cudaMalloc((void **)&B->bar, 2 * sizeof(unsigned)));
     BBPD_CUDA_TRY(cudaMemset(B->bar, 0, 2 * sizeof(unsigned)));
-    BBPD_CUDA_TRY(cudaMalloc((void **)&B->work, sizeof(unsigned long long)));
     BBPD_CUDA_TRY(cudaMalloc((void **)&B->err, sizeof(int)));
     BBPD_CUDA_TRY(cudaMemset(B->err, 0, sizeof(int)));
     BBPD_CUDA_TRY(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
@@ -2581,9 +2620,18 @@ extern "C" int bbpd_batch_create(int device, int precision, bbpd_batch **out)
     BBPD_CUDA_TRY(cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, device));
     BBPD_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
     if (!coop) return fail(BBPD_ERR_UNSUPPORTED, "device lacks cooperative launch");
-    BBPD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B->occ, (const void *)B->kernel, kBlock, 0));
-    if (B->occ < 1) return fail(BBPD_ERR_CUDA, "batch kernel cannot be resident");
-    B->blocks_per_sm = B->occ;
+    // resident blocks per SM: the smallest over the kernels this batch may run
+    int occ = 1 << 30;
+    for (int law = 0; law < 4; law++)
+        for (int pv : {kP64, kP32X, kP32D}) {
+            if ((pv == kP64) != (B->prec == kP64)) continue;
+            int o = 0;
+            BBPD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void *)pick_batch_kernel(law, pv), kBlock, 0));
+            occ = std::min(occ, o);
+        }
+    if (occ < 1) return fail(BBPD_ERR_CUDA, "batch kernel cannot be resident");
+    B->occ = occ;
+    B->blocks_per_sm = occ;
     *out = guard_.release();
     return BBPD_OK;
 }
@@ -2606,6 +2654,7 @@ extern "C" int bbpd_batch_add(bbpd_batch *B, bbpd_solver *S)
         return fail(BBPD_ERR_UNSUPPORTED, "batch members need 16-bit dictionary ids and input or Morton node order");
     BBPD_CUDA_TRY(cudaSetDevice(S->device));
     BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(B->stream));
     B->members.push_back(S);
     S->batch = B;
     B->dirty = true;
@@ -2625,79 +2674,121 @@ extern "C" int bbpd_batch_remove(bbpd_batch *B, bbpd_solver *S)
     return BBPD_OK;
 }
 
-// Device copies of the member descriptors, slice prefix and step numbers.
+// Class tables (member descriptors, slice prefix, step numbers) of the
+// current membership, members grouped by (precision variant, law) in the
+// order they joined.
 static int batch_rebuild(bbpd_batch *B)
 {
-    const size_t S = B->members.size();
-    if (S > B->cap) {
-        for (void *p : {(void *)B->d_members, (void *)B->d_prefix, (void *)B->d_mstep})
-            if (p) cudaFree(p);
-        B->d_members = nullptr;
-        B->d_prefix = B->d_mstep = nullptr;
-        const size_t c = std::max<size_t>(S, 2 * B->cap);
-        BBPD_CUDA_TRY(cudaMalloc((void **)&B->d_members, sizeof(Dev) * c));
-        BBPD_CUDA_TRY(cudaMalloc((void **)&B->d_prefix, sizeof(int64_t) * (c + 1)));
-        BBPD_CUDA_TRY(cudaMalloc((void **)&B->d_mstep, sizeof(int64_t) * c));
-        B->cap = c;
+    std::vector<BatchClass> old;
+    old.swap(B->classes);
+    for (bbpd_solver *S : B->members) {
+        BatchClass *c = nullptr;
+        for (BatchClass &k : B->classes)
+            if (k.law == S->prm.law && k.prec == S->prec) c = &k;
+        if (!c) {
+            B->classes.emplace_back();
+            c = &B->classes.back();
+            c->law = S->prm.law;
+            c->prec = S->prec;
+            c->kernel = pick_batch_kernel(c->law, c->prec);
+            // reuse the device tables of the same class from before
+            for (BatchClass &o : old)
+                if (o.law == c->law && o.prec == c->prec && o.cap) {
+                    c->d_members = o.d_members;
+                    c->d_prefix = o.d_prefix;
+                    c->d_mstep = o.d_mstep;
+                    c->work = o.work;
+                    c->cap = o.cap;
+                    o.cap = 0;
+                    o.d_members = nullptr;
+                    o.d_prefix = o.d_mstep = nullptr;
+                    o.work = nullptr;
+                }
+        }
+        c->members.push_back(S);
     }
-    std::vector<Dev> devs(S);
-    std::vector<int64_t> prefix(S + 1, 0), mstep(S);
-    for (size_t m = 0; m < S; m++) {
-        devs[m] = B->members[m]->d;
-        prefix[m + 1] = prefix[m] + B->members[m]->ns;
-        mstep[m] = B->members[m]->step;
-    }
-    if (S) {
-        BBPD_CUDA_TRY(cudaMemcpy(B->d_members, devs.data(), sizeof(Dev) * S, cudaMemcpyHostToDevice));
-        BBPD_CUDA_TRY(cudaMemcpy(B->d_mstep, mstep.data(), sizeof(int64_t) * S, cudaMemcpyHostToDevice));
-    }
-    BBPD_CUDA_TRY(cudaMemcpy(B->d_prefix, prefix.data(), sizeof(int64_t) * (S + 1), cudaMemcpyHostToDevice));
-    B->total = prefix[S];
-    BatchCtl &c = B->ctl;
-    c.members = B->d_members;
-    c.prefix = B->d_prefix;
-    c.mstep = B->d_mstep;
-    c.S = (int)S;
-    c.total = B->total;
-    c.bar = B->bar;
-    c.work = B->work;
-    c.err = B->err;
-    double to = 0;
-    for (bbpd_solver *M : B->members) to = std::max(to, M->prm.barrier_timeout_s > 0 ? M->prm.barrier_timeout_s : 2.0);
-    c.timeout_ns = (unsigned long long)((to > 0 ? to : 2.0) * 1e9);
+    for (BatchClass &o : old) o.release();
     B->drop_graph();
+    B->total = 0;
+    double to = 0;
+    for (BatchClass &c : B->classes) {
+        const size_t S = c.members.size();
+        if (S > c.cap) {
+            c.release();
+            const size_t cap = std::max<size_t>(S, 8);
+            BBPD_CUDA_TRY(cudaMalloc((void **)&c.d_members, sizeof(Dev) * cap));
+            BBPD_CUDA_TRY(cudaMalloc((void **)&c.d_prefix, sizeof(int64_t) * (cap + 1)));
+            BBPD_CUDA_TRY(cudaMalloc((void **)&c.d_mstep, sizeof(int64_t) * cap));
+            BBPD_CUDA_TRY(cudaMalloc((void **)&c.work, sizeof(unsigned long long)));
+            c.cap = cap;
+        }
+        std::vector<Dev> devs(S);
+        std::vector<int64_t> prefix(S + 1, 0), mstep(S);
+        for (size_t m = 0; m < S; m++) {
+            devs[m] = c.members[m]->d;
+            prefix[m + 1] = prefix[m] + c.members[m]->ns;
+            mstep[m] = c.members[m]->step;
+            const double t = c.members[m]->prm.barrier_timeout_s;
+            to = std::max(to, t > 0 ? t : 2.0);
+        }
+        BBPD_CUDA_TRY(cudaMemcpy(c.d_members, devs.data(), sizeof(Dev) * S, cudaMemcpyHostToDevice));
+        BBPD_CUDA_TRY(cudaMemcpy(c.d_mstep, mstep.data(), sizeof(int64_t) * S, cudaMemcpyHostToDevice));
+        BBPD_CUDA_TRY(cudaMemcpy(c.d_prefix, prefix.data(), sizeof(int64_t) * (S + 1), cudaMemcpyHostToDevice));
+        c.ctl.members = c.d_members;
+        c.ctl.prefix = c.d_prefix;
+        c.ctl.mstep = c.d_mstep;
+        c.ctl.S = (int)S;
+        c.ctl.total = prefix[S];
+        c.ctl.bar = B->bar;
+        c.ctl.work = c.work;
+        c.ctl.err = B->err;
+        B->total += prefix[S];
+    }
+    B->timeout_s = to > 0 ? to : 2.0;
+    for (BatchClass &c : B->classes) c.ctl.timeout_ns = (unsigned long long)(B->timeout_s * 1e9);
     B->dirty = false;
     return BBPD_OK;
 }
 
-// Enqueue one launch of nsteps steps with the given schedule (graph replay
-// when enabled and the capture succeeds, a direct launch otherwise).
+// Enqueue the launches of every class for nsteps steps with the given
+// schedule: counter reset and one persistent launch per class.
+static int batch_enqueue(bbpd_batch *B, int64_t nsteps, int blocks_per_sm, int grab)
+{
+    for (BatchClass &c : B->classes) {
+        int64_t want = (c.ctl.total * 32 + kBlock - 1) / kBlock;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)B->nsm * blocks_per_sm, want));
+        c.ctl.grab = grab;
+        void *args[] = {(void *)&c.ctl, (void *)&nsteps};
+        BBPD_CUDA_TRY(cudaMemsetAsync(c.work, 0, sizeof(unsigned long long), B->stream));
+        BBPD_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)c.kernel, dim3(grid), dim3(kBlock), args, 0, B->stream));
+    }
+    return BBPD_OK;
+}
+
+// Launch nsteps steps of every member: graph replay when enabled and the
+// capture succeeds, direct launches otherwise.
 static int batch_launch(bbpd_batch *B, int64_t nsteps, int blocks_per_sm, int grab, bool graph)
 {
-    int64_t want = (B->total * 32 + kBlock - 1) / kBlock;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)B->nsm * blocks_per_sm, want));
-    B->ctl.grab = grab;
-    void *args[] = {(void *)&B->ctl, (void *)&nsteps};
     B->last_graph = false;
     if (graph && B->use_graph) {
-        if (!B->gexec || B->g_nsteps != nsteps || B->g_grid != grid || B->g_grab != grab) {
+        if (!B->gexec || B->g_nsteps != nsteps || B->g_bps != blocks_per_sm || B->g_grab != grab) {
             B->drop_graph();
             cudaGraph_t g = nullptr;
             bool ok = cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
             if (ok) {
-                cudaMemsetAsync(B->work, 0, sizeof(unsigned long long), B->stream);
-                cudaLaunchCooperativeKernel((const void *)B->kernel, dim3(grid), dim3(kBlock), args, 0, B->stream);
-                ok = cudaStreamEndCapture(B->stream, &g) == cudaSuccess && g;
+                const int rc = batch_enqueue(B, nsteps, blocks_per_sm, grab);
+                ok = cudaStreamEndCapture(B->stream, &g) == cudaSuccess && g && rc == BBPD_OK;
             }
             if (ok) ok = cudaGraphInstantiate(&B->gexec, g, 0) == cudaSuccess;
             if (g) cudaGraphDestroy(g);
-            if (!ok) {   // capture of this launch is not available here: launch directly from now on
+            if (!ok) {   // capture of these launches is not available here: launch directly from now on
                 cudaGetLastError();
+                clear_error();
                 B->drop_graph();
                 B->use_graph = false;
             } else {
                 B->g_nsteps = nsteps;
-                B->g_grid = grid;
+                B->g_bps = blocks_per_sm;
                 B->g_grab = grab;
             }
         }
@@ -2709,14 +2800,13 @@ static int batch_launch(bbpd_batch *B, int64_t nsteps, int blocks_per_sm, int gr
             return BBPD_OK;
         }
     }
-    BBPD_CUDA_TRY(cudaMemsetAsync(B->work, 0, sizeof(unsigned long long), B->stream));
     BBPD_CUDA_TRY(cudaEventRecord(B->ev0, B->stream));
-    BBPD_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)B->kernel, dim3(grid), dim3(kBlock), args, 0, B->stream));
+    TRY(batch_enqueue(B, nsteps, blocks_per_sm, grab));
     BBPD_CUDA_TRY(cudaEventRecord(B->ev1, B->stream));
     return BBPD_OK;
 }
 
-// Wait for the launch, then account it to every member: step numbers, and
+// Wait for the launches, then account them to every member: step numbers, and
 // error flags (the batch's barrier flag and each member's own flag).
 static int batch_finish(bbpd_batch *B, int64_t nsteps)
 {
@@ -2726,7 +2816,7 @@ static int batch_finish(bbpd_batch *B, int64_t nsteps)
     if (h) {
         int z = 0;
         BBPD_CUDA_TRY(cudaMemcpy(B->err, &z, sizeof(int), cudaMemcpyHostToDevice));
-        B->dirty = true;   // step numbers on the device were not advanced
+        B->dirty = true;   // step numbers on the device may not have advanced
         return fail(BBPD_ERR_TIMEOUT, "batch grid barrier wait exceeded its limit; kernel returned early");
     }
     int bad = -1;
@@ -2771,7 +2861,6 @@ extern "C" int bbpd_batch_tune(bbpd_batch *B, int64_t nsteps_per_trial, int *blo
         for (int g : {1, 2, 4}) {
             TRY(batch_launch(B, nsteps_per_trial, bps, g, false));
             TRY(batch_finish(B, nsteps_per_trial));
-            TRY(batch_rebuild(B));   // step numbers on the host are authoritative
             float ms = 0;
             BBPD_CUDA_TRY(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
             if (first || ms < best) {
@@ -2784,6 +2873,7 @@ extern "C" int bbpd_batch_tune(bbpd_batch *B, int64_t nsteps_per_trial, int *blo
     B->blocks_per_sm = bb;
     B->grab = bg;
     B->tuned = true;
+    B->drop_graph();
     if (blocks_per_sm) *blocks_per_sm = bb;
     if (grab) *grab = bg;
     return BBPD_OK;
@@ -2808,6 +2898,7 @@ extern "C" int bbpd_batch_get_info(bbpd_batch *B, bbpd_batch_info *info)
     info->grab = B->grab;
     info->graph = B->last_graph ? 1 : 0;
     info->total_slices = B->total;
+    info->n_classes = (int32_t)B->classes.size();
     int64_t bytes = 0;
     for (bbpd_solver *S : B->members) bytes += S->device_bytes;
     info->device_bytes = bytes;

@@ -321,7 +321,9 @@ int bbpd_get_reaction(bbpd_solver *s, int64_t n, double *host_out);
  * Serving and batching form. Members keep their own state, step number,
  * damping coefficient and reaction history, and compute exactly what a solo
  * launch computes (results are bit-identical alone and in a batch); the batch
- * only shares the SMs: slices of all members are taken from one work counter.
+ * only shares the SMs. Members are grouped in classes (law x kernel
+ * variant); each class is one persistent launch of a kernel specialised for
+ * it, whose warps take slices of all its members from one work counter.
  * Members: ADR solvers of the batch's precision form, 16-bit dictionary ids,
  * input or Morton node order. Membership may change between launches
  * (continuous batching); a launch is captured into a CUDA graph and replayed
@@ -332,6 +334,8 @@ typedef struct bbpd_batch_info {
     int32_t blocks_per_sm;     /* schedule in use */
     int32_t grab;              /* slices taken per work-counter grab */
     int32_t graph;             /* 1 if the last launch replayed a CUDA graph */
+    int32_t n_classes;         /* member classes (law x kernel variant): one launch each */
+    int32_t reserved;
     int64_t total_slices;
     int64_t device_bytes;      /* device memory held by the members */
 } bbpd_batch_info;
