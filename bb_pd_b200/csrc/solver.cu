@@ -88,7 +88,9 @@ constexpr int kTileCapMax = 4096;        // staged nodes per tile (12-bit local 
 constexpr int kDictCache = 1024;         // dictionary entries kept in shared memory
 
 // Kernel precision variants. The FP32 form runs as kP32X when the bond vectors
-// compress into the dictionary and as kP32D (FP64 differences) otherwise.
+// compress into its dictionary (16-bit ids); otherwise the solver runs the
+// FP64 kernel, which is faster there than FP32 arithmetic on FP64 differences.
+// kP32D (FP64 differences, FP32 force) is the FP32 form's general path.
 constexpr int kP64 = 0, kP32D = 1, kP32X = 2;
 
 // Entry k of the list of lane `lane` in the slice whose entries start at sbase:
@@ -102,8 +104,7 @@ __host__ __device__ __forceinline__ int64_t entry_pos(int64_t sbase, int64_t k, 
 
 // One dictionary entry: the bond constants in FP64 and RN(1/L0) for the
 // shared-divisor division. rl0 is set to -1 when a constant is not finite or
-// L0 lies outside [2^-100, 2^100]: entries using it take the general path. A
-// parallel float table holds BONDSTIFFNESS * cellVolume * VCF for the FP32 form.
+// L0 lies outside [2^-100, 2^100]: entries using it take the general path.
 struct DictEntry {
     double l0, rl0, vcf, bs;
 };
@@ -124,7 +125,6 @@ struct Dev {
     uint8_t *st;
     double *bsf;
     const DictEntry *dict;
-    const float *dict32;             // BONDSTIFFNESS * cellVolume * VCF per dictionary entry (FP32 form)
     const float4 *dictx;             // FP32 form, 2 per entry: (xi_x, xi_y, xi_z, L0), (k32, |xi|^2-L0^2, regular, 0)
     float4 *urh0, *urh1;             // FP32 form: per node (uh_x, uh_y, uh_z, ul_x), ping-pong like positions
     float2 *url0, *url1;             // FP32 form: per node (ul_y, ul_z); uh + ul is the FP32 split of u
@@ -504,7 +504,7 @@ __device__ BBPD_GENERAL_ATTR double3 entry_general(const Dev &d, int64_t e, uint
     return f;
 }
 
-// Force of one entry. The common case, an intact and undamaged bond whose law
+// Force of one entry (FP64). The common case, an intact and undamaged bond whose law
 // stays quiet, is computed inline: with fail = 1 and BSF = 0 the reference
 // product fail*BS*(1-BSF)*s*V*VCF rounds exactly like ((BS*s)*V)*VCF, and with
 // 0 < L < inf and a regular dictionary entry (rl0 > 0) no NaN can arise.
@@ -515,7 +515,7 @@ __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fe
     const int bt = (f.w >> BT_SHIFT) & 3;
     const double s0b = d.s0e ? __ldg(d.s0e + e) : d.P.s0;
     double3 r;
-    if (PREC == kP64) {
+    {
         // calculatedeformedlengthMex.c:37-43 with its division by L0 and the
         // three of calculatebondforcesMex.c:34-36 by L done as correctly
         // rounded quotients with shared reciprocals (divide.cuh): bit-identical
@@ -533,31 +533,11 @@ __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fe
             r.z = t * quot_rn(dZ, L, rL);
             return r;
         }
-    } else {
-        // FP64 difference and squared length (no cancellation loss), FP32 rest:
-        // s = (L^2 - L0^2) / (L0 (L + L0)); FP64 sums of the FP32 forces.
-        const double dX = f.xj - xi, dY = f.yj - yi, dZ = f.zj - zi;
-        const double L2 = dX * dX + dY * dY + dZ * dZ;
-        const double diff = L2 - f.g.l0 * f.g.l0;
-        const float L2f = (float)L2, l0f = (float)f.g.l0;
-        const float ri = rsqrtf(L2f);
-        const float Lf = L2f * ri;
-        const float sf = __fdividef((float)diff, l0f * (Lf + l0f));
-        const double crit = (LAW == BBPD_LAW_LINEAR) ? linear_crit(d.P, bt, f.sc) : f.sc;
-        // guard band: near the critical stretch the general path decides in FP64
-        if (f.sv == 0 && f.g.rl0 > 0 && L2f > 0.f && L2f < INFINITY &&
-            !(fabs((double)sf - crit) < d.guard) && law_quiet<LAW>(d.P, bt, (double)sf, s0b, f.sc)) {
-            const float q = __ldg(&d.dict32[f.c]) * sf * ri;
-            r.x = (double)(q * (float)dX);
-            r.y = (double)(q * (float)dY);
-            r.z = (double)(q * (float)dZ);
-            return r;
-        }
     }
     return entry_general<LAW, PREC>(d, e, f.w, f.sv, f.g, f.sc, xi, yi, zi, f.xj, f.yj, f.zj);
 }
 
-// Forces of the 32 nodes of one slice (FP64 form and FP32 difference form).
+// Forces of the 32 nodes of one slice (FP64 form).
 // Lane `lane` owns node sl*32+lane and walks its entries in bond order, a group
 // of 4 at a time: the next group's streams load while the current group's 12
 // coordinate gathers are issued together and its entries computed. Returns the
@@ -596,68 +576,47 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
                 xj[q] = xi + 1.0; yj[q] = yi; zj[q] = zi;
             }
         }
-        if constexpr (PREC == kP64) {
-            // pass 1: the fast path of all entries of the group, without
-            // branches, so that the four dependency chains interleave
-            double fx[4], fy[4], fz[4];
-            unsigned slow = 0;
+        // pass 1: the fast path of all entries of the group, without
+        // branches, so that the four dependency chains interleave
+        double fx[4], fy[4], fz[4];
+        unsigned slow = 0;
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const bool valid = q < nq;
-                const uint32_t w = group_w(Gc, q), c = valid ? Gc.cid(q) : 0u, sv = (Gc.s >> (8 * q)) & 0xFFu;
-                const DictEntry g = ldg_dict(d.dict, c);
-                const double scv = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
-                const double s0b = d.s0e ? __ldg(d.s0e + e0 + q) : d.P.s0;
-                const int bt = (w >> BT_SHIFT) & 3;
-                const double dX = xj[q] - xi, dY = yj[q] - yi, dZ = zj[q] - zi;
-                const double L = sqrt(dX * dX + dY * dY + dZ * dZ);
-                const double s = quot_rn(L - g.l0, g.l0, g.rl0);
-                bool okr;
-                const double rL = recip_rn(L, okr);
-                const bool fast = safe && okr && sv == 0 && g.rl0 > 0 && L > 0 && law_quiet<LAW>(d.P, bt, s, s0b, scv);
-                const double t = ((g.bs * s) * d.V) * g.vcf;
-                fx[q] = t * quot_rn(dX, L, rL);
-                fy[q] = t * quot_rn(dY, L, rL);
-                fz[q] = t * quot_rn(dZ, L, rL);
-                if (valid && !fast) slow |= 1u << q;
-            }
-            // pass 2: the rare general entries, and the sum in the reference's order
+        for (int q = 0; q < 4; q++) {
+            const bool valid = q < nq;
+            const uint32_t w = group_w(Gc, q), c = valid ? Gc.cid(q) : 0u, sv = (Gc.s >> (8 * q)) & 0xFFu;
+            const DictEntry g = ldg_dict(d.dict, c);
+            const double scv = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
+            const double s0b = d.s0e ? __ldg(d.s0e + e0 + q) : d.P.s0;
+            const int bt = (w >> BT_SHIFT) & 3;
+            const double dX = xj[q] - xi, dY = yj[q] - yi, dZ = zj[q] - zi;
+            const double L = sqrt(dX * dX + dY * dY + dZ * dZ);
+            const double s = quot_rn(L - g.l0, g.l0, g.rl0);
+            bool okr;
+            const double rL = recip_rn(L, okr);
+            const bool fast = safe && okr && sv == 0 && g.rl0 > 0 && L > 0 && law_quiet<LAW>(d.P, bt, s, s0b, scv);
+            const double t = ((g.bs * s) * d.V) * g.vcf;
+            fx[q] = t * quot_rn(dX, L, rL);
+            fy[q] = t * quot_rn(dY, L, rL);
+            fz[q] = t * quot_rn(dZ, L, rL);
+            if (valid && !fast) slow |= 1u << q;
+        }
+        // pass 2: the rare general entries, and the sum in the reference's order
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                if (q < nq) {
-                    const uint32_t w = group_w(Gc, q);
-                    double3 r = make_double3(fx[q], fy[q], fz[q]);
-                    if (slow & (1u << q)) {
-                        const uint32_t j = w & COL_MASK;
-                        const double scv = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
-                        r = entry_general<LAW, PREC>(d, e0 + q, w, (Gc.s >> (8 * q)) & 0xFFu,
-                                                     ldg_dict(d.dict, Gc.cid(q)), scv, xi, yi, zi, x0[j], x1[j], x2[j]);
-                    }
-                    if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
-                        tx = tx + ax; ty = ty + ay; tz = tz + az;
-                        ax = 0.0; ay = 0.0; az = 0.0;
-                    }
-                    ax = ax + r.x; ay = ay + r.y; az = az + r.z;
+        for (int q = 0; q < 4; q++) {
+            if (q < nq) {
+                const uint32_t w = group_w(Gc, q);
+                double3 r = make_double3(fx[q], fy[q], fz[q]);
+                if (slow & (1u << q)) {
+                    const uint32_t j = w & COL_MASK;
+                    const double scv = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
+                    r = entry_general<LAW, PREC>(d, e0 + q, w, (Gc.s >> (8 * q)) & 0xFFu,
+                                                 ldg_dict(d.dict, Gc.cid(q)), scv, xi, yi, zi, x0[j], x1[j], x2[j]);
                 }
-            }
-        } else {
-    #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                if (q < nq) {
-                    Fetch f;
-                    f.w = group_w(Gc, q);
-                    f.c = Gc.cid(q);
-                    f.sv = (Gc.s >> (8 * q)) & 0xFFu;
-                    f.sc = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
-                    f.xj = xj[q]; f.yj = yj[q]; f.zj = zj[q];
-                    f.g = ldg_dict(d.dict, f.c);
-                    const double3 r = entry_force<LAW, PREC>(d, e0 + q, f, safe, xi, yi, zi);
-                    if (f.w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
-                        tx = tx + ax; ty = ty + ay; tz = tz + az;
-                        ax = 0.0; ay = 0.0; az = 0.0;
-                    }
-                    ax = ax + r.x; ay = ay + r.y; az = az + r.z;
+                if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
+                    tx = tx + ax; ty = ty + ay; tz = tz + az;
+                    ax = 0.0; ay = 0.0; az = 0.0;
                 }
+                ax = ax + r.x; ay = ay + r.y; az = az + r.z;
             }
         }
         Gc = Gn;
@@ -1386,7 +1345,6 @@ batch_kernel_t pick_batch_law(int law)
 batch_kernel_t pick_batch_kernel(int law, int prec)
 {
     if (prec == kP32X) return pick_batch_law<kP32X>(law);
-    if (prec == kP32D) return pick_batch_law<kP32D>(law);
     return pick_batch_law<kP64>(law);
 }
 
@@ -1415,7 +1373,6 @@ template <int LAW, int SCHEME>
 kernel_t pick_prec(int prec, bool wide, bool sce)
 {
     if (prec == kP32X) return pick_cid<LAW, SCHEME, kP32X>(wide, sce);
-    if (prec == kP32D) return pick_cid<LAW, SCHEME, kP32D>(wide, sce);
     return pick_cid<LAW, SCHEME, kP64>(wide, sce);
 }
 
@@ -1613,7 +1570,7 @@ struct bbpd_solver {
     bbpd_params prm{};
     int64_t nN = 0, nB = 0, ns = 0, ne = 0, ndict = 0;
     bool wide = false;
-    int prec = kP64;                    // kernel variant (kP64, kP32D, kP32X)
+    int prec = kP64;                    // kernel variant (kP64 or kP32X)
     int64_t step = 1;
     double cn = 0;
     std::vector<int32_t> perm;          // device position -> input node
@@ -1773,7 +1730,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     std::vector<float4> dictx;
     S->prec = kP64;
     if (prm->precision == BBPD_PREC_FP32) {
-        S->prec = kP32D;
+        S->prec = kP64;   // unless the dictionary of bond vectors fits (below)
         const double *X = pb->undeformed_coordinates;
         auto keyx = [&](int64_t k, int side) {
             int64_t a = (int64_t)bl[k] - 1, b = (int64_t)bl[nB + k] - 1;
@@ -1978,7 +1935,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     std::vector<int64_t> hptr;
     std::vector<uint32_t> halo;
     int tile_cap = 0;
-    if (prm->node_order == BBPD_ORDER_TILED && !S->wide && S->prec != kP32D) {
+    if (prm->node_order == BBPD_ORDER_TILED && !S->wide) {
         const int64_t ntiles = (nN + kTile - 1) / kTile;
         std::vector<std::vector<uint32_t>> hl(ntiles);
         std::vector<int> over(HT, 0), capt(HT, 0);
@@ -2136,11 +2093,6 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         TRY(S->put(&d.urh1, uh));
         TRY(S->put(&d.url0, ul));
         TRY(S->put(&d.url1, ul));
-    }
-    {
-        std::vector<float> k32(dict.size());
-        for (size_t q = 0; q < dict.size(); q++) k32[q] = (float)(dict[q].bs * prm->cell_volume * dict[q].vcf);
-        TRY(S->put((float **)&d.dict32, k32));
     }
     d.s0e = d.s1e = d.sce = nullptr;
     if (pb->s0) TRY(S->put((double **)&d.s0e, s0e));
@@ -2623,8 +2575,8 @@ extern "C" int bbpd_batch_create(int device, int precision, bbpd_batch **out)
     // resident blocks per SM: the smallest over the kernels this batch may run
     int occ = 1 << 30;
     for (int law = 0; law < 4; law++)
-        for (int pv : {kP64, kP32X, kP32D}) {
-            if ((pv == kP64) != (B->prec == kP64)) continue;
+        for (int pv : {kP64, kP32X}) {
+            if (pv == kP32X && B->prec == kP64) continue;
             int o = 0;
             BBPD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void *)pick_batch_kernel(law, pv), kBlock, 0));
             occ = std::min(occ, o);
@@ -2648,7 +2600,7 @@ extern "C" int bbpd_batch_add(bbpd_batch *B, bbpd_solver *S)
     if (S->batch) return fail(BBPD_ERR_ARG, "solver already belongs to a batch");
     if (S->device != B->device) return fail(BBPD_ERR_ARG, "solver and batch live on different devices");
     if (S->prm.scheme != BBPD_SCHEME_ADR) return fail(BBPD_ERR_UNSUPPORTED, "batches run the ADR scheme");
-    if ((S->prec == kP64) != (B->prec == kP64))
+    if (S->prm.precision != (B->prec == kP64 ? BBPD_PREC_FP64 : BBPD_PREC_FP32))
         return fail(BBPD_ERR_UNSUPPORTED, "solver precision form differs from the batch's");
     if (S->wide || S->tiled)
         return fail(BBPD_ERR_UNSUPPORTED, "batch members need 16-bit dictionary ids and input or Morton node order");

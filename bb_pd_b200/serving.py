@@ -104,14 +104,15 @@ def _new_solver(req: Request, precision: str, device: int) -> Solver:
 
 
 def run_batched(requests: list[Request], *, hbm_budget: float = 150e9, precision: str = "fp64",
-                chunk: int = 100, device: int = 0, tune: bool = True) -> tuple[list[Result], dict]:
-    """Continuous batching. Solvers of arrived requests are built by a worker
-    thread (host layout and upload) while the GPU steps the batch; a request
+                chunk: int = 100, device: int = 0, tune: bool = True,
+                builders: int = 2) -> tuple[list[Result], dict]:
+    """Continuous batching. Solvers of arrived requests are built by worker
+    threads (host layout and upload) while the GPU steps the batch; a request
     is admitted when its estimated device memory fits the budget. Returns the
     results and run statistics."""
     pending = sorted(requests, key=lambda r: r.arrival)
     batch = Batch(precision, device)
-    pool = ThreadPoolExecutor(max_workers=1)
+    pool = ThreadPoolExecutor(max_workers=builders)
     creating: list = []                 # (request, future, estimate)
     active: list = []                   # (request, solver, track, admitted, bytes)
     results: list[Result] = []

@@ -47,7 +47,9 @@ enum { BBPD_LAW_LINEAR = 0,       /* brittle: calculatebondfailureMex.c:26-44 */
        BBPD_LAW_EXPONENTIAL = 3   /* calculatebsfexponentialMex.c:26-66 */ };
 enum { BBPD_SCHEME_EULERCROMER = 0, BBPD_SCHEME_ADR = 1 };
 enum { BBPD_PREC_FP64 = 0,        /* plain form: bit-identical to the reference chain */
-       BBPD_PREC_FP32 = 1         /* FP32 stretch/force, FP64 sums, FP64 guard band */ };
+       BBPD_PREC_FP32 = 1         /* FP32 stretch/force, FP64 sums, FP64 guard band; inputs
+                                     whose FP32 bond-vector dictionary exceeds 65 535
+                                     entries run the FP64 kernel */ };
 enum { BBPD_AMP_LINEAR = 0,       /* U(n) = rate * n */
        BBPD_AMP_SMOOTHSTEP = 1    /* smoothstepdata.m:40-42 from step 1 to nTimeSteps */ };
 enum { BBPD_ORDER_INPUT = 0,      /* input node order, neighbours gathered from HBM/L2
