@@ -254,6 +254,32 @@ __global__ void __launch_bounds__(1024) k_damping_final(const double *part, int6
     }
 }
 
+// calculatedamage.m:34-43: unbroken bonds per node, accumulated into
+// damage[] (fail is 0 or 1, so the sums are exact integers in any order).
+// Ids outside [1, nN] are skipped and reported through *bad.
+__global__ void k_damage_count(const double *__restrict__ bl, const double *__restrict__ fail_,
+                               int64_t nB, int64_t nN, double *damage, int *bad)
+{
+    GRID_STRIDE(k, nB)
+    {
+        const double di = bl[k], dj = bl[nB + k];
+        if (!(di >= 1 && dj >= 1 && di <= (double)nN && dj <= (double)nN)) {
+            *bad = 1;
+            continue;
+        }
+        const double f = fail_[k];
+        atomicAdd(&damage[(int64_t)di - 1], f);
+        atomicAdd(&damage[(int64_t)dj - 1], f);
+    }
+}
+
+// calculatedamage.m:45: damage = 1 - unbroken / nFAMILYMEMBERS.
+__global__ void k_damage_final(const double *__restrict__ nfam, int64_t nN, double *damage)
+{
+    GRID_STRIDE(i, nN)
+    damage[i] = 1 - (damage[i] / nfam[i]);
+}
+
 // ---- nodal force plan ----
 
 __global__ void k_plan_keys(const double *__restrict__ bl, int64_t nB, int64_t nN,
@@ -394,6 +420,35 @@ extern "C" int bbpd_dev_calculatebondfailure(double *fail_, double ff, const dou
     P.sc = csc; P.sc_steel = css; P.ff = ff;
     k_bondfailure<<<blocks_for(nB), kThreads, 0, as_stream(stream)>>>(fail_, P, BT, s, nB);
     return launch_check();
+}
+
+extern "C" int bbpd_dev_calculatedamage(const double *bl, const double *fail_, const double *nfam,
+        int64_t nB, int64_t nN, double *damage, void *stream)
+{
+    if (nB < 0 || nN < 0) return fail(BBPD_ERR_ARG, "negative size");
+    if (nN == 0) return BBPD_OK;
+    int rc = require_device();
+    if (rc) return rc;
+    cudaStream_t st = as_stream(stream);
+    int *bad = nullptr;
+    BBPD_CUDA_TRY(cudaMallocAsync(&bad, sizeof(int), st));
+    cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(damage, 0, sizeof(double) * (size_t)nN, st);
+    if (e == cudaSuccess && nB > 0) {
+        k_damage_count<<<blocks_for(nB), kThreads, 0, st>>>(bl, fail_, nB, nN, damage, bad);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        k_damage_final<<<blocks_for(nN), kThreads, 0, st>>>(nfam, nN, damage);
+        e = cudaGetLastError();
+    }
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFreeAsync(bad, st);
+    if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "damage: %s", cudaGetErrorString(e));
+    if (h) return fail(BBPD_ERR_ARG, "BONDLIST holds node ids outside [1, nNodes]");
+    return BBPD_OK;
 }
 
 extern "C" int bbpd_dev_calculatebondforces(double *fX, double *fY, double *fZ,
@@ -701,6 +756,20 @@ extern "C" int bbpd_calculatebondforces(double *fX, double *fY, double *fZ, cons
     TRY(bbpd_dev_calculatebondforces(dfX, dfY, dfZ, dfa, ddX, ddY, ddZ, dL, ds, dsp, dBS, V, dV, dB, nB, nullptr));
     TRY(finish());
     TRY(download(fX, dfX, b)); TRY(download(fY, dfY, b)); TRY(download(fZ, dfZ, b));
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_calculatedamage(const double *bl, const double *fail_, const double *nfam,
+        int64_t nB, int64_t nN, double *damage)
+{
+    TRY(require_device());
+    std::lock_guard<std::mutex> lk(g_mu);
+    const size_t b = sizeof(double) * (size_t)nB, n = sizeof(double) * (size_t)nN;
+    double *dbl, *dfa, *dnf, *ddm;
+    MIRROR_IN(bl, 2 * b, dbl); MIRROR_IN(fail_, b, dfa); MIRROR_IN(nfam, n, dnf); MIRROR_OUT(damage, n, ddm);
+    TRY(bbpd_dev_calculatedamage(dbl, dfa, dnf, nB, nN, ddm, nullptr));
+    TRY(finish());
+    TRY(download(damage, ddm, n));
     return BBPD_OK;
 }
 

@@ -46,6 +46,7 @@ def _sig():
     L.bbpd_timeintegrationeulercromer.argtypes = [p, p, d, p, p, p, d, p, p, p, i64, i]
     L.bbpd_calculatedampingcoefficient.argtypes = [p, p, p, d, p, p, i64, p]
     L.bbpd_timeintegrationADR.argtypes = [i64, d, p, p, p, d, p, p, p, i64]
+    L.bbpd_calculatedamage.argtypes = [p, p, p, i64, i64, p]
     return L
 
 
@@ -110,6 +111,16 @@ def calculatebondfailureMex(fail, failureFunctionality, BONDTYPE, stretch,
         _arr(stretch, "stretch"), float(criticalStretchConcrete), float(criticalStretchSteel),
         _rows(fail)))
     return fail
+
+
+def calculatedamage(bondlist, fail, nFAMILYMEMBERS) -> np.ndarray:
+    """calculatedamage.m:1 on the GPU: the fraction of broken bonds of every node."""
+    nN = _rows(nFAMILYMEMBERS)
+    damage = np.zeros(nN, dtype=np.float64)
+    N.check(_lib().bbpd_calculatedamage(_arr(bondlist, "bondlist"), _arr(fail, "fail"),
+                                        _arr(nFAMILYMEMBERS, "nFAMILYMEMBERS"), _rows(bondlist), nN,
+                                        _arr(damage, "damage", True)))
+    return damage
 
 
 def calculatebondforcesMex(bForceX, bForceY, bForceZ, fail, deformedX, deformedY, deformedZ,

@@ -198,6 +198,15 @@ int bbpd_dev_calculatedampingcoefficient_noalloc(const double *nodalForce,
         const double *nodalVelocityPreviousHalf, const double *nodalDisplacement,
         int64_t nNodes, double *cn, void *stream);
 
+/* replaces calculatedamage.m:1 (damage = fraction of broken bonds per node,
+ * :34-45): damage[i] = 1 - (sum of fail over node i's bonds) / nFAMILYMEMBERS[i].
+ * fail holds 0 or 1, so the sums are exact whatever their order. */
+int bbpd_dev_calculatedamage(const double *bondlist, const double *fail,
+        const double *nFAMILYMEMBERS, int64_t nBonds, int64_t nNodes,
+        double *damage, void *stream);
+int bbpd_calculatedamage(const double *bondlist, const double *fail,
+        const double *nFAMILYMEMBERS, int64_t nBonds, int64_t nNodes, double *damage);
+
 /* Free the device mirrors and cached plan of the host-pointer entry points
  * (the gateways register it with mexAtExit). */
 int bbpd_release_mirrors(void);

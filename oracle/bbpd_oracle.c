@@ -328,6 +328,55 @@ void orc_adr_integrate(int64_t iTimeStep, double dt, double *vh, const double *F
 }
 
 /* smoothstepdata.m:40-42 (xi^3 taken as (xi*xi)*xi, xi^2 as xi*xi) */
+/* calculatedamage.m:29-45: unbroken bonds counted per node in bond order,
+ * then damage = 1 - unbroken / nFAMILYMEMBERS. */
+void orc_damage(const double *bl, const double *fail, const double *nFamily,
+                int64_t nBonds, int64_t nNodes, double *damage)
+{
+    for (int64_t i = 0; i < nNodes; i++) damage[i] = 0.0;
+    for (int64_t k = 0; k < nBonds; k++) {
+        const int64_t i = (int64_t)bl[k] - 1, j = (int64_t)bl[nBonds + k] - 1;
+        damage[i] = damage[i] + fail[k];
+        damage[j] = damage[j] + fail[k];
+    }
+    for (int64_t i = 0; i < nNodes; i++) damage[i] = 1 - (damage[i] / nFamily[i]);
+}
+
+/* calculatecontactforce.m:29-80 (literal: distances from the positions at
+ * entry, then the nodes inside the radius in family order). */
+double orc_contact(const orc_penetrator *pen, double *cz, const double *X,
+                   double *x, double *u, double *v, double dt, double V,
+                   const double *rho, int64_t nNodes)
+{
+    const int64_t nN = nNodes;
+    *cz = *cz + pen->increment;                                  /* :41 */
+    double fz = 0.0;
+    for (int64_t f = 0; f < pen->nFamily; f++) {
+        const int64_t i = (int64_t)pen->family[f] - 1;
+        const double dX = x[i] - pen->cx, dZ = x[i + 2 * nN] - *cz;   /* :43-45 */
+        const double dist = sqrt((dX * dX) + (dZ * dZ));
+        if (dist < pen->radius) {                                /* :49 */
+            const double ux = dX / dist, uz = dZ / dist;         /* :58-61 */
+            const double uxs = ux * pen->radius, uzs = uz * pen->radius;
+            x[i] = pen->cx + uxs;                                /* :69-71 */
+            x[i + 2 * nN] = *cz + uzs;
+            double un[3], vn[3];
+            for (int c = 0; c < 3; c++) {
+                const int64_t e = i + c * nN;
+                un[c] = x[e] - X[e];                             /* :74 */
+                vn[c] = (un[c] - u[e]) / dt;                     /* :77 */
+            }
+            const double dpz = -1 * rho[i] * (vn[2] - v[i + 2 * nN]) / dt * V;   /* :80-82 */
+            fz = fz + dpz;                                       /* :88 sum in family order */
+            for (int c = 0; c < 3; c++) {
+                u[i + c * nN] = un[c];
+                v[i + c * nN] = vn[c];
+            }
+        }
+    }
+    return fz;
+}
+
 double orc_smoothstep(double t, double t0, double t1, double v0, double v1)
 {
     double xi = (t - t0) / (t1 - t0);
@@ -357,6 +406,8 @@ void orc_init_state(const orc_problem *p, orc_state *st)
         if (p->PF && p->PF[e] == 1) st->u[e] = U1;
         st->x[e] = p->X[e] + st->u[e];
     }
+    for (int q = 0; q < 4; q++) st->penCz[q] = q < p->nPen ? p->pen[q].cz : 0.0;
+    st->reaction = 0.0;
 }
 
 /* ---- kernel tables ---- */
@@ -542,6 +593,20 @@ void orc_run(const orc_problem *p, orc_state *st, const orc_kernels *k,
                 st->x[e] = p->X[e] + st->u[e];
             }
             memcpy(st->Fp, st->F, sizeof(double) * (size_t)(3 * nN));
+        }
+        /* contact bodies after the integration (dynamicsolverdisplacementcontrolled.m:107-115) */
+        if (p->nPen > 0) {
+            double r = 0.0;
+            int first = 1;
+            for (int q = 0; q < p->nPen; q++) {
+                const double fz = orc_contact(&p->pen[q], &st->penCz[q], p->X, st->x, st->u, st->v,
+                                              p->dt, p->V, p->rho, nN);
+                if (p->pen[q].reaction) {
+                    r = first ? fz : r + fz;
+                    first = 0;
+                }
+            }
+            st->reaction = r;
         }
         st->step = n + 1;
     }

@@ -117,6 +117,10 @@ void orc_adr_integrate(int64_t iTimeStep, double dt, double *vh, const double *F
                        const double *m, double cn, const double *vhp, double *u,
                        const double *CF, int64_t nNodes);
 
+/* calculatedamage.m:29-45 (damage per node, nNodes entries). */
+void orc_damage(const double *bl, const double *fail, const double *nFamily,
+                int64_t nBonds, int64_t nNodes, double *damage);
+
 /* smoothstepdata.m:40-42 */
 double orc_smoothstep(double t, double t0, double t1, double v0, double v1);
 
@@ -128,6 +132,25 @@ enum { ORC_LAW_LINEAR = 0, ORC_LAW_BILINEAR = 1, ORC_LAW_TRILINEAR = 2,
        ORC_LAW_EXPONENTIAL = 3 };
 enum { ORC_SCHEME_EULERCROMER = 0, ORC_SCHEME_ADR = 1 };
 enum { ORC_AMP_LINEAR = 0, ORC_AMP_SMOOTHSTEP = 1 };
+
+/* A rigid cylinder (axis along y) pushed into the body: the penetrator and
+ * supports of calculatecontactforce.m. */
+typedef struct orc_penetrator {
+    double cx, cz;          /* centre before step 1 */
+    double radius;
+    double increment;       /* centre z change per step (0 for a support) */
+    const double *family;   /* 1-based node ids checked for contact, in order */
+    int64_t nFamily;
+    int reaction;           /* its force counts toward the reaction */
+} orc_penetrator;
+
+/* calculatecontactforce.m:29-80: moves the centre by `increment` (*cz), pushes
+ * family nodes inside the radius back onto the surface, updates their
+ * displacement, velocity and deformed position, and returns the z force on
+ * the cylinder (sum over the family in order). */
+double orc_contact(const orc_penetrator *pen, double *cz, const double *X,
+                   double *x, double *u, double *v, double dt, double V,
+                   const double *rho, int64_t nNodes);
 
 typedef struct orc_problem {
     int64_t nNodes, nBonds;
@@ -147,6 +170,8 @@ typedef struct orc_problem {
     double appliedFinal;    /* smooth-step amplitude final value */
     int64_t nTimeSteps;     /* smooth-step final step */
     int cnOrder;            /* 0 = fixed tree (GPU order), 1 = literal sequential */
+    int nPen;               /* contact bodies applied after each integration, in order */
+    orc_penetrator pen[4];
 } orc_problem;
 
 typedef struct orc_state {
@@ -156,6 +181,8 @@ typedef struct orc_state {
     double *fail, *BSF, *flag;      /* nBonds */
     double *L, *dX, *dY, *dZ, *s, *fX, *fY, *fZ, *bsf; /* nBonds scratch */
     double *nfX, *nfY, *nfZ;        /* nNodes x nChunks scratch (nodal-force partials) */
+    double penCz[4];                /* current centre z of each contact body */
+    double reaction;                /* reactionForce of the last step (contact runs) */
 } orc_state;
 
 /* Prescribed displacement at step n for the chosen amplitude. */

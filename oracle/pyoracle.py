@@ -25,6 +25,11 @@ AMP = {"linear": 0, "smoothstep": 1}
 _P = C.POINTER(C.c_double)
 
 
+class OrcPenetrator(C.Structure):
+    _fields_ = [("cx", C.c_double), ("cz", C.c_double), ("radius", C.c_double), ("increment", C.c_double),
+                ("family", _P), ("nFamily", C.c_int64), ("reaction", C.c_int)]
+
+
 class OrcProblem(C.Structure):
     _fields_ = [
         ("nNodes", C.c_int64), ("nBonds", C.c_int64), ("X", _P), ("bl", _P), ("L0", _P),
@@ -35,14 +40,15 @@ class OrcProblem(C.Structure):
         ("damping", C.c_double), ("rho", _P), ("mass", _P), ("CF", _P), ("PF", _P),
         ("law", C.c_int), ("scheme", C.c_int), ("amplitude", C.c_int), ("nChunks", C.c_int),
         ("rate", C.c_double), ("appliedFinal", C.c_double), ("nTimeSteps", C.c_int64),
-        ("cnOrder", C.c_int),
+        ("cnOrder", C.c_int), ("nPen", C.c_int), ("pen", OrcPenetrator * 4),
     ]
 
 
 class OrcState(C.Structure):
     _fields_ = [("step", C.c_int64), ("cn", C.c_double)] + [
         (n, _P) for n in ("x", "u", "v", "a", "F", "Fp", "fail", "BSF", "flag", "L", "dX", "dY",
-                          "dZ", "s", "fX", "fY", "fZ", "bsf", "nfX", "nfY", "nfZ")]
+                          "dZ", "s", "fX", "fY", "fZ", "bsf", "nfX", "nfY", "nfZ")] + [
+        ("penCz", C.c_double * 4), ("reaction", C.c_double)]
 
 
 def build(ref_dir: str | None = None) -> None:
@@ -85,6 +91,7 @@ def lib() -> C.CDLL:
         L.orc_bsf_trilinear.argtypes = [_P, _P, C.c_int, _P, C.c_int, _P, C.c_int, C.c_double, _P, _P, _P, C.c_int64]
         L.orc_bsf_bilinear.argtypes = [_P, _P, C.c_int, _P, C.c_int, _P, _P, _P, C.c_int64]
         L.orc_bondfailure.argtypes = [_P, C.c_double, _P, _P, _P, C.c_int, C.c_double, C.c_int64]
+        L.orc_damage.argtypes = [_P, _P, _P, C.c_int64, C.c_int64, _P]
         L.orc_bondforces.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_double, _P, _P, C.c_int64]
         L.orc_nodalforces_chunked.argtypes = [C.c_int64, C.c_int64, _P, _P, _P, _P, _P, C.c_int]
         L.orc_eulercromer.argtypes = [_P, _P, C.c_double, _P, _P, _P, C.c_double, _P, _P, _P, C.c_int64, C.c_int]
@@ -136,7 +143,8 @@ class Run:
                  amplitude="linear", rate=0.0, applied_final=0.0, n_time_steps=0,
                  s0=1e-4, s1=3e-4, sc=2e-3, sc_steel=1.0, k_exp=25.0, alpha_exp=0.25,
                  beta_tri=0.25, failure_functionality=0.0, damping=0.0, dt=None,
-                 cell_volume=None, per_bond_sc=None, cn_order="tree", kernels="restated"):
+                 cell_volume=None, per_bond_sc=None, cn_order="tree", kernels="restated",
+                 penetrators=()):
         L = lib()
         nN, nB = int(inp["nNodes"]), int(inp["nBonds"])
         self.nN, self.nB = nN, nB
@@ -166,6 +174,13 @@ class Run:
         p.law, p.scheme, p.amplitude, p.nChunks = LAW[law], SCHEME[scheme], AMP[amplitude], n_chunks
         p.rate, p.appliedFinal, p.nTimeSteps = rate, applied_final, n_time_steps
         p.cnOrder = 0 if cn_order == "tree" else 1
+        # contact bodies: dicts with centre_x, centre_z, radius, increment, family (1-based ids), reaction
+        self.fam = [f64(np.asarray(q["family"], dtype=np.float64)) for q in penetrators]
+        p.nPen = len(penetrators)
+        for j, q in enumerate(penetrators):
+            pp = p.pen[j]
+            pp.cx, pp.cz, pp.radius, pp.increment = q["centre_x"], q["centre_z"], q["radius"], q["increment"]
+            pp.family, pp.nFamily, pp.reaction = P(self.fam[j]), len(self.fam[j]), int(q.get("reaction", 0))
         self.p = p
         z3 = lambda: np.zeros((nN, 3), order="F")
         zb = lambda: np.zeros(nB)
@@ -197,6 +212,11 @@ class Run:
     @property
     def cn(self) -> float:
         return float(self.st.cn)
+
+    @property
+    def reaction(self) -> float:
+        """reactionForce of the last step (contact runs)."""
+        return float(self.st.reaction)
 
     def get(self, field: str) -> np.ndarray:
         m = {"displacement": "u", "velocity": "v", "force": "F", "deformed": "x",

@@ -201,3 +201,20 @@ def test_division_selftest():
     print(f"samples {n.value}, rcp.approx max rel err {err.value:.3e}")
     assert n.value > 150_000_000
     assert rb.value == 0 and qb.value == 0, (rb.value, qb.value)
+
+
+def test_damage_vs_oracle():
+    inp = bb.beam.build(bb.beam.small(nx=20, ny=4, nz=6))
+    bl, nfam = inp["BONDLIST"], inp["nFAMILYMEMBERS"]
+    rng = np.random.default_rng(5)
+    fail = (rng.random(inp["nBonds"]) > 0.3).astype(np.float64)
+    d = R.calculatedamage(bl, fail, nfam)
+    do = np.zeros(inp["nNodes"])
+    po.lib().orc_damage(P(bl), P(fail), P(nfam), inp["nBonds"], inp["nNodes"], P(do))
+    assert same(d, do)
+    assert same(R.calculatedamage(bl, np.ones(inp["nBonds"]), nfam), np.zeros(inp["nNodes"]))
+    bad = np.asfortranarray(bl.copy())
+    bad[0, 0] = inp["nNodes"] + 1
+    with pytest.raises(bb.BBPDError) as e:
+        R.calculatedamage(bad, fail, nfam)
+    assert e.value.status == bb._native.ERR_ARG

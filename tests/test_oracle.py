@@ -310,3 +310,15 @@ int main(int c, char **v) { int n = atoi(v[1]); int lo[8], hi[8];
                 assert got[c] == (-1, -1)
             else:
                 assert got[c] == (lo, hi)
+
+
+def test_damage_known_answers():
+    """calculatedamage.m:29-45: 1 - (intact bonds) / family size; a family
+    counted before bonds were removed (a notch) leaves damage where no bond
+    ever broke."""
+    bl = np.asfortranarray(np.array([[1, 2], [1, 3], [2, 3], [3, 4]], dtype=np.float64))
+    fail = np.array([1.0, 0.0, 1.0, 1.0])
+    nfam = np.array([2.0, 2.0, 3.0, 2.0])          # node 4 lost one bond to a notch
+    dmg = np.zeros(4)
+    po.lib().orc_damage(po.P(bl), po.P(fail), po.P(nfam), 4, 4, po.P(dmg))
+    assert list(dmg) == [0.5, 0.0, 1 - 2 / 3, 0.5]
