@@ -71,6 +71,12 @@ class Info(C.Structure):
     ]
 
 
+class Penetrator(C.Structure):
+    _fields_ = [("centre_x", C.c_double), ("centre_z", C.c_double), ("radius", C.c_double),
+                ("increment", C.c_double), ("family", _P), ("n_family", C.c_int64),
+                ("reaction", C.c_int32), ("reserved", C.c_int32)]
+
+
 class BatchInfo(C.Structure):
     _fields_ = [
         ("n_members", C.c_int32), ("blocks_per_sm", C.c_int32), ("grab", C.c_int32),
@@ -126,6 +132,7 @@ def lib() -> C.CDLL:
         L.bbpd_selftest_wait_timeout.argtypes = [C.c_double]
         L.bbpd_selftest_division.argtypes = [C.c_int64, C.c_uint64] + [C.POINTER(C.c_int64)] * 3 + [_P]
         L.bbpd_get_reaction.argtypes = [C.c_void_p, C.c_int64, _P]
+        L.bbpd_set_contact.argtypes = [C.c_void_p, C.c_int, C.POINTER(Penetrator)]
         L.bbpd_batch_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
         for name in ("bbpd_batch_destroy",):
             getattr(L, name).argtypes = [C.c_void_p]

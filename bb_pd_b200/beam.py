@@ -137,3 +137,20 @@ def serving_stream(n: int = 200, seed: int = 20261203, nodes_range=(1e4, 1e6), r
         s = geometric_beam(depth, dx, width=0.5 * depth)
         out.append(dict(arrival=float(t[k]), spec=s, law=str(laws[k]), nodes=int(s.nx) * int(s.ny) * int(s.nz)))
     return out
+
+
+def penetrator(inp: dict, centre_x: float, radius: float, search_radius: float, increment: float,
+               *, top: bool = True, reaction: bool = True) -> dict:
+    """A rigid cylinder (axis along y) resting on the top (or, for a support,
+    under the bottom) surface at x = centre_x, as the reference's
+    buildpenetrator.m and its centre correction build it: the family is every
+    node within search_radius (x-z distance) of the centre, and the centre is
+    moved until the nearest family node touches the cylinder."""
+    X = np.asarray(inp["undeformedCoordinates"])
+    z = X[:, 2].max() + radius if top else X[:, 2].min() - radius
+    d = np.sqrt((X[:, 0] - centre_x) ** 2 + (X[:, 2] - z) ** 2)
+    fam = np.nonzero(d < search_radius)[0]
+    gap = d[fam].min() - radius
+    z = z - gap if top else z + gap
+    return dict(centre_x=float(centre_x), centre_z=float(z), radius=float(radius), increment=float(increment),
+                family=(fam + 1).astype(np.float64), reaction=bool(reaction))

@@ -139,6 +139,14 @@ struct Dev {
     double *tree3;                   // partial sums of the reaction, same tree
     double *react;                   // reaction of step `it` of the last launch at [it]
     int64_t react_cap;               // entries of react[]
+    int n_pen;                       // contact cylinders (0: none)
+    double pen_cx[4], pen_r[4], pen_inc[4];
+    int pen_react[4];                // 1: force counts toward the reaction
+    int64_t pen_off[5];              // family of cylinder p: contact entries [pen_off[p], pen_off[p+1])
+    const int32_t *cidx;             // per node: its contact entry, or -1
+    double *cforce;                  // per contact entry: z force of the step, two buffers by step parity
+    double *pen_cz;                  // centre z of every cylinder, two buffers by step parity ([2][4])
+    int64_t n_contact;
     int law;                         // BBPD_LAW_* (read by the batch kernel)
     int prec;                        // kernel precision variant (read by the batch kernel)
     unsigned *tcnt;                  // arrival counters of the groups of levels >= 2
@@ -791,6 +799,71 @@ __device__ __forceinline__ StepBufs step_bufs(const Dev &d, int64_t n)
     return b;
 }
 
+// calculatecontactforce.m:43-82 for node i right after its integration (u,
+// v, x: its displacement, velocity and position). Families are disjoint, so
+// every node meets at most one cylinder and the per-node work is independent;
+// the cylinder's centre for step n is the stored one of step n - 1 plus the
+// increment, the same accumulation as the reference. The node's z force on
+// the cylinder goes to cforce for the step's reaction sum.
+__device__ __forceinline__ void apply_contact(const Dev &d, int64_t n, int64_t i, double u[3], double v[3],
+                                              double x[3])
+{
+    const int k = d.cidx[i];
+    if (k < 0) return;
+    int p = 0;
+    while (p + 1 < d.n_pen && k >= d.pen_off[p + 1]) p++;
+    const double cz = d.pen_cz[((n - 1) & 1) * 4 + p] + d.pen_inc[p];
+    const double cx = d.pen_cx[p], R = d.pen_r[p];
+    const double dX = x[0] - cx, dZ = x[2] - cz;
+    const double dist = sqrt((dX * dX) + (dZ * dZ));
+    double fz = 0.0;
+    if (dist < R) {
+        const double ux = dX / dist, uz = dZ / dist;
+        x[0] = cx + (ux * R);
+        x[2] = cz + (uz * R);
+        const int64_t nN = d.n_nodes;
+        double un[3], vn[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            un[c] = x[c] - d.X[i + c * nN];
+            vn[c] = (un[c] - u[c]) / d.dt;
+        }
+        fz = -1 * d.rho[i] * (vn[2] - v[2]) / d.dt * d.V;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            u[c] = un[c];
+            v[c] = vn[c];
+        }
+    }
+    d.cforce[(n & 1) * d.n_contact + k] = fz;
+}
+
+// Once during step n (one thread): store the centres of step n, which nodes
+// of step n + 1 read (nodes of step n read those of step n - 1).
+__device__ __forceinline__ void contact_advance(const Dev &d, int64_t n)
+{
+    for (int p = 0; p < d.n_pen; p++)
+        d.pen_cz[(n & 1) * 4 + p] = d.pen_cz[((n - 1) & 1) * 4 + p] + d.pen_inc[p];
+}
+
+// After step n (every node done; one thread): the reaction of the step, the
+// forces of the flagged cylinders summed in family order
+// (dynamicsolverdisplacementcontrolled.m:115 with calculatecontactforce.m:88).
+__device__ __forceinline__ void contact_reaction(const Dev &d, int64_t n, int64_t it)
+{
+    double r = 0.0;
+    bool first = true;
+    const double *f = d.cforce + (n & 1) * d.n_contact;
+    for (int p = 0; p < d.n_pen; p++) {
+        if (!d.pen_react[p]) continue;
+        double fz = 0.0;
+        for (int64_t k = d.pen_off[p]; k < d.pen_off[p + 1]; k++) fz = fz + f[k];
+        r = first ? fz : r + fz;
+        first = false;
+    }
+    if (it < d.react_cap) d.react[it] = r;
+}
+
 // Work on one slice after its nodal forces (tx, ty, tz of lane's node) are
 // summed: Euler-Cromer integrates the node; ADR stores F, forms the node's
 // Rayleigh-quotient terms, folds them over the slice and enters the tree.
@@ -806,8 +879,7 @@ __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, in
             // timeintegrationeulercromerMex.c:33-50 on the node just summed
             const uint8_t fl = d.nflag[i];
             const double Fv[3] = {tx, ty, tz};
-            float uh[3], ul[3];
-            bool bad = false, far = false;
+            double un[3], vn[3], xn3[3];
 #pragma unroll
             for (int dof = 0; dof < 3; dof++) {
                 const int64_t e = i + nN * dof;
@@ -819,10 +891,18 @@ __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, in
                 double xe = d.X[e] + ue;
                 if (fl & (8 << dof)) { ue = b.Un1; xe = d.X[e] + ue; }
                 if (d.a) d.a[e] = ae;
-                d.v[e] = ve; d.u[e] = ue; b.xn[e] = xe;
-                uh[dof] = (float)ue; ul[dof] = (float)(ue - (double)uh[dof]);
-                bad |= !isfinite(ue) || !isfinite(ve);
-                far |= coord_out_of_range(xe);
+                un[dof] = ue; vn[dof] = ve; xn3[dof] = xe;
+            }
+            if (d.n_pen) apply_contact(d, b.n, i, un, vn, xn3);
+            float uh[3], ul[3];
+            bool bad = false, far = false;
+#pragma unroll
+            for (int dof = 0; dof < 3; dof++) {
+                const int64_t e = i + nN * dof;
+                d.v[e] = vn[dof]; d.u[e] = un[dof]; b.xn[e] = xn3[dof];
+                uh[dof] = (float)un[dof]; ul[dof] = (float)(un[dof] - (double)uh[dof]);
+                bad |= !isfinite(un[dof]) || !isfinite(vn[dof]);
+                far |= coord_out_of_range(xn3[dof]);
             }
             if (PREC == kP32X) {
                 b.urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
@@ -877,8 +957,7 @@ __device__ __forceinline__ void adr_update_slice(const Dev &d, const StepBufs &b
         if (i >= nN) return;
         const uint8_t fl = d.nflag[i];
         const double minv = 1.0 / d.mass[i];
-        float uh[3], ul[3];
-        bool bad = false, far = false;
+        double un[3], vn[3], xn3[3];
 #pragma unroll
         for (int dof = 0; dof < 3; dof++) {
             const int64_t e = i + nN * dof;
@@ -889,11 +968,18 @@ __device__ __forceinline__ void adr_update_slice(const Dev &d, const StepBufs &b
             double ue = d.u[e] + (d.dt * vh);
             if (fl & (1 << dof)) { ue = 0; vh = 0; }
             if (fl & (8 << dof)) { ue = b.Un1; vh = 0; }
-            const double xe = d.X[e] + ue;
-            d.v[e] = vh; d.u[e] = ue; b.xn[e] = xe;
-            uh[dof] = (float)ue; ul[dof] = (float)(ue - (double)uh[dof]);
-            bad |= !isfinite(ue) || !isfinite(vh);
-            far |= coord_out_of_range(xe);
+            un[dof] = ue; vn[dof] = vh; xn3[dof] = d.X[e] + ue;
+        }
+        if (d.n_pen) apply_contact(d, b.n, i, un, vn, xn3);
+        float uh[3], ul[3];
+        bool bad = false, far = false;
+#pragma unroll
+        for (int dof = 0; dof < 3; dof++) {
+            const int64_t e = i + nN * dof;
+            d.v[e] = vn[dof]; d.u[e] = un[dof]; b.xn[e] = xn3[dof];
+            uh[dof] = (float)un[dof]; ul[dof] = (float)(un[dof] - (double)uh[dof]);
+            bad |= !isfinite(un[dof]) || !isfinite(vn[dof]);
+            far |= coord_out_of_range(xn3[dof]);
         }
         if (PREC == kP32X) {
             b.urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
@@ -926,6 +1012,7 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
     for (int64_t it = 0; it < nsteps; it++) {
         const StepBufs b = step_bufs(d, step0 + it);
         const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
+        if (d.n_pen && blockIdx.x == 0 && threadIdx.x == 0) contact_advance(d, b.n);
 
         // ---- phase A: bond forces (+ Euler-Cromer / ADR terms) ----
         // Warps take slices from a shared counter, so warps that finish early
@@ -950,6 +1037,7 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
             adr_update<PREC>(d, b, lane, gwarp, nwarps);
         }
         if (!grid_barrier(d)) return;
+        if (d.n_pen && blockIdx.x == 0 && threadIdx.x == 0) contact_reaction(d, b.n, it);
     }
 }
 
@@ -1168,6 +1256,7 @@ __global__ void __launch_bounds__(kBlock, 2) tstep_kernel(Dev d, int64_t step0, 
     for (int64_t it = 0; it < nsteps; it++) {
         const StepBufs b = step_bufs(d, step0 + it);
         const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
+        if (d.n_pen && blockIdx.x == 0 && threadIdx.x == 0) contact_advance(d, b.n);
         // Blocks take tiles from a shared counter; each block stops at its
         // first grab past the last tile, so a step uses exactly
         // ntiles + gridDim.x counter values.
@@ -1225,6 +1314,7 @@ __global__ void __launch_bounds__(kBlock, 2) tstep_kernel(Dev d, int64_t step0, 
             adr_update<PREC>(d, b, lane, gwarp, nwarps);
         }
         if (!grid_barrier(d)) return;
+        if (d.n_pen && blockIdx.x == 0 && threadIdx.x == 0) contact_reaction(d, b.n, it);
     }
 }
 
@@ -1296,6 +1386,9 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
     __syncwarp();
 
     for (int64_t it = 0; it < nsteps; it++) {
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            for (int m = 0; m < B.S; m++)
+                if (B.members[m].n_pen) contact_advance(B.members[m], __ldg(&B.mstep[m]) + it);
         // one failing grab per warp and step: ngrabs + nwarps values per step
         const int64_t base = it * (ngrabs + nwarps);
         int64_t gi = grab_counter(B.work, lane) - base;
@@ -1323,6 +1416,9 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
             adr_update_slice<PREC>(d, b, w - __ldg(&B.prefix[m]), lane);
         }
         if (!grid_barrier_raw(B.bar, B.err, B.timeout_ns)) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            for (int m = 0; m < B.S; m++)
+                if (B.members[m].n_pen) contact_reaction(B.members[m], __ldg(&B.mstep[m]) + it, it);
     }
     // every block has read the step numbers of the last step (barrier above)
     if (blockIdx.x == 0)
@@ -1585,6 +1681,7 @@ struct bbpd_solver {
     bool tiled = false;                 // tiled kernel with shared-memory staging
     size_t smem = 0;                    // its dynamic shared memory per block
     bbpd_batch *batch = nullptr;        // batch this solver is a member of
+    bool has_density = false;          // DENSITY given (contact needs it)
     bool cn_stale = false;              // cn on the device is newer than S->cn
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1684,6 +1781,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     S->prm = *prm;
     S->nN = nN;
     S->nB = nB;
+    S->has_density = pb->density != nullptr;
     const int T = prm->n_chunks;
 
     // node order
@@ -2864,10 +2962,67 @@ extern "C" int bbpd_batch_last_kernel_ms(bbpd_batch *B, float *ms)
     return BBPD_OK;
 }
 
+extern "C" int bbpd_set_contact(bbpd_solver *S, int n, const bbpd_penetrator *pen)
+{
+    if (!S || n < 0 || n > 4 || (n > 0 && !pen)) return fail(BBPD_ERR_ARG, "bad argument (at most 4 cylinders)");
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    if (S->batch) TRY(batch_member_changed(S->batch));
+    Dev &d = S->d;
+    if (n == 0) {
+        d.n_pen = 0;
+        return BBPD_OK;
+    }
+    if (!S->has_density) return fail(BBPD_ERR_UNSUPPORTED, "contact needs DENSITY (calculatecontactforce.m:80)");
+    const int64_t nN = S->nN;
+    std::vector<int32_t> cidx(nN, -1);
+    int64_t off[5] = {0, 0, 0, 0, 0};
+    for (int p = 0; p < n; p++) {
+        const bbpd_penetrator &q = pen[p];
+        if (!(q.radius > 0) || !std::isfinite(q.radius) || !std::isfinite(q.centre_x) ||
+            !std::isfinite(q.centre_z) || !std::isfinite(q.increment) || q.n_family < 0 ||
+            (q.n_family > 0 && !q.family))
+            return fail(BBPD_ERR_ARG, "cylinder %d: bad centre, radius, increment or family", p);
+        off[p + 1] = off[p] + q.n_family;
+        for (int64_t f = 0; f < q.n_family; f++) {
+            const double id = q.family[f];
+            if (!(id >= 1 && id <= (double)nN && id == std::floor(id)))
+                return fail(BBPD_ERR_ARG, "cylinder %d: family[%lld] = %g is not a node id", p, (long long)f, id);
+            const int32_t dev = S->inv[(int64_t)id - 1];
+            if (cidx[dev] >= 0)
+                return fail(BBPD_ERR_UNSUPPORTED, "node %g is in two cylinder families (families must be disjoint)", id);
+            cidx[dev] = (int32_t)(off[p] + f);
+        }
+    }
+    const int64_t ntot = off[n];
+    std::vector<double> cz(8, 0.0), zero(2 * std::max<int64_t>(ntot, 1), 0.0);
+    for (int p = 0; p < n; p++) cz[p] = cz[4 + p] = pen[p].centre_z;
+    int32_t *dcidx = nullptr;
+    double *dcf = nullptr, *dcz = nullptr;
+    TRY(S->put(&dcidx, cidx));
+    TRY(S->put(&dcf, zero));
+    TRY(S->put(&dcz, cz));
+    d.cidx = dcidx;
+    d.cforce = dcf;
+    d.pen_cz = dcz;
+    d.n_contact = ntot;
+    for (int p = 0; p < 4; p++) {
+        const bool on = p < n;
+        d.pen_cx[p] = on ? pen[p].centre_x : 0.0;
+        d.pen_r[p] = on ? pen[p].radius : 0.0;
+        d.pen_inc[p] = on ? pen[p].increment : 0.0;
+        d.pen_react[p] = on ? (pen[p].reaction != 0) : 0;
+    }
+    for (int p = 0; p <= 4; p++) d.pen_off[p] = off[std::min(p, n)];
+    d.n_pen = n;
+    return BBPD_OK;
+}
+
 extern "C" int bbpd_get_reaction(bbpd_solver *S, int64_t n, double *out)
 {
     if (!S || !out || n < 0) return fail(BBPD_ERR_ARG, "bad argument");
-    if (S->prm.scheme != BBPD_SCHEME_ADR) return fail(BBPD_ERR_UNSUPPORTED, "the reaction is summed by the ADR scheme");
+    if (S->prm.scheme != BBPD_SCHEME_ADR && S->d.n_pen == 0)
+        return fail(BBPD_ERR_UNSUPPORTED, "without contact the reaction is summed by the ADR scheme");
     if (n > kReactCap) return fail(BBPD_ERR_ARG, "at most %lld per-step reactions are kept", (long long)kReactCap);
     BBPD_CUDA_TRY(cudaSetDevice(S->device));
     BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));

@@ -134,6 +134,18 @@ class Solver:
     def set_step(self, step: int, cn: float = 0.0) -> None:
         N.check(N.lib().bbpd_set_step(self._h, step, cn))
 
+    def set_contact(self, penetrators: list[dict]) -> None:
+        """Rigid cylinders applied after every integration (calculatecontactforce.m):
+        dicts with centre_x, centre_z, radius, increment (per step), family
+        (1-based node ids) and reaction (bool)."""
+        self._fam = [np.ascontiguousarray(np.asarray(q["family"], dtype=np.float64)) for q in penetrators]
+        arr = (N.Penetrator * max(1, len(penetrators)))()
+        for j, q in enumerate(penetrators):
+            a = arr[j]
+            a.centre_x, a.centre_z, a.radius, a.increment = q["centre_x"], q["centre_z"], q["radius"], q["increment"]
+            a.family, a.n_family, a.reaction = N.ptr(self._fam[j]), len(self._fam[j]), int(bool(q.get("reaction", 0)))
+        N.check(N.lib().bbpd_set_contact(self._h, len(penetrators), arr))
+
     def reaction(self, n: int) -> np.ndarray:
         """Reaction of the first n steps of the last launch (ADR): the internal
         force summed over the prescribed DOFs; the applied load is its negative."""

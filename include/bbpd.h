@@ -320,12 +320,33 @@ typedef struct bbpd_info {
 } bbpd_info;
 int bbpd_get_info(bbpd_solver *s, bbpd_info *info);
 
-/* Reaction of each step of the last launch (ADR only): the internal nodal
- * force summed over the prescribed DOFs, in the fixed tree order of the damping
- * sums; out[k] belongs to the k-th step of that launch (at most 4096 kept).
- * The applied load is its negative. The reference reads its load from the
- * platen contact (dynamicsolverdisplacementcontrolled.m:115); with prescribed
- * displacements this is the equivalent quantity. */
+/* replaces calculatecontactforce.m:1 (dynamicsolverdisplacementcontrolled.m:107-112,
+ * dynamicsolverdisplacementcontrolledADR.m:147-150): rigid cylinders (axis
+ * along y) applied after every integration, in the given order. Each step a
+ * cylinder's centre moves by `increment` in z; family nodes closer than the
+ * radius in the x-z plane are put back on its surface, and their displacement
+ * and velocity follow; the cylinder's z force is the momentum change of those
+ * nodes (DENSITY x cellVolume), summed in family order. Families must be
+ * disjoint; the solver needs DENSITY. With contact, bbpd_get_reaction returns
+ * the sum of the forces of the cylinders flagged `reaction` (the reference's
+ * reactionForce). n = 0 removes contact. At most 4 cylinders. */
+typedef struct bbpd_penetrator {
+    double centre_x, centre_z;   /* centre before step 1 */
+    double radius;
+    double increment;            /* centre z change per step (0 for a support) */
+    const double *family;        /* 1-based node ids checked for contact, in order */
+    int64_t n_family;
+    int32_t reaction;            /* 1: its force is part of the reaction */
+    int32_t reserved;
+} bbpd_penetrator;
+int bbpd_set_contact(bbpd_solver *s, int n, const bbpd_penetrator *penetrators);
+
+/* Reaction of each step of the last launch: with contact (bbpd_set_contact),
+ * the reference's reactionForce (dynamicsolverdisplacementcontrolled.m:115),
+ * either scheme; without contact (ADR only), the internal nodal force summed
+ * over the prescribed DOFs in the fixed tree order of the damping sums, the
+ * equivalent quantity under prescribed displacements (the applied load is its
+ * negative). out[k] belongs to the k-th step of that launch (4096 kept). */
 int bbpd_get_reaction(bbpd_solver *s, int64_t n, double *host_out);
 
 /* ---- batches: many solver states stepped by one persistent launch ----

@@ -263,3 +263,65 @@ def test_info(small):
     assert i["n_nodes"] == small["nNodes"] and i["n_bonds"] == small["nBonds"]
     assert i["n_entries"] >= 2 * small["nBonds"] and i["n_entries"] % 32 == 0
     assert i["grid_blocks"] >= 1 and i["device_bytes"] > 0
+
+
+def _contact_setup(small, inc):
+    """Midspan loading cylinder and two support cylinders, no prescribed DOFs
+    (the cylinder loads the beam, as in the reference's drivers)."""
+    inp = dict(small)
+    inp["BODYFORCEFLAG"] = np.zeros_like(small["BODYFORCEFLAG"], order="F")
+    X = small["undeformedCoordinates"]
+    x0, x1 = X[:, 0].min(), X[:, 0].max()
+    pens = [bb.beam.penetrator(inp, 0.5 * (x0 + x1), 0.01, 0.03, inc),
+            bb.beam.penetrator(inp, x0 + 0.015, 0.005, 0.015, 0.0, top=False, reaction=False),
+            bb.beam.penetrator(inp, x1 - 0.015, 0.005, 0.015, 0.0, top=False, reaction=False)]
+    return inp, pens
+
+
+@pytest.mark.parametrize("scheme", ["eulercromer", "adr"])
+def test_contact_vs_oracle(small, scheme):
+    """calculatecontactforce.m fused into the integration: state bit-identical
+    to the oracle's literal restatement, reaction equal."""
+    inp, pens = _contact_setup(small, -2e-6 if scheme == "adr" else -4e-6)
+    kw = dict(LAWKW["trilinear"], scheme=scheme)
+    s = bb.Solver(inp, **kw)
+    s.set_contact(pens)
+    r = po.Run(inp, penetrators=pens, **kw)
+    for n in (1, 60, 79):
+        s.step(n)
+        r.step(n)
+        compare(s, r, "trilinear")
+        assert s.reaction(n)[-1] == r.reaction
+    assert r.reaction != 0.0 and (np.abs(s.get("displacement")[:, 2]) > 0).any()
+
+
+def test_contact_in_batch_identical(small):
+    inp, pens = _contact_setup(small, -2e-6)
+    kw = dict(LAWKW["trilinear"], scheme="adr", rate=0.0)
+    a = bb.Solver(inp, **kw)
+    a.set_contact(pens)
+    a.step(70)
+    b = bb.Solver(inp, **kw)
+    b.set_contact(pens)
+    other = bb.Solver(small, **kw, )
+    batch = bb.Batch("fp64")
+    batch.add(b)
+    batch.add(other)
+    batch.step(70)
+    for f in NODAL + BOND:
+        assert same(a.get(f), b.get(f)), f
+    assert same(a.reaction(70), b.reaction(70))
+    batch.close()
+
+
+def test_contact_rejects_overlap_and_missing_density(small):
+    inp, pens = _contact_setup(small, -2e-6)
+    s = bb.Solver(inp, **LAWKW["linear"], scheme="adr")
+    with pytest.raises(bb.BBPDError) as e:
+        s.set_contact([pens[0], dict(pens[0], increment=0.0)])
+    assert e.value.status == bb._native.ERR_UNSUPPORTED
+    nod = dict(inp)
+    del nod["DENSITY"]
+    t = bb.Solver(nod, **LAWKW["linear"], scheme="adr")
+    with pytest.raises(bb.BBPDError):
+        t.set_contact(pens[:1])
