@@ -133,6 +133,8 @@ def lib() -> C.CDLL:
         L.bbpd_selftest_division.argtypes = [C.c_int64, C.c_uint64] + [C.POINTER(C.c_int64)] * 3 + [_P]
         L.bbpd_get_reaction.argtypes = [C.c_void_p, C.c_int64, _P]
         L.bbpd_set_contact.argtypes = [C.c_void_p, C.c_int, C.POINTER(Penetrator)]
+        L.bbpd_set_probes.argtypes = [C.c_void_p, C.c_int, _P, C.POINTER(C.c_int32)]
+        L.bbpd_get_probes.argtypes = [C.c_void_p, C.c_int64, _P]
         L.bbpd_batch_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
         for name in ("bbpd_batch_destroy",):
             getattr(L, name).argtypes = [C.c_void_p]

@@ -139,6 +139,10 @@ struct Dev {
     double *tree3;                   // partial sums of the reaction, same tree
     double *react;                   // reaction of step `it` of the last launch at [it]
     int64_t react_cap;               // entries of react[]
+    int n_probe;                     // DOFs recorded every step (0: none)
+    int64_t probe_node[8];           // device node of probe k
+    int probe_dof[8];                // 0 x, 1 y, 2 z
+    double *probe_hist;              // displacement of probe k at step it of the launch: [it * n_probe + k]
     int n_pen;                       // contact cylinders (0: none)
     double pen_cx[4], pen_r[4], pen_inc[4];
     int pen_react[4];                // 1: force counts toward the reaction
@@ -838,6 +842,15 @@ __device__ __forceinline__ void apply_contact(const Dev &d, int64_t n, int64_t i
     d.cforce[(n & 1) * d.n_contact + k] = fz;
 }
 
+// Record the final displacement of node i for the probes on it (CMOD and
+// similar per-step outputs, dynamicsolverdisplacementcontrolled.m:118).
+__device__ __forceinline__ void record_probes(const Dev &d, int64_t it, int64_t i, const double u[3])
+{
+    if (it >= d.react_cap) return;
+    for (int k = 0; k < d.n_probe; k++)
+        if (d.probe_node[k] == i) d.probe_hist[it * d.n_probe + k] = u[d.probe_dof[k]];
+}
+
 // Once during step n (one thread): store the centres of step n, which nodes
 // of step n + 1 read (nodes of step n read those of step n - 1).
 __device__ __forceinline__ void contact_advance(const Dev &d, int64_t n)
@@ -894,6 +907,7 @@ __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, in
                 un[dof] = ue; vn[dof] = ve; xn3[dof] = xe;
             }
             if (d.n_pen) apply_contact(d, b.n, i, un, vn, xn3);
+            if (d.n_probe) record_probes(d, it, i, un);
             float uh[3], ul[3];
             bool bad = false, far = false;
 #pragma unroll
@@ -948,7 +962,8 @@ __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, in
 
 // ADR phase B (timeintegrationADR.m:168-197) on the nodes of slice sb.
 template <int PREC>
-__device__ __forceinline__ void adr_update_slice(const Dev &d, const StepBufs &b, int64_t sb, int lane)
+__device__ __forceinline__ void adr_update_slice(const Dev &d, const StepBufs &b, int64_t sb, int lane,
+                                                 int64_t it)
 {
     const int64_t nN = d.n_nodes;
     const double cn = __ldcg(&d.scal[0]);
@@ -971,6 +986,7 @@ __device__ __forceinline__ void adr_update_slice(const Dev &d, const StepBufs &b
             un[dof] = ue; vn[dof] = vh; xn3[dof] = d.X[e] + ue;
         }
         if (d.n_pen) apply_contact(d, b.n, i, un, vn, xn3);
+        if (d.n_probe) record_probes(d, it, i, un);
         float uh[3], ul[3];
         bool bad = false, far = false;
 #pragma unroll
@@ -993,9 +1009,9 @@ __device__ __forceinline__ void adr_update_slice(const Dev &d, const StepBufs &b
 // ADR phase B on slices gwarp, gwarp + nwarps, ...
 template <int PREC>
 __device__ __forceinline__ void adr_update(const Dev &d, const StepBufs &b, int lane, int64_t gwarp,
-                                           int64_t nwarps)
+                                           int64_t nwarps, int64_t it)
 {
-    for (int64_t sb = gwarp; sb < d.n_slices; sb += nwarps) adr_update_slice<PREC>(d, b, sb, lane);
+    for (int64_t sb = gwarp; sb < d.n_slices; sb += nwarps) adr_update_slice<PREC>(d, b, sb, lane, it);
 }
 
 // Global-gather kernel: neighbour data read from HBM/L2 per entry. Used for
@@ -1034,7 +1050,7 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
         }
         if (SCHEME == BBPD_SCHEME_ADR) {
             if (!grid_barrier(d)) return;
-            adr_update<PREC>(d, b, lane, gwarp, nwarps);
+            adr_update<PREC>(d, b, lane, gwarp, nwarps, it);
         }
         if (!grid_barrier(d)) return;
         if (d.n_pen && blockIdx.x == 0 && threadIdx.x == 0) contact_reaction(d, b.n, it);
@@ -1311,7 +1327,7 @@ __global__ void __launch_bounds__(kBlock, 2) tstep_kernel(Dev d, int64_t step0, 
         }
         if (SCHEME == BBPD_SCHEME_ADR) {
             if (!grid_barrier(d)) return;
-            adr_update<PREC>(d, b, lane, gwarp, nwarps);
+            adr_update<PREC>(d, b, lane, gwarp, nwarps, it);
         }
         if (!grid_barrier(d)) return;
         if (d.n_pen && blockIdx.x == 0 && threadIdx.x == 0) contact_reaction(d, b.n, it);
@@ -1413,7 +1429,7 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
             const int m = member_of(B, w);
             const Dev &d = warp_member(B, m, &s_dev[wib], &s_held[wib], lane);
             const StepBufs b = step_bufs(d, __ldg(&B.mstep[m]) + it);
-            adr_update_slice<PREC>(d, b, w - __ldg(&B.prefix[m]), lane);
+            adr_update_slice<PREC>(d, b, w - __ldg(&B.prefix[m]), lane, it);
         }
         if (!grid_barrier_raw(B.bar, B.err, B.timeout_ns)) return;
         if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -3015,6 +3031,46 @@ extern "C" int bbpd_set_contact(bbpd_solver *S, int n, const bbpd_penetrator *pe
     }
     for (int p = 0; p <= 4; p++) d.pen_off[p] = off[std::min(p, n)];
     d.n_pen = n;
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_set_probes(bbpd_solver *S, int n, const double *node_ids, const int32_t *dofs)
+{
+    if (!S || n < 0 || n > 8 || (n > 0 && (!node_ids || !dofs))) return fail(BBPD_ERR_ARG, "bad argument (at most 8 probes)");
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    if (S->batch) TRY(batch_member_changed(S->batch));
+    Dev &d = S->d;
+    for (int k = 0; k < n; k++) {
+        const double id = node_ids[k];
+        if (!(id >= 1 && id <= (double)S->nN && id == std::floor(id)) || dofs[k] < 0 || dofs[k] > 2)
+            return fail(BBPD_ERR_ARG, "probe %d: node %g / dof %d out of range", k, id, dofs[k]);
+    }
+    if (n > 0 && !d.probe_hist) {
+        double *h = nullptr;
+        TRY(S->alloc(&h, (size_t)(8 * kReactCap)));
+        BBPD_CUDA_TRY(cudaMemset(h, 0, sizeof(double) * 8 * kReactCap));
+        d.probe_hist = h;
+    }
+    for (int k = 0; k < 8; k++) {
+        d.probe_node[k] = k < n ? S->inv[(int64_t)node_ids[k] - 1] : -1;
+        d.probe_dof[k] = k < n ? dofs[k] : 0;
+    }
+    d.n_probe = n;
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_get_probes(bbpd_solver *S, int64_t nsteps, double *out)
+{
+    if (!S || !out || nsteps < 0) return fail(BBPD_ERR_ARG, "bad argument");
+    if (nsteps > kReactCap) return fail(BBPD_ERR_ARG, "at most %lld steps of probes are kept", (long long)kReactCap);
+    if (S->d.n_probe == 0) return fail(BBPD_ERR_ARG, "no probes set");
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    if (S->batch) TRY(batch_member_changed(S->batch));
+    if (nsteps)
+        BBPD_CUDA_TRY(cudaMemcpy(out, S->d.probe_hist, sizeof(double) * (size_t)(nsteps * S->d.n_probe),
+                                 cudaMemcpyDeviceToHost));
     return BBPD_OK;
 }
 

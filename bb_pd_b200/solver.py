@@ -146,6 +146,34 @@ class Solver:
             a.family, a.n_family, a.reaction = N.ptr(self._fam[j]), len(self._fam[j]), int(bool(q.get("reaction", 0)))
         N.check(N.lib().bbpd_set_contact(self._h, len(penetrators), arr))
 
+    def set_probes(self, nodes, dofs) -> None:
+        """Record the displacement of these DOFs (1-based node ids; dof 0 x,
+        1 y, 2 z) at every step; CMOD is the difference of two x probes."""
+        self._pn = np.ascontiguousarray(np.asarray(nodes, dtype=np.float64))
+        self._pd = np.ascontiguousarray(np.asarray(dofs, dtype=np.int32))
+        N.check(N.lib().bbpd_set_probes(self._h, len(self._pn), N.ptr(self._pn),
+                                        self._pd.ctypes.data_as(C.POINTER(C.c_int32))))
+
+    def probes(self, n: int) -> np.ndarray:
+        """Probe values of the first n steps of the last launch, shape (n, n_probes)."""
+        out = np.zeros((n, len(self._pn)), dtype=np.float64)
+        N.check(N.lib().bbpd_get_probes(self._h, n, N.ptr(out)))
+        return out
+
+    def savedata(self, folder: str, name: str) -> str:
+        """Write the state as savedata.m does (output/savedata.m:33-53): a .mat
+        file `<name>_<step>.mat` with deformedCoordinates, fail and
+        flagBondSoftening, step = the last completed time step."""
+        import os
+        import scipy.io
+        step = self.next_step - 1
+        os.makedirs(folder, exist_ok=True)
+        path = os.path.join(folder, f"{name}_{step}.mat")
+        scipy.io.savemat(path, {"deformedCoordinates": self.get("deformed"),
+                                "fail": self.get("fail")[:, None],
+                                "flagBondSoftening": self.get("flag")[:, None]})
+        return path
+
     def reaction(self, n: int) -> np.ndarray:
         """Reaction of the first n steps of the last launch (ADR): the internal
         force summed over the prescribed DOFs; the applied load is its negative."""

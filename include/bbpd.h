@@ -341,6 +341,14 @@ typedef struct bbpd_penetrator {
 } bbpd_penetrator;
 int bbpd_set_contact(bbpd_solver *s, int n, const bbpd_penetrator *penetrators);
 
+/* Record the displacement of up to 8 DOFs (node ids 1-based; dof 0 x, 1 y,
+ * 2 z) at every step of a launch; bbpd_get_probes returns them step-major,
+ * out[it * n + k], for the first nsteps steps of the last launch (4096 kept).
+ * The reference's CMOD (dynamicsolverdisplacementcontrolled.m:118) is the
+ * difference of two x probes. n = 0 removes the probes. */
+int bbpd_set_probes(bbpd_solver *s, int n, const double *node_ids, const int32_t *dofs);
+int bbpd_get_probes(bbpd_solver *s, int64_t nsteps, double *host_out);
+
 /* Reaction of each step of the last launch: with contact (bbpd_set_contact),
  * the reference's reactionForce (dynamicsolverdisplacementcontrolled.m:115),
  * either scheme; without contact (ADR only), the internal nodal force summed

@@ -325,3 +325,34 @@ def test_contact_rejects_overlap_and_missing_density(small):
     t = bb.Solver(nod, **LAWKW["linear"], scheme="adr")
     with pytest.raises(bb.BBPDError):
         t.set_contact(pens[:1])
+
+
+@pytest.mark.parametrize("scheme", ["eulercromer", "adr"])
+def test_probes_record_every_step(small, scheme):
+    """Probes hold each step's displacement of their DOFs: the history of one
+    40-step launch equals 40 single-step launches read back one by one."""
+    kw = dict(LAWKW["trilinear"], scheme=scheme, rate=-3e-6)
+    nodes = [3, 17, small["nNodes"]]
+    dofs = [0, 0, 2]
+    a = bb.Solver(small, **kw)
+    a.set_probes(nodes, dofs)
+    a.step(40)
+    hist = a.probes(40)
+    b = bb.Solver(small, **kw)
+    for it in range(40):
+        b.step(1)
+        u = b.get("displacement")
+        assert all(hist[it, k] == u[n - 1, c] for k, (n, c) in enumerate(zip(nodes, dofs))), it
+    cmod = hist[:, 1] - hist[:, 0]
+    assert cmod.shape == (40,)
+
+
+def test_savedata_mat(small, tmp_path):
+    import scipy.io
+    s = bb.Solver(small, **LAWKW["trilinear"], scheme="adr", rate=-3e-6)
+    s.step(12)
+    path = s.savedata(str(tmp_path), "beam")
+    assert path.endswith("beam_12.mat")
+    m = scipy.io.loadmat(path)
+    assert same(m["deformedCoordinates"], s.get("deformed"))
+    assert m["fail"].shape == (small["nBonds"], 1) and m["flagBondSoftening"].shape == (small["nBonds"], 1)
