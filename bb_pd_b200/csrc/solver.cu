@@ -44,6 +44,9 @@
 #include "physics.cuh"
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -1467,6 +1470,56 @@ __global__ void wait_selftest_kernel(unsigned *word, int *err, unsigned long lon
     if (threadIdx.x == 0 && blockIdx.x == 0) bounded_wait_change(word, 0u, err, timeout_ns);
 }
 
+// Per-bond views of the per-entry state: bond k's two copies sit at ent[k]
+// and ent[nB + k] (the copies are identical, the gather reads the first).
+template <class IDX>
+__global__ void k_bond_gather(const IDX *__restrict__ ent, int64_t nB, const double *__restrict__ bsf,
+                              const uint8_t *__restrict__ st, int field, double *out)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nB; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pos = (int64_t)ent[k];
+        if (field == BBPD_FIELD_BSF) {
+            out[k] = bsf[pos];
+        } else {
+            const uint8_t w = st[pos];
+            out[k] = field == BBPD_FIELD_FLAG ? ((w & ST_SOFT) ? 1.0 : 0.0) : ((w & ST_BROKEN) ? 0.0 : 1.0);
+        }
+    }
+}
+
+// Flag or fail bit of every bond as one byte (0/1).
+template <class IDX>
+__global__ void k_bond_gather_bits(const IDX *__restrict__ ent, int64_t nB, const uint8_t *__restrict__ st,
+                                   int field, uint8_t *out)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nB; k += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t w = st[(int64_t)ent[k]];
+        out[k] = field == BBPD_FIELD_FLAG ? ((w & ST_SOFT) ? 1 : 0) : ((w & ST_BROKEN) ? 0 : 1);
+    }
+}
+
+template <class IDX>
+__global__ void k_bond_scatter(const IDX *__restrict__ ent, int64_t nB, const double *__restrict__ in, int field,
+                               double *bsf, uint8_t *st)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nB; k += (int64_t)gridDim.x * blockDim.x) {
+        const double v = in[k];
+        for (int side = 0; side < 2; side++) {
+            const int64_t pos = (int64_t)ent[side * nB + k];
+            uint8_t w = st[pos];
+            if (field == BBPD_FIELD_BSF) {
+                bsf[pos] = v;
+                w = __double_as_longlong(v) != 0 ? (uint8_t)(w | ST_DAMAGED) : (uint8_t)(w & ~ST_DAMAGED);
+            } else if (field == BBPD_FIELD_FLAG) {
+                w = v == 1 ? (uint8_t)(w | ST_SOFT) : (uint8_t)(w & ~ST_SOFT);
+            } else {
+                w = v == 0 ? (uint8_t)(w | ST_BROKEN) : (uint8_t)(w & ~ST_BROKEN);
+            }
+            st[pos] = w;
+        }
+    }
+}
+
 typedef void (*kernel_t)(Dev, int64_t, int64_t);
 
 // Instances: law x scheme x precision x dictionary-index width x per-entry
@@ -1687,7 +1740,9 @@ struct bbpd_solver {
     double cn = 0;
     std::vector<int32_t> perm;          // device position -> input node
     std::vector<int32_t> inv;           // input node -> device position
-    std::vector<int64_t> ent_i, ent_j;  // bond -> entry positions of its two copies
+    std::unique_ptr<int64_t[]> ent_i, ent_j;  // bond -> entry positions of its two copies (host, until uploaded)
+    void *d_ent = nullptr;              // the same on the device, [ent_i | ent_j], 32-bit when they fit
+    bool ent32 = false;
     Dev d{};
     std::vector<void *> allocs;
     int64_t device_bytes = 0;
@@ -1736,13 +1791,45 @@ struct bbpd_solver {
 // one (a member's descriptor or step changed on the host).
 static int batch_member_changed(bbpd_batch *B);
 
+// Smallest k in [0, n) with bad(k), or -1; the ranges are checked in parallel.
+template <class F>
+static int64_t first_bad(int64_t n, F bad)
+{
+    const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, n / 65536));
+    std::vector<int64_t> first(HT, -1);
+    host_ranges(n, HT, [&](int t, int64_t lo, int64_t hi) {
+        for (int64_t k = lo; k < hi; k++)
+            if (bad(k)) {
+                first[t] = k;
+                return;
+            }
+    });
+    for (int64_t f : first)
+        if (f >= 0) return f;
+    return -1;
+}
+
 static int validate_01(const double *a, int64_t n, const char *name)
 {
     if (!a) return BBPD_OK;
-    for (int64_t i = 0; i < n; i++)
-        if (!(a[i] == 0.0 || a[i] == 1.0)) return fail(BBPD_ERR_ARG, "%s[%lld] is %g, expected 0 or 1", name, (long long)i, a[i]);
+    const int64_t i = first_bad(n, [&](int64_t k) { return !(a[k] == 0.0 || a[k] == 1.0); });
+    if (i >= 0) return fail(BBPD_ERR_ARG, "%s[%lld] is %g, expected 0 or 1", name, (long long)i, a[i]);
     return BBPD_OK;
 }
+
+// Host phases of bbpd_create, printed to stderr when BBPD_TIMING is set.
+struct PhaseTimer {
+    bool on = std::getenv("BBPD_TIMING") != nullptr;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    void mark(const char *name)
+    {
+        if (!on) return;
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "bbpd_create %-16s %8.1f ms\n", name,
+                     std::chrono::duration<double, std::milli>(now - t).count());
+        t = now;
+    }
+};
 
 extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int device,
                            bbpd_solver **out)
@@ -1751,6 +1838,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     if (!pb || !prm || !out) return fail(BBPD_ERR_ARG, "null argument");
     *out = nullptr;
     TRY(require_device());
+    PhaseTimer phase;
     const int64_t nN = pb->n_nodes, nB = pb->n_bonds;
     if (nN < 1 || nB < 0) return fail(BBPD_ERR_ARG, "n_nodes must be >= 1 and n_bonds >= 0");
     if (nN >= MAX_NODES) return fail(BBPD_ERR_UNSUPPORTED, "at most %lld nodes per solver", (long long)MAX_NODES - 1);
@@ -1770,21 +1858,26 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     TRY(validate_01(pb->fail, nB, "fail"));
     TRY(validate_01(pb->constraint_flag, 3 * nN, "CONSTRAINTFLAG"));
     TRY(validate_01(pb->prescribed_flag, 3 * nN, "prescribed flag"));
-    if (pb->bond_type)
-        for (int64_t k = 0; k < nB; k++) {
-            double t = pb->bond_type[k];
-            if (!(t == 0 || t == 1 || t == 2)) return fail(BBPD_ERR_ARG, "BONDTYPE[%lld] = %g", (long long)k, t);
-        }
-    if (pb->stretch_plastic)
-        for (int64_t k = 0; k < nB; k++)
-            if (pb->stretch_plastic[k] != 0)
-                return fail(BBPD_ERR_UNSUPPORTED, "non-zero stretchPlastic (steel plasticity) is not on this path");
+    if (pb->bond_type) {
+        const double *bt = pb->bond_type;
+        const int64_t k = first_bad(nB, [&](int64_t q) { return !(bt[q] == 0 || bt[q] == 1 || bt[q] == 2); });
+        if (k >= 0) return fail(BBPD_ERR_ARG, "BONDTYPE[%lld] = %g", (long long)k, bt[k]);
+    }
+    if (pb->stretch_plastic) {
+        const double *sp = pb->stretch_plastic;
+        if (first_bad(nB, [&](int64_t q) { return sp[q] != 0; }) >= 0)
+            return fail(BBPD_ERR_UNSUPPORTED, "non-zero stretchPlastic (steel plasticity) is not on this path");
+    }
     const double *bl = pb->bondlist;
-    for (int64_t k = 0; k < nB; k++) {
-        double a = bl[k], b = bl[nB + k];
-        if (!(a >= 1 && b >= 1 && a <= (double)nN && b <= (double)nN && a == std::floor(a) &&
-              b == std::floor(b) && a != b))
-            return fail(BBPD_ERR_ARG, "BONDLIST row %lld = (%g, %g) is not a pair of distinct node ids", (long long)k + 1, a, b);
+    {
+        const int64_t k = first_bad(nB, [&](int64_t q) {
+            const double a = bl[q], b = bl[nB + q];
+            return !(a >= 1 && b >= 1 && a <= (double)nN && b <= (double)nN && a == std::floor(a) &&
+                     b == std::floor(b) && a != b);
+        });
+        if (k >= 0)
+            return fail(BBPD_ERR_ARG, "BONDLIST row %lld = (%g, %g) is not a pair of distinct node ids", (long long)k + 1,
+                        bl[k], bl[nB + k]);
     }
 
     if (cudaSetDevice(device) != cudaSuccess) {
@@ -1800,6 +1893,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     S->has_density = pb->density != nullptr;
     const int T = prm->n_chunks;
 
+    phase.mark("validate");
     // node order
     S->perm.resize(nN);
     S->inv.resize(nN);
@@ -1837,6 +1931,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     for (int64_t p = 0; p < nN; p++) S->inv[S->perm[p]] = (int32_t)p;
     const int32_t *inv = S->inv.data();
 
+    phase.mark("node order");
     // FP32 form: a dictionary of (L0, VCF, BONDSTIFFNESS, bond vector in FP32)
     // with one id per directed entry; kept when it fits 16-bit ids
     std::vector<uint32_t> bond_cid(nB), cid_j;
@@ -1854,20 +1949,26 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
             return KeyX{bits_of(pb->undeformed_length[k]), bits_of(pb->volume_correction[k]),
                         bits_of(pb->bond_stiffness[k]), fbits(fx), fbits(fy), fbits(fz)};
         };
+        // The reverse copy's key is the forward key with the bond vector
+        // negated (IEEE subtraction is sign-symmetric; a +0 component stays
+        // +0), so only forward keys are hashed and the reverse ids come from
+        // the negation of each dictionary key.
+        auto negx = [](uint32_t f) { return (f & 0x7FFFFFFFu) ? (f ^ 0x80000000u) : f; };
+        auto neg = [&](const KeyX &q) { return KeyX{q.a, q.b, q.c, negx(q.x), negx(q.y), negx(q.z)}; };
         const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
         std::vector<std::unordered_map<KeyX, uint32_t, KeyXHash>> local(HT);
         host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
             auto &m = local[t];
-            for (int64_t k = lo; k < hi && m.size() <= 70000; k++) {
-                m.emplace(keyx(k, 0), 0u);
-                m.emplace(keyx(k, 1), 0u);
-            }
+            for (int64_t k = lo; k < hi && m.size() <= 70000; k++) m.emplace(keyx(k, 0), 0u);
         });
         std::unordered_map<KeyX, uint32_t, KeyXHash> all;
         bool overflow = false;
         for (auto &m : local) {
             if (m.size() > 70000) overflow = true;
-            for (auto &kv : m) all.emplace(kv.first, 0u);
+            for (auto &kv : m) {
+                all.emplace(kv.first, 0u);
+                all.emplace(neg(kv.first), 0u);
+            }
         }
         if (all.size() > 65535) overflow = true;
         if (!overflow) {
@@ -1876,11 +1977,14 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
             for (auto &kv : all) keys.push_back(kv.first);
             std::sort(keys.begin(), keys.end());
             for (size_t q = 0; q < keys.size(); q++) all[keys[q]] = (uint32_t)q;
+            std::vector<uint32_t> negid(keys.size());
+            for (size_t q = 0; q < keys.size(); q++) negid[q] = all.find(neg(keys[q]))->second;
             cid_j.resize(nB);
             host_ranges(nB, HT, [&](int, int64_t lo, int64_t hi) {
                 for (int64_t k = lo; k < hi; k++) {
-                    bond_cid[k] = all.find(keyx(k, 0))->second;
-                    cid_j[k] = all.find(keyx(k, 1))->second;
+                    const uint32_t id = all.find(keyx(k, 0))->second;
+                    bond_cid[k] = id;
+                    cid_j[k] = negid[id];
                 }
             });
             dict.resize(keys.size());
@@ -1904,6 +2008,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
             S->ndict = (int64_t)dict.size();
         }
     }
+    phase.mark("fp32 dictionary");
     if (S->prec != kP32X) {
         const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
         std::vector<std::unordered_map<Key3, uint32_t, Key3Hash>> local(HT);
@@ -1959,6 +2064,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         S->ndict = (int64_t)dict.size();
     }
 
+    phase.mark("dictionary");
     // per-node lists in bond order, laid out in 32-node slices. Stable
     // counting sort over HT contiguous bond ranges.
     const int64_t ns = (nN + 31) / 32;
@@ -1993,19 +2099,21 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     }
     const int64_t ne = sptr[ns];
     S->ne = ne;
-    std::vector<uint32_t> colw(ne, 0);
-    std::vector<uint16_t> cid16;
-    std::vector<uint32_t> cid32;
-    if (S->wide) cid32.assign(ne, 0);
-    else cid16.assign(ne, 0);
-    std::vector<uint8_t> st(ne, 0);
-    std::vector<int32_t> bond_of(ne, -1);
+    // Entry streams, left uninitialised here: the scatter below writes every
+    // real entry and the chunk pass zeroes the padding, both in parallel.
+    std::unique_ptr<uint32_t[]> colw(new uint32_t[std::max<int64_t>(ne, 1)]);
+    std::unique_ptr<uint16_t[]> cid16;
+    std::unique_ptr<uint32_t[]> cid32;
+    if (S->wide) cid32.reset(new uint32_t[std::max<int64_t>(ne, 1)]);
+    else cid16.reset(new uint16_t[std::max<int64_t>(ne, 1)]);
+    std::unique_ptr<uint8_t[]> st(new uint8_t[std::max<int64_t>(ne, 1)]);
+    std::unique_ptr<int32_t[]> bond_of(new int32_t[std::max<int64_t>(ne, 1)]);
     std::vector<double> s0e, s1e, sce;
     if (pb->s0) s0e.assign(ne, 0.0);
     if (pb->s1) s1e.assign(ne, 0.0);
     if (pb->sc || S->wide) sce.assign(ne, prm->sc);   // 32-bit-index instances always read a stream
-    S->ent_i.resize(nB);
-    S->ent_j.resize(nB);
+    S->ent_i.reset(new int64_t[std::max<int64_t>(nB, 1)]);
+    S->ent_j.reset(new int64_t[std::max<int64_t>(nB, 1)]);
     host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
         int32_t *rank = cnt[t].data();
         for (int64_t k = lo; k < hi; k++) {
@@ -2029,20 +2137,31 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
             }
         }
     });
+    phase.mark("slices");
     // chunk starts: an entry whose bond lies in another OpenMP chunk than the
-    // previous entry of the same list
-    host_parallel_for(nN, [&](int64_t me) {
+    // previous entry of the same list; padding slots (up to the slice's list
+    // length, lanes past the last node included) are zeroed
+    host_parallel_for(ns * 32, [&](int64_t me) {
         int prev = -1;
-        for (int32_t r = 0; r < deg[me]; r++) {
+        const int32_t dme = me < nN ? deg[me] : 0;
+        for (int32_t r = 0; r < dme; r++) {
             const int64_t pos = entry_pos(sptr[me / 32], r, (int)(me % 32));
             const int c = chunk_of_host(bond_of[pos], nB, T);
             if (c != prev) colw[pos] |= F_CHUNK;
             prev = c;
         }
+        for (int32_t r = dme; r < slen[me / 32]; r++) {
+            const int64_t pos = entry_pos(sptr[me / 32], r, (int)(me % 32));
+            colw[pos] = 0;
+            if (S->wide) cid32[pos] = 0;
+            else cid16[pos] = 0;
+            st[pos] = 0;
+        }
     });
-    std::vector<int32_t>().swap(bond_of);
+    bond_of.reset();
     cnt.clear();
 
+    phase.mark("chunk starts");
     // Tiles for the tiled kernel: per tile the sorted list of outside nodes its
     // entries read, and per entry a 12-bit index into [tile nodes, halo].
     std::vector<uint16_t> jw;
@@ -2131,6 +2250,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         }
     }
 
+    phase.mark("tiles");
     // node arrays in device order
     auto perm3 = [&](const double *src, std::vector<double> &dst) {
         dst.assign(3 * nN, 0.0);
@@ -2169,6 +2289,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         nflag[p] = f;
     }
 
+    phase.mark("node arrays");
     // device buffers
     Dev &d = S->d;
     d.n_nodes = nN;
@@ -2185,13 +2306,13 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         TRY(S->put((int64_t **)&d.halo_ptr, hptr));
         TRY(S->put((uint32_t **)&d.halo, halo));
     } else {
-        TRY(S->put((uint32_t **)&d.colw, colw));
+        TRY(S->put((uint32_t **)&d.colw, colw.get(), (size_t)ne));
     }
-    std::vector<uint32_t>().swap(colw);
+    colw.reset();
     std::vector<uint16_t>().swap(jw);
-    if (S->wide) TRY(S->put((uint32_t **)&d.cid, cid32));
-    else TRY(S->put((uint16_t **)&d.cid, cid16));
-    TRY(S->put(&d.st, st));
+    if (S->wide) TRY(S->put((uint32_t **)&d.cid, cid32.get(), (size_t)ne));
+    else TRY(S->put((uint16_t **)&d.cid, cid16.get(), (size_t)ne));
+    TRY(S->put(&d.st, st.get(), (size_t)ne));
     TRY(S->alloc(&d.bsf, (size_t)ne));
     BBPD_CUDA_TRY(cudaMemset(d.bsf, 0, sizeof(double) * std::max<int64_t>(ne, 1)));
     TRY(S->put((DictEntry **)&d.dict, dict));
@@ -2268,6 +2389,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         if (!coord_safe(x0[e])) sticky[0] = 1u;
     TRY(S->put(&d.sticky, sticky));
 
+    phase.mark("uploads");
     // scalars
     LawScalars &P = d.P;
     P.s0 = prm->s0; P.s1 = prm->s1; P.sc = prm->sc;
@@ -2323,6 +2445,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     }
     // the uploads above ran on the legacy default stream; wait for them only,
     // not for other solvers' launches on their own streams
+    phase.mark("kernel setup");
     BBPD_CUDA_TRY(cudaStreamSynchronize(0));
     *out = guard_.release();
     return BBPD_OK;
@@ -2412,6 +2535,35 @@ static double *field_ptr(bbpd_solver *S, int field, bool &nodal)
     }
 }
 
+// The bond -> entry map on the device (first per-bond get or set): 32-bit
+// positions when the layout allows; the host copy is released after.
+static int upload_entry_map(bbpd_solver *S)
+{
+    if (S->d_ent) return BBPD_OK;
+    const int64_t nB = S->nB;
+    S->ent32 = S->ne < ((int64_t)1 << 32);
+    if (S->ent32) {
+        std::vector<uint32_t> m(2 * nB);
+        host_parallel_for(nB, [&](int64_t k) {
+            m[k] = (uint32_t)S->ent_i[k];
+            m[nB + k] = (uint32_t)S->ent_j[k];
+        });
+        uint32_t *d = nullptr;
+        TRY(S->put(&d, m));
+        S->d_ent = d;
+    } else {
+        std::vector<int64_t> m(2 * nB);
+        std::copy(S->ent_i.get(), S->ent_i.get() + nB, m.begin());
+        std::copy(S->ent_j.get(), S->ent_j.get() + nB, m.begin() + nB);
+        int64_t *d = nullptr;
+        TRY(S->put(&d, m));
+        S->d_ent = d;
+    }
+    S->ent_i.reset();
+    S->ent_j.reset();
+    return BBPD_OK;
+}
+
 extern "C" int bbpd_get(bbpd_solver *S, int field, double *out)
 {
     if (!S || !out) return fail(BBPD_ERR_ARG, "null argument");
@@ -2428,22 +2580,40 @@ extern "C" int bbpd_get(bbpd_solver *S, int field, double *out)
             for (int64_t p = 0; p < nN; p++) out[S->perm[p] + c * nN] = h[p + c * nN];
         return BBPD_OK;
     }
-    if (field == BBPD_FIELD_BSF) {
-        std::vector<double> h(std::max<int64_t>(S->ne, 1));
-        BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.bsf, sizeof(double) * S->ne, cudaMemcpyDeviceToHost));
-        for (int64_t k = 0; k < nB; k++) out[k] = h[S->ent_i[k]];
+    if (field != BBPD_FIELD_BSF && field != BBPD_FIELD_FLAG && field != BBPD_FIELD_FAIL)
+        return fail(BBPD_ERR_ARG, "unknown field %d", field);
+    if (nB == 0) return BBPD_OK;
+    TRY(upload_entry_map(S));
+    const int blocks = (int)std::min<int64_t>((nB + 255) / 256, 148 * 32);
+    if (field != BBPD_FIELD_BSF) {   // 0/1 values cross as bytes
+        uint8_t *tb = nullptr;
+        BBPD_CUDA_TRY(cudaMallocAsync(&tb, (size_t)nB, S->stream));
+        if (S->ent32)
+            k_bond_gather_bits<uint32_t><<<blocks, 256, 0, S->stream>>>((const uint32_t *)S->d_ent, nB, S->d.st, field, tb);
+        else
+            k_bond_gather_bits<int64_t><<<blocks, 256, 0, S->stream>>>((const int64_t *)S->d_ent, nB, S->d.st, field, tb);
+        std::unique_ptr<uint8_t[]> hb(new uint8_t[nB]);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hb.get(), tb, (size_t)nB, cudaMemcpyDeviceToHost, S->stream);
+        cudaFreeAsync(tb, S->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+        if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "get field %d: %s", field, cudaGetErrorString(e));
+        const uint8_t *b = hb.get();
+        host_parallel_for(nB, [&](int64_t k) { out[k] = (double)b[k]; });
         return BBPD_OK;
     }
-    if (field == BBPD_FIELD_FLAG || field == BBPD_FIELD_FAIL) {
-        std::vector<uint8_t> h(std::max<int64_t>(S->ne, 1));
-        BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.st, S->ne, cudaMemcpyDeviceToHost));
-        for (int64_t k = 0; k < nB; k++) {
-            const uint8_t w = h[S->ent_i[k]];
-            out[k] = field == BBPD_FIELD_FLAG ? ((w & ST_SOFT) ? 1.0 : 0.0) : ((w & ST_BROKEN) ? 0.0 : 1.0);
-        }
-        return BBPD_OK;
-    }
-    return fail(BBPD_ERR_ARG, "unknown field %d", field);
+    double *tmp = nullptr;
+    BBPD_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(double) * (size_t)nB, S->stream));
+    if (S->ent32)
+        k_bond_gather<uint32_t><<<blocks, 256, 0, S->stream>>>((const uint32_t *)S->d_ent, nB, S->d.bsf, S->d.st, field, tmp);
+    else
+        k_bond_gather<int64_t><<<blocks, 256, 0, S->stream>>>((const int64_t *)S->d_ent, nB, S->d.bsf, S->d.st, field, tmp);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, sizeof(double) * (size_t)nB, cudaMemcpyDeviceToHost, S->stream);
+    cudaFreeAsync(tmp, S->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+    if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "get field %d: %s", field, cudaGetErrorString(e));
+    return BBPD_OK;
 }
 
 extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
@@ -2486,29 +2656,22 @@ extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
     if (field != BBPD_FIELD_BSF && field != BBPD_FIELD_FLAG && field != BBPD_FIELD_FAIL)
         return fail(BBPD_ERR_ARG, "unknown field %d", field);
     if (field != BBPD_FIELD_BSF) TRY(validate_01(in, nB, field == BBPD_FIELD_FLAG ? "flagBondSoftening" : "fail"));
-    const int64_t ne1 = std::max<int64_t>(S->ne, 1);
-    std::vector<uint8_t> st(ne1);
-    BBPD_CUDA_TRY(cudaMemcpy(st.data(), S->d.st, S->ne, cudaMemcpyDeviceToHost));
-    if (field == BBPD_FIELD_BSF) {
-        std::vector<double> h(ne1);
-        BBPD_CUDA_TRY(cudaMemcpy(h.data(), S->d.bsf, sizeof(double) * S->ne, cudaMemcpyDeviceToHost));
-        for (int64_t k = 0; k < nB; k++) {
-            const bool dmg = bits_of(in[k]) != 0;
-            for (int64_t pos : {S->ent_i[k], S->ent_j[k]}) {
-                h[pos] = in[k];
-                st[pos] = dmg ? (uint8_t)(st[pos] | ST_DAMAGED) : (uint8_t)(st[pos] & ~ST_DAMAGED);
-            }
-        }
-        BBPD_CUDA_TRY(cudaMemcpy(S->d.bsf, h.data(), sizeof(double) * S->ne, cudaMemcpyHostToDevice));
-    } else {
-        const uint8_t bit = field == BBPD_FIELD_FLAG ? ST_SOFT : ST_BROKEN;
-        for (int64_t k = 0; k < nB; k++) {
-            const bool on = field == BBPD_FIELD_FLAG ? in[k] == 1 : in[k] == 0;
-            for (int64_t pos : {S->ent_i[k], S->ent_j[k]})
-                st[pos] = on ? (uint8_t)(st[pos] | bit) : (uint8_t)(st[pos] & ~bit);
-        }
+    if (nB == 0) return BBPD_OK;
+    TRY(upload_entry_map(S));
+    double *tmp = nullptr;
+    BBPD_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(double) * (size_t)nB, S->stream));
+    cudaError_t e = cudaMemcpyAsync(tmp, in, sizeof(double) * (size_t)nB, cudaMemcpyHostToDevice, S->stream);
+    const int blocks = (int)std::min<int64_t>((nB + 255) / 256, 148 * 32);
+    if (e == cudaSuccess) {
+        if (S->ent32)
+            k_bond_scatter<uint32_t><<<blocks, 256, 0, S->stream>>>((const uint32_t *)S->d_ent, nB, tmp, field, S->d.bsf, S->d.st);
+        else
+            k_bond_scatter<int64_t><<<blocks, 256, 0, S->stream>>>((const int64_t *)S->d_ent, nB, tmp, field, S->d.bsf, S->d.st);
+        e = cudaGetLastError();
     }
-    BBPD_CUDA_TRY(cudaMemcpy(S->d.st, st.data(), S->ne, cudaMemcpyHostToDevice));
+    cudaFreeAsync(tmp, S->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+    if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "set field %d: %s", field, cudaGetErrorString(e));
     return BBPD_OK;
 }
 
