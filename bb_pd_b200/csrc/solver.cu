@@ -1387,11 +1387,11 @@ __device__ __forceinline__ const Dev &warp_member(const BatchCtl &B, int m, Dev 
     return *slot;
 }
 
-// The members of one class (one law, one kernel precision variant) stepped by
-// one persistent launch; a batch of mixed classes replays one such launch per
-// class. Every instance is as specialised as the single-solver kernel; the
-// per-entry critical stretch is decided from each member's descriptor.
-template <int LAW, int PREC>
+// The members of one class (one law, one kernel precision variant, per-entry
+// critical stretch or not) stepped by one persistent launch; a batch of mixed
+// classes replays one such launch per class. Every instance is as
+// specialised as the single-solver kernel.
+template <int LAW, int PREC, bool SCE>
 __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl B, int64_t nsteps)
 {
     __shared__ Dev s_dev[kBlock / 32];
@@ -1421,8 +1421,8 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
                 const StepBufs b = step_bufs(d, __ldg(&B.mstep[m]) + it);
                 const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
                 double tx, ty, tz;
-                if (PREC == kP32X) slice_forces_x<LAW, uint16_t, 2>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
-                else slice_forces<LAW, PREC, uint16_t, 2>(d, sl, lane, safe, b.xs, tx, ty, tz);
+                if (PREC == kP32X) slice_forces_x<LAW, uint16_t, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
+                else slice_forces<LAW, PREC, uint16_t, SCE>(d, sl, lane, safe, b.xs, tx, ty, tz);
                 finish_slice<BBPD_SCHEME_ADR, PREC>(d, b, sl, lane, tx, ty, tz, it);
             }
             gi = gnext;
@@ -1446,21 +1446,21 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
 
 typedef void (*batch_kernel_t)(BatchCtl, int64_t);
 
-template <int PREC>
+template <int PREC, bool SCE>
 batch_kernel_t pick_batch_law(int law)
 {
     switch (law) {
-    case BBPD_LAW_LINEAR: return batch_kernel<BBPD_LAW_LINEAR, PREC>;
-    case BBPD_LAW_BILINEAR: return batch_kernel<BBPD_LAW_BILINEAR, PREC>;
-    case BBPD_LAW_TRILINEAR: return batch_kernel<BBPD_LAW_TRILINEAR, PREC>;
-    default: return batch_kernel<BBPD_LAW_EXPONENTIAL, PREC>;
+    case BBPD_LAW_LINEAR: return batch_kernel<BBPD_LAW_LINEAR, PREC, SCE>;
+    case BBPD_LAW_BILINEAR: return batch_kernel<BBPD_LAW_BILINEAR, PREC, SCE>;
+    case BBPD_LAW_TRILINEAR: return batch_kernel<BBPD_LAW_TRILINEAR, PREC, SCE>;
+    default: return batch_kernel<BBPD_LAW_EXPONENTIAL, PREC, SCE>;
     }
 }
 
-batch_kernel_t pick_batch_kernel(int law, int prec)
+batch_kernel_t pick_batch_kernel(int law, int prec, bool sce)
 {
-    if (prec == kP32X) return pick_batch_law<kP32X>(law);
-    return pick_batch_law<kP64>(law);
+    if (prec == kP32X) return sce ? pick_batch_law<kP32X, true>(law) : pick_batch_law<kP32X, false>(law);
+    return sce ? pick_batch_law<kP64, true>(law) : pick_batch_law<kP64, false>(law);
 }
 
 // Self-test of the bounded wait: one thread waits on a word that nothing
@@ -2753,6 +2753,7 @@ extern "C" int bbpd_get_info(bbpd_solver *S, bbpd_info *info)
 // by one persistent launch of its own specialised kernel.
 struct BatchClass {
     int law = 0, prec = kP64;
+    bool sce = false;                        // members read a per-entry critical stretch
     batch_kernel_t kernel = nullptr;
     std::vector<bbpd_solver *> members;
     Dev *d_members = nullptr;
@@ -2854,9 +2855,11 @@ extern "C" int bbpd_batch_create(int device, int precision, bbpd_batch **out)
     for (int law = 0; law < 4; law++)
         for (int pv : {kP64, kP32X}) {
             if (pv == kP32X && B->prec == kP64) continue;
-            int o = 0;
-            BBPD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void *)pick_batch_kernel(law, pv), kBlock, 0));
-            occ = std::min(occ, o);
+            for (bool sce : {false, true}) {
+                int o = 0;
+                BBPD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void *)pick_batch_kernel(law, pv, sce), kBlock, 0));
+                occ = std::min(occ, o);
+            }
         }
     if (occ < 1) return fail(BBPD_ERR_CUDA, "batch kernel cannot be resident");
     B->occ = occ;
@@ -2912,17 +2915,19 @@ static int batch_rebuild(bbpd_batch *B)
     old.swap(B->classes);
     for (bbpd_solver *S : B->members) {
         BatchClass *c = nullptr;
+        const bool sce = S->d.sce != nullptr;
         for (BatchClass &k : B->classes)
-            if (k.law == S->prm.law && k.prec == S->prec) c = &k;
+            if (k.law == S->prm.law && k.prec == S->prec && k.sce == sce) c = &k;
         if (!c) {
             B->classes.emplace_back();
             c = &B->classes.back();
             c->law = S->prm.law;
             c->prec = S->prec;
-            c->kernel = pick_batch_kernel(c->law, c->prec);
+            c->sce = sce;
+            c->kernel = pick_batch_kernel(c->law, c->prec, sce);
             // reuse the device tables of the same class from before
             for (BatchClass &o : old)
-                if (o.law == c->law && o.prec == c->prec && o.cap) {
+                if (o.law == c->law && o.prec == c->prec && o.sce == c->sce && o.cap) {
                     c->d_members = o.d_members;
                     c->d_prefix = o.d_prefix;
                     c->d_mstep = o.d_mstep;
