@@ -10,6 +10,7 @@
 // synchronize.
 #include "bbpd_internal.h"
 #include "physics.cuh"
+#include "staging.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -624,13 +625,13 @@ int mirror(const void *h, size_t bytes, bool in, double **d)
         it = g_mirrors.find(h);
     }
     *d = (double *)it->second.dev;
-    if (in && bytes) BBPD_CUDA_TRY(cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
+    if (in && bytes) return staging::upload_copy((char *)*d, (const char *)h, (int64_t)bytes, 0);
     return BBPD_OK;
 }
 
 int download(void *h, const double *d, size_t bytes)
 {
-    if (bytes) BBPD_CUDA_TRY(cudaMemcpy(h, d, bytes, cudaMemcpyDeviceToHost));
+    if (bytes) return staging::download_copy((char *)h, (const char *)d, (int64_t)bytes, 0);
     return BBPD_OK;
 }
 

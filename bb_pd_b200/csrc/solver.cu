@@ -1,6 +1,7 @@
 // Fused solver: the whole BB_PD time loop in one persistent cooperative kernel.
 //
-// Layout in HBM (built on the host at bbpd_create):
+// Layout in HBM (built at bbpd_create, on the device for the input and Morton
+// node orders and on the host for the tiled order):
 //   nodes   SoA float64 (x of all nodes, then y, then z), in input order or
 //           Morton order; one flags byte per node (held / prescribed DOFs). The
 //           FP32 form adds the displacement split into FP32 high and low parts
@@ -42,6 +43,9 @@
 #include "bbpd_internal.h"
 #include "divide.cuh"
 #include "physics.cuh"
+#include "staging.cuh"
+
+#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <chrono>
@@ -1520,6 +1524,139 @@ __global__ void k_bond_scatter(const IDX *__restrict__ ent, int64_t nB, const do
     }
 }
 
+// ---- layout build on the device (input and Morton node orders) ----
+//
+// Directed entry q = 2k + side of bond k sits in the list of node key[q]
+// (side 0: the bond's first BONDLIST column, side 1: its second). A stable
+// radix sort of the entries by node keeps every list in bond order, exactly
+// as the reference's nodal loop meets the bonds; the run bounds of the sorted
+// keys give each node its degree and each entry its rank in the list.
+
+__global__ void k_iota(uint32_t *v, int64_t n)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        v[q] = (uint32_t)q;
+}
+
+// first[p] / last[p]: sorted positions bounding node p's run (both stay 0 for
+// a node without bonds)
+__global__ void k_run_bounds(const uint32_t *__restrict__ skey, int64_t n, uint32_t *first, uint32_t *last)
+{
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = skey[r];
+        if (r == 0 || skey[r - 1] != p) first[p] = (uint32_t)r;
+        if (r == n - 1 || skey[r + 1] != p) last[p] = (uint32_t)(r + 1);
+    }
+}
+
+// One warp per 32-node slice: node degrees, the slice's list length (its
+// longest list rounded up to whole groups of 4) and its entry count.
+__global__ void k_slice_lengths(const uint32_t *__restrict__ first, const uint32_t *__restrict__ last, int64_t nN,
+                                int64_t ns, int32_t *deg, int32_t *slen, int64_t *scount)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t s = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; s < ns; s += warps) {
+        const int64_t p = s * 32 + lane;
+        const int32_t dg = p < nN ? (int32_t)(last[p] - first[p]) : 0;
+        if (p < nN) deg[p] = dg;
+        const int32_t m = (__reduce_max_sync(0xffffffffu, (unsigned)dg) + 3) & ~3;
+        if (lane == 0) {
+            slen[s] = m;
+            scount[s] = (int64_t)m * 32;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) scount[ns] = 0;
+}
+
+struct LayoutArgs {
+    const uint32_t *key;      // [2 nB] node of entry q, unsorted
+    const uint32_t *skey;     // sorted keys
+    const uint32_t *sval;     // sorted entry ids q
+    const uint32_t *first;    // [nN] first sorted position of each node
+    const int64_t *sptr;      // [ns + 1] slice offsets
+    const uint16_t *bcid;     // [nB] dictionary id of the forward copy; null: id = k (32-bit ids)
+    const uint16_t *negid;    // FP32 form: id of the reversed bond vector, else null
+    const uint8_t *bflag;     // [nB] bit 0: fail == 0, bits 1-2: BONDTYPE; or null
+    const double *s0, *s1, *sc;   // per-bond law parameters or null
+    int64_t nB;
+    int T;                    // OpenMP chunks of the reference's bond loop
+    uint32_t *colw;
+    void *cid;                // u16, or u32 when bcid is null
+    uint8_t *st;
+    double *s0e, *s1e, *sce;
+    void *ent;                // [2 nB] bond -> entry map, u32 or i64
+    int ent32;
+};
+
+// Every directed entry to its slot: neighbour, BONDTYPE and chunk-start bits,
+// dictionary id, fail state, optional law parameters, and the bond -> entry
+// map. An entry starts an OpenMP chunk when its bond lies in another chunk
+// than the previous entry of the same list.
+__global__ void k_layout_scatter(LayoutArgs a)
+{
+    const int64_t n = 2 * a.nB;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t q = a.sval[r], p = a.skey[r];
+        const int64_t k = q >> 1;
+        const int side = (int)(q & 1u);
+        const int64_t rank = r - (int64_t)a.first[p];
+        const int64_t pos = entry_pos(a.sptr[p >> 5], rank, (int)(p & 31u));
+        const uint8_t fl = a.bflag ? a.bflag[k] : (uint8_t)0;
+        const bool cs = rank == 0 || omp_chunk_of(k, a.nB, a.T) != omp_chunk_of((int64_t)(a.sval[r - 1] >> 1), a.nB, a.T);
+        a.colw[pos] = a.key[q ^ 1u] | ((uint32_t)(fl >> 1) << BT_SHIFT) | (cs ? F_CHUNK : 0u);
+        if (a.bcid) {
+            uint16_t c = a.bcid[k];
+            if (side && a.negid) c = a.negid[c];
+            ((uint16_t *)a.cid)[pos] = c;
+        } else {
+            ((uint32_t *)a.cid)[pos] = (uint32_t)k;
+        }
+        a.st[pos] = (fl & 1u) ? ST_BROKEN : (uint8_t)0;
+        if (a.s0) a.s0e[pos] = a.s0[k];
+        if (a.s1) a.s1e[pos] = a.s1[k];
+        if (a.sc) a.sce[pos] = a.sc[k];
+        if (a.ent32) ((uint32_t *)a.ent)[side * a.nB + k] = (uint32_t)pos;
+        else ((int64_t *)a.ent)[side * a.nB + k] = pos;
+    }
+}
+
+__global__ void k_fill(double *v, int64_t n, double x)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        v[q] = x;
+}
+
+// Initial node state from the staged coordinates and flags: u holds the step-1
+// prescribed value U1 on prescribed DOFs and 0 elsewhere, both position
+// buffers hold X + u, and the FP32 form gets the split record of u.
+__global__ void k_node_init(Dev d, double U1)
+{
+    const int64_t nN = d.n_nodes;
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nN; p += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t f = d.nflag[p];
+        bool far = false;
+        float uh[3], ul[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const int64_t e = p + c * nN;
+            const double u = (f & (8 << c)) ? U1 : 0.0;
+            const double x = d.X[e] + u;
+            d.u[e] = u;
+            d.xb0[e] = x;
+            d.xb1[e] = x;
+            far |= coord_out_of_range(x);
+            uh[c] = (float)u;
+            ul[c] = (float)(u - (double)uh[c]);
+        }
+        if (d.urh0) {
+            d.urh0[p] = d.urh1[p] = make_float4(uh[0], uh[1], uh[2], ul[0]);
+            d.url0[p] = d.url1[p] = make_float2(ul[1], ul[2]);
+        }
+        if (far) atomicOr(d.sticky, 1u);
+    }
+}
+
 typedef void (*kernel_t)(Dev, int64_t, int64_t);
 
 // Instances: law x scheme x precision x dictionary-index width x per-entry
@@ -1682,6 +1819,68 @@ struct Key3Hash {
     }
 };
 
+// Open-addressing hash map (linear probing, power-of-two capacity, at most
+// half full) from a dictionary key to a 32-bit id, for the passes over every
+// bond. The slot is taken from the top bits of a Fibonacci multiply of the
+// key's hash, so every bit of the hash matters.
+template <class K, class H>
+struct FlatMap {
+    static constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+    std::vector<K> keys;
+    std::vector<uint32_t> vals;
+    int bits = 0;
+    size_t count = 0;
+    explicit FlatMap(int b = 10) { reset(b); }
+    void reset(int b)
+    {
+        bits = b;
+        keys.assign((size_t)1 << b, K{});
+        vals.assign((size_t)1 << b, kEmpty);
+        count = 0;
+    }
+    size_t slot(const K &k) const { return (size_t)(((uint64_t)H()(k) * 0x9E3779B97F4A7C15ull) >> (64 - bits)); }
+    size_t probe(const K &k) const
+    {
+        const size_t mask = ((size_t)1 << bits) - 1;
+        size_t h = slot(k);
+        while (vals[h] != kEmpty && !(keys[h] == k)) h = (h + 1) & mask;
+        return h;
+    }
+    // the id of k, storing v for it when k is new
+    uint32_t insert(const K &k, uint32_t v)
+    {
+        if (2 * (count + 1) > ((size_t)1 << bits)) {
+            std::vector<K> ok;
+            std::vector<uint32_t> ov;
+            ok.swap(keys);
+            ov.swap(vals);
+            reset(bits + 1);
+            for (size_t i = 0; i < ov.size(); i++)
+                if (ov[i] != kEmpty) {
+                    const size_t h = probe(ok[i]);
+                    keys[h] = ok[i];
+                    vals[h] = ov[i];
+                    count++;
+                }
+        }
+        const size_t h = probe(k);
+        if (vals[h] == kEmpty) {
+            keys[h] = k;
+            vals[h] = v;
+            count++;
+        }
+        return vals[h];
+    }
+    uint32_t find(const K &k) const { return vals[probe(k)]; }
+    void set(const K &k, uint32_t v) { vals[probe(k)] = v; }   // k present
+    template <class F>
+    void for_each(F f) const
+    {
+        for (size_t i = 0; i < vals.size(); i++)
+            if (vals[i] != kEmpty) f(keys[i], vals[i]);
+    }
+};
+
 DictEntry make_entry(double l0, double vcf, double bs)
 {
     DictEntry e;
@@ -1817,13 +2016,15 @@ static int validate_01(const double *a, int64_t n, const char *name)
     return BBPD_OK;
 }
 
-// Host phases of bbpd_create, printed to stderr when BBPD_TIMING is set.
+// Phases of bbpd_create, printed to stderr when BBPD_TIMING is set (each
+// phase then also waits for the device work it queued).
 struct PhaseTimer {
     bool on = std::getenv("BBPD_TIMING") != nullptr;
     std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
     void mark(const char *name)
     {
         if (!on) return;
+        cudaDeviceSynchronize();
         const auto now = std::chrono::steady_clock::now();
         std::fprintf(stderr, "bbpd_create %-16s %8.1f ms\n", name,
                      std::chrono::duration<double, std::milli>(now - t).count());
@@ -1831,244 +2032,27 @@ struct PhaseTimer {
     }
 };
 
-extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int device,
-                           bbpd_solver **out)
+// Layout built on the host, for the tiled node order: besides the slices it
+// needs each tile's halo list and per-entry local neighbour indices.
+template <class FwdIds>
+static int host_layout(bbpd_solver *S, const bbpd_problem *pb, const int32_t *inv, FwdIds fwd_ids,
+                       const std::vector<uint32_t> &negid, std::vector<DictEntry> &dict, std::vector<float4> &dictx,
+                       PhaseTimer &phase)
 {
-    clear_error();
-    if (!pb || !prm || !out) return fail(BBPD_ERR_ARG, "null argument");
-    *out = nullptr;
-    TRY(require_device());
-    PhaseTimer phase;
-    const int64_t nN = pb->n_nodes, nB = pb->n_bonds;
-    if (nN < 1 || nB < 0) return fail(BBPD_ERR_ARG, "n_nodes must be >= 1 and n_bonds >= 0");
-    if (nN >= MAX_NODES) return fail(BBPD_ERR_UNSUPPORTED, "at most %lld nodes per solver", (long long)MAX_NODES - 1);
-    if (nB >= ((int64_t)1 << 31)) return fail(BBPD_ERR_UNSUPPORTED, "at most 2^31 - 1 bonds per solver");
-    if (!pb->undeformed_coordinates || (nB && (!pb->bondlist || !pb->undeformed_length ||
-        !pb->bond_stiffness || !pb->volume_correction)))
-        return fail(BBPD_ERR_ARG, "missing coordinates or bond arrays");
-    if (prm->law < 0 || prm->law > 3 || prm->scheme < 0 || prm->scheme > 1 || prm->precision < 0 ||
-        prm->precision > 1 || prm->n_chunks < 1 || prm->n_chunks > 4096)
-        return fail(BBPD_ERR_ARG, "bad law/scheme/precision/n_chunks");
-    if (!(prm->failure_functionality == 0.0 || prm->failure_functionality == 1.0))
-        return fail(BBPD_ERR_UNSUPPORTED, "failure_functionality must be 0 or 1");
-    if (prm->scheme == BBPD_SCHEME_ADR && !pb->mass) return fail(BBPD_ERR_ARG, "ADR needs mass");
-    if (prm->scheme == BBPD_SCHEME_EULERCROMER && !pb->density) return fail(BBPD_ERR_ARG, "Euler-Cromer needs density");
-    if (prm->amplitude == BBPD_AMP_SMOOTHSTEP && prm->n_time_steps < 2)
-        return fail(BBPD_ERR_ARG, "smooth step needs n_time_steps >= 2");
-    TRY(validate_01(pb->fail, nB, "fail"));
-    TRY(validate_01(pb->constraint_flag, 3 * nN, "CONSTRAINTFLAG"));
-    TRY(validate_01(pb->prescribed_flag, 3 * nN, "prescribed flag"));
-    if (pb->bond_type) {
-        const double *bt = pb->bond_type;
-        const int64_t k = first_bad(nB, [&](int64_t q) { return !(bt[q] == 0 || bt[q] == 1 || bt[q] == 2); });
-        if (k >= 0) return fail(BBPD_ERR_ARG, "BONDTYPE[%lld] = %g", (long long)k, bt[k]);
-    }
-    if (pb->stretch_plastic) {
-        const double *sp = pb->stretch_plastic;
-        if (first_bad(nB, [&](int64_t q) { return sp[q] != 0; }) >= 0)
-            return fail(BBPD_ERR_UNSUPPORTED, "non-zero stretchPlastic (steel plasticity) is not on this path");
-    }
-    const double *bl = pb->bondlist;
-    {
-        const int64_t k = first_bad(nB, [&](int64_t q) {
-            const double a = bl[q], b = bl[nB + q];
-            return !(a >= 1 && b >= 1 && a <= (double)nN && b <= (double)nN && a == std::floor(a) &&
-                     b == std::floor(b) && a != b);
-        });
-        if (k >= 0)
-            return fail(BBPD_ERR_ARG, "BONDLIST row %lld = (%g, %g) is not a pair of distinct node ids", (long long)k + 1,
-                        bl[k], bl[nB + k]);
-    }
-
-    if (cudaSetDevice(device) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(BBPD_ERR_CUDA, "cudaSetDevice(%d) failed", device);
-    }
-    auto *S = new bbpd_solver;
-    std::unique_ptr<bbpd_solver> guard_(S);
-    S->device = device;
-    S->prm = *prm;
-    S->nN = nN;
-    S->nB = nB;
-    S->has_density = pb->density != nullptr;
+    const bbpd_params *prm = &S->prm;
+    const int64_t nN = S->nN, nB = S->nB, ns = S->ns;
     const int T = prm->n_chunks;
-
-    phase.mark("validate");
-    // node order
-    S->perm.resize(nN);
-    S->inv.resize(nN);
-    std::iota(S->perm.begin(), S->perm.end(), 0);
-    if (prm->node_order == BBPD_ORDER_MORTON || prm->node_order == BBPD_ORDER_TILED) {
-        const double *X = pb->undeformed_coordinates;
-        double lo[3], hi[3];
-        for (int c = 0; c < 3; c++) {
-            lo[c] = *std::min_element(X + c * nN, X + (c + 1) * nN);
-            hi[c] = *std::max_element(X + c * nN, X + (c + 1) * nN);
-        }
-        // Quantize on the shortest bond length when that resolves the domain
-        // in 21 bits per axis: a regular lattice then maps to its integer
-        // indices and aligned Morton blocks are exact bricks (a 512-node tile
-        // is an 8 x 8 x 8 brick). Otherwise scale each axis to 21 bits.
-        double h = 0;
-        for (int64_t k = 0; k < nB; k++) {
-            const double l = pb->undeformed_length[k];
-            if (l > 0 && std::isfinite(l) && (h == 0 || l < h)) h = l;
-        }
-        bool lattice = h > 0;
-        for (int c = 0; c < 3 && lattice; c++) lattice = (hi[c] - lo[c]) / h < 2097000.0;
-        std::vector<uint64_t> key(nN);
-        for (int64_t i = 0; i < nN; i++) {
-            uint32_t q[3];
-            for (int c = 0; c < 3; c++) {
-                const double span = hi[c] - lo[c];
-                if (lattice) q[c] = (uint32_t)std::floor((X[i + c * nN] - lo[c]) / h + 0.5);
-                else q[c] = span > 0 ? (uint32_t)((X[i + c * nN] - lo[c]) / span * 2097151.0) : 0;
-            }
-            key[i] = morton3(q[0], q[1], q[2]);
-        }
-        std::stable_sort(S->perm.begin(), S->perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
-    }
-    for (int64_t p = 0; p < nN; p++) S->inv[S->perm[p]] = (int32_t)p;
-    const int32_t *inv = S->inv.data();
-
-    phase.mark("node order");
-    // FP32 form: a dictionary of (L0, VCF, BONDSTIFFNESS, bond vector in FP32)
-    // with one id per directed entry; kept when it fits 16-bit ids
+    const double *bl = pb->bondlist;
     std::vector<uint32_t> bond_cid(nB), cid_j;
-    std::vector<DictEntry> dict;
-    std::vector<float4> dictx;
-    S->prec = kP64;
-    if (prm->precision == BBPD_PREC_FP32) {
-        S->prec = kP64;   // unless the dictionary of bond vectors fits (below)
-        const double *X = pb->undeformed_coordinates;
-        auto keyx = [&](int64_t k, int side) {
-            int64_t a = (int64_t)bl[k] - 1, b = (int64_t)bl[nB + k] - 1;
-            if (side) std::swap(a, b);   // bond vector X[other] - X[me]
-            const float fx = (float)(X[b] - X[a]), fy = (float)(X[b + nN] - X[a + nN]),
-                        fz = (float)(X[b + 2 * nN] - X[a + 2 * nN]);
-            return KeyX{bits_of(pb->undeformed_length[k]), bits_of(pb->volume_correction[k]),
-                        bits_of(pb->bond_stiffness[k]), fbits(fx), fbits(fy), fbits(fz)};
-        };
-        // The reverse copy's key is the forward key with the bond vector
-        // negated (IEEE subtraction is sign-symmetric; a +0 component stays
-        // +0), so only forward keys are hashed and the reverse ids come from
-        // the negation of each dictionary key.
-        auto negx = [](uint32_t f) { return (f & 0x7FFFFFFFu) ? (f ^ 0x80000000u) : f; };
-        auto neg = [&](const KeyX &q) { return KeyX{q.a, q.b, q.c, negx(q.x), negx(q.y), negx(q.z)}; };
-        const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
-        std::vector<std::unordered_map<KeyX, uint32_t, KeyXHash>> local(HT);
-        host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
-            auto &m = local[t];
-            for (int64_t k = lo; k < hi && m.size() <= 70000; k++) m.emplace(keyx(k, 0), 0u);
-        });
-        std::unordered_map<KeyX, uint32_t, KeyXHash> all;
-        bool overflow = false;
-        for (auto &m : local) {
-            if (m.size() > 70000) overflow = true;
-            for (auto &kv : m) {
-                all.emplace(kv.first, 0u);
-                all.emplace(neg(kv.first), 0u);
-            }
-        }
-        if (all.size() > 65535) overflow = true;
-        if (!overflow) {
-            std::vector<KeyX> keys;
-            keys.reserve(all.size());
-            for (auto &kv : all) keys.push_back(kv.first);
-            std::sort(keys.begin(), keys.end());
-            for (size_t q = 0; q < keys.size(); q++) all[keys[q]] = (uint32_t)q;
-            std::vector<uint32_t> negid(keys.size());
-            for (size_t q = 0; q < keys.size(); q++) negid[q] = all.find(neg(keys[q]))->second;
-            cid_j.resize(nB);
-            host_ranges(nB, HT, [&](int, int64_t lo, int64_t hi) {
-                for (int64_t k = lo; k < hi; k++) {
-                    const uint32_t id = all.find(keyx(k, 0))->second;
-                    bond_cid[k] = id;
-                    cid_j[k] = negid[id];
-                }
-            });
-            dict.resize(keys.size());
-            dictx.resize(2 * keys.size());
-            for (size_t q = 0; q < keys.size(); q++) {
-                double l0, vcf, bs;
-                std::memcpy(&l0, &keys[q].a, 8);
-                std::memcpy(&vcf, &keys[q].b, 8);
-                std::memcpy(&bs, &keys[q].c, 8);
-                dict[q] = make_entry(l0, vcf, bs);
-                float xf, yf, zf;
-                std::memcpy(&xf, &keys[q].x, 4);
-                std::memcpy(&yf, &keys[q].y, 4);
-                std::memcpy(&zf, &keys[q].z, 4);
-                const double c0 = ((double)xf * xf + (double)yf * yf + (double)zf * zf) - l0 * l0;
-                dictx[2 * q] = make_float4(xf, yf, zf, (float)l0);
-                dictx[2 * q + 1] = make_float4((float)(bs * prm->cell_volume * vcf), (float)c0,
-                                               dict[q].rl0 > 0 ? 1.f : 0.f, 0.f);
-            }
-            S->prec = kP32X;
-            S->ndict = (int64_t)dict.size();
-        }
-    }
-    phase.mark("fp32 dictionary");
-    if (S->prec != kP32X) {
-        const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
-        std::vector<std::unordered_map<Key3, uint32_t, Key3Hash>> local(HT);
-        host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
-            auto &m = local[t];
-            for (int64_t k = lo; k < hi; k++) {
-                Key3 key{bits_of(pb->undeformed_length[k]), bits_of(pb->volume_correction[k]), bits_of(pb->bond_stiffness[k])};
-                if (m.size() <= 70000) m.emplace(key, 0u);
-            }
-        });
-        std::vector<Key3> keys;
-        bool overflow = false;
-        {
-            std::unordered_map<Key3, uint32_t, Key3Hash> all;
-            for (auto &m : local) {
-                if (m.size() > 70000) overflow = true;
-                for (auto &kv : m) all.emplace(kv.first, 0u);
-            }
-            if (all.size() > 65535) overflow = true;
-            if (!overflow) {
-                keys.reserve(all.size());
-                for (auto &kv : all) keys.push_back(kv.first);
-            }
-        }
-        if (!overflow) {
-            std::sort(keys.begin(), keys.end());
-            std::unordered_map<Key3, uint32_t, Key3Hash> id;
-            for (size_t q = 0; q < keys.size(); q++) id.emplace(keys[q], (uint32_t)q);
-            host_ranges(nB, HT, [&](int, int64_t lo, int64_t hi) {
-                for (int64_t k = lo; k < hi; k++) {
-                    Key3 key{bits_of(pb->undeformed_length[k]), bits_of(pb->volume_correction[k]), bits_of(pb->bond_stiffness[k])};
-                    bond_cid[k] = id.find(key)->second;
-                }
-            });
-            dict.resize(keys.size());
-            for (size_t q = 0; q < keys.size(); q++) {
-                double l0, vcf, bs;
-                std::memcpy(&l0, &keys[q].a, 8);
-                std::memcpy(&vcf, &keys[q].b, 8);
-                std::memcpy(&bs, &keys[q].c, 8);
-                dict[q] = make_entry(l0, vcf, bs);
-            }
-        } else {
-            // irregular input: one dictionary entry per bond, 32-bit ids
-            S->wide = true;
-            dict.resize(nB);
-            for (int64_t k = 0; k < nB; k++) {
-                dict[k] = make_entry(pb->undeformed_length[k], pb->volume_correction[k], pb->bond_stiffness[k]);
-                bond_cid[k] = (uint32_t)k;
-            }
-        }
-        if (dict.empty()) dict.push_back(make_entry(1.0, 0.0, 0.0));
-        S->ndict = (int64_t)dict.size();
-    }
-
-    phase.mark("dictionary");
+    if (S->prec == kP32X) cid_j.resize(nB);
+    const int HT0 = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
+    host_ranges(nB, HT0, [&](int, int64_t lo, int64_t hi) {
+        fwd_ids(lo, hi - lo, bond_cid.data() + lo);
+        if (S->prec == kP32X)
+            for (int64_t k = lo; k < hi; k++) cid_j[k] = negid[bond_cid[k]];
+    });
     // per-node lists in bond order, laid out in 32-node slices. Stable
     // counting sort over HT contiguous bond ranges.
-    const int64_t ns = (nN + 31) / 32;
-    S->ns = ns;
     const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
     std::vector<std::vector<int32_t>> cnt(HT, std::vector<int32_t>(nN, 0));
     host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
@@ -2195,7 +2179,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         }
         tile_cap = (tile_cap + 31) & ~31;
         int optin = 0;
-        BBPD_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+        BBPD_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, S->device));
         const int ncache = (int)std::min<int64_t>(kDictCache, (int64_t)dict.size());
         const size_t smem = (size_t)32 * ncache + (size_t)24 * tile_cap;
         if (fits && smem <= (size_t)optin) {
@@ -2251,23 +2235,522 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     }
 
     phase.mark("tiles");
-    // node arrays in device order
-    auto perm3 = [&](const double *src, std::vector<double> &dst) {
-        dst.assign(3 * nN, 0.0);
-        if (src)
-            for (int c = 0; c < 3; c++)
-                for (int64_t p = 0; p < nN; p++) dst[p + c * nN] = src[S->perm[p] + c * nN];
+    Dev &d = S->d;
+    TRY(S->put((int64_t **)&d.slice_ptr, sptr));
+    TRY(S->put((int32_t **)&d.deg, deg));
+    TRY(S->put((int32_t **)&d.slice_len, slen));
+    if (S->tiled) {
+        TRY(S->put((uint16_t **)&d.jw, jw));
+        TRY(S->put((int64_t **)&d.halo_ptr, hptr));
+        TRY(S->put((uint32_t **)&d.halo, halo));
+    } else {
+        TRY(S->put((uint32_t **)&d.colw, colw.get(), (size_t)ne));
+    }
+    if (S->wide) TRY(S->put((uint32_t **)&d.cid, cid32.get(), (size_t)ne));
+    else TRY(S->put((uint16_t **)&d.cid, cid16.get(), (size_t)ne));
+    TRY(S->put(&d.st, st.get(), (size_t)ne));
+    TRY(S->alloc(&d.bsf, (size_t)ne));
+    BBPD_CUDA_TRY(cudaMemset(d.bsf, 0, sizeof(double) * std::max<int64_t>(ne, 1)));
+    if (pb->s0) TRY(S->put((double **)&d.s0e, s0e));
+    if (pb->s1) TRY(S->put((double **)&d.s1e, s1e));
+    if (pb->sc || S->wide) TRY(S->put((double **)&d.sce, sce));
+    return BBPD_OK;
+}
+
+// Device buffers that live only while the layout is built, released in
+// stream order (no device-wide synchronisation, so other solvers' launches
+// keep running while this one is built).
+struct TempBufs {
+    cudaStream_t st;
+    std::vector<void *> p;
+    explicit TempBufs(cudaStream_t s) : st(s) {}
+    template <class T>
+    int get(T **out, size_t count)
+    {
+        BBPD_CUDA_TRY(cudaMallocAsync((void **)out, sizeof(T) * std::max<size_t>(count, 1), st));
+        p.push_back((void *)*out);
+        return BBPD_OK;
+    }
+    ~TempBufs()
+    {
+        for (void *q : p) cudaFreeAsync(q, st);
+    }
+};
+
+inline int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+// Layout built on the device, for the input and Morton node orders. The host
+// converts the per-bond arrays while staging them (node ids to device
+// positions, dictionary ids, fail and BONDTYPE packed in a byte); the sort of
+// the directed entries by node, the slice shapes and the scatter into the entry
+// streams run as kernels, and the bond -> entry map is written on the way.
+template <class FwdIds>
+static int device_layout(bbpd_solver *S, const bbpd_problem *pb, const int32_t *inv, FwdIds fwd_ids,
+                         const std::vector<uint32_t> &negid, PhaseTimer &phase)
+{
+    const bbpd_params *prm = &S->prm;
+    const int64_t nN = S->nN, nB = S->nB, ns = S->ns, n2 = 2 * nB;
+    const double *bl = pb->bondlist;
+    cudaStream_t st = S->stream;
+    Dev &d = S->d;
+    TempBufs tmp(st);
+
+    // staged per-bond inputs
+    uint32_t *key = nullptr;
+    TRY(tmp.get(&key, (size_t)n2));
+    TRY(staging::upload(key, n2, st, [&](int64_t q0, int64_t cnt, uint32_t *out) {
+        for (int64_t i = 0; i < cnt; i++) {
+            const int64_t q = q0 + i;
+            out[i] = (uint32_t)inv[(int64_t)bl[(q & 1) * nB + (q >> 1)] - 1];
+        }
+    }));
+    LayoutArgs a{};
+    a.nB = nB;
+    a.T = prm->n_chunks;
+    a.key = key;
+    if (pb->fail || pb->bond_type) {
+        uint8_t *bflag = nullptr;
+        TRY(tmp.get(&bflag, (size_t)nB));
+        const double *fl = pb->fail, *bt = pb->bond_type;
+        TRY(staging::upload(bflag, nB, st, [&](int64_t k0, int64_t cnt, uint8_t *out) {
+            for (int64_t i = 0; i < cnt; i++) {
+                const int64_t k = k0 + i;
+                out[i] = (uint8_t)((fl && fl[k] == 0 ? 1 : 0) | (bt ? (int)bt[k] << 1 : 0));
+            }
+        }));
+        a.bflag = bflag;
+    }
+    if (!S->wide) {
+        uint16_t *bcid = nullptr;
+        TRY(tmp.get(&bcid, (size_t)nB));
+        TRY(staging::upload(bcid, nB, st, [&](int64_t k0, int64_t cnt, uint16_t *out) { fwd_ids(k0, cnt, out); }));
+        a.bcid = bcid;
+        if (S->prec == kP32X) {
+            uint16_t *ng = nullptr;
+            TRY(tmp.get(&ng, negid.size()));
+            TRY(staging::upload(ng, (int64_t)negid.size(), st, [&](int64_t k0, int64_t cnt, uint16_t *out) {
+                for (int64_t i = 0; i < cnt; i++) out[i] = (uint16_t)negid[k0 + i];
+            }));
+            a.negid = ng;
+        }
+    }
+    const double *lawp[3] = {pb->s0, pb->s1, pb->sc};
+    const double **lawd[3] = {&a.s0, &a.s1, &a.sc};
+    for (int m = 0; m < 3; m++)
+        if (lawp[m]) {
+            double *v = nullptr;
+            TRY(tmp.get(&v, (size_t)nB));
+            TRY(staging::upload_copy(v, lawp[m], nB, st));
+            *lawd[m] = v;
+        }
+    phase.mark("staged bonds");
+
+    // stable sort of the directed entries by node
+    uint32_t *skey = nullptr, *val = nullptr, *sval = nullptr;
+    TRY(tmp.get(&skey, (size_t)n2));
+    TRY(tmp.get(&val, (size_t)n2));
+    TRY(tmp.get(&sval, (size_t)n2));
+    int end_bit = 1;
+    while (end_bit < 32 && ((int64_t)1 << end_bit) < nN) end_bit++;
+    if (n2 > 0) {
+        k_iota<<<grid_for(n2), 256, 0, st>>>(val, n2);
+        BBPD_CUDA_TRY(cudaGetLastError());
+        size_t tb = 0;
+        BBPD_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, val, sval, n2, 0, end_bit, st));
+        void *tstore = nullptr;
+        TRY(tmp.get((uint8_t **)&tstore, tb));
+        BBPD_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tstore, tb, key, skey, val, sval, n2, 0, end_bit, st));
+    }
+
+    // degrees, slice shapes and offsets
+    uint32_t *first = nullptr, *last = nullptr;
+    int64_t *scount = nullptr;
+    TRY(tmp.get(&first, (size_t)nN));
+    TRY(tmp.get(&last, (size_t)nN));
+    TRY(tmp.get(&scount, (size_t)ns + 1));
+    BBPD_CUDA_TRY(cudaMemsetAsync(first, 0, sizeof(uint32_t) * nN, st));
+    BBPD_CUDA_TRY(cudaMemsetAsync(last, 0, sizeof(uint32_t) * nN, st));
+    if (n2 > 0) {
+        k_run_bounds<<<grid_for(n2), 256, 0, st>>>(skey, n2, first, last);
+        BBPD_CUDA_TRY(cudaGetLastError());
+    }
+    TRY(S->alloc((int32_t **)&d.deg, (size_t)nN));
+    TRY(S->alloc((int32_t **)&d.slice_len, (size_t)ns));
+    TRY(S->alloc((int64_t **)&d.slice_ptr, (size_t)ns + 1));
+    k_slice_lengths<<<grid_for(ns * 32), 256, 0, st>>>(first, last, nN, ns, (int32_t *)d.deg, (int32_t *)d.slice_len,
+                                                         scount);
+    BBPD_CUDA_TRY(cudaGetLastError());
+    {
+        size_t tb = 0;
+        BBPD_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, scount, (int64_t *)d.slice_ptr, ns + 1, st));
+        void *tstore = nullptr;
+        TRY(tmp.get((uint8_t **)&tstore, tb));
+        BBPD_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tstore, tb, scount, (int64_t *)d.slice_ptr, ns + 1, st));
+    }
+    int64_t ne = 0;
+    BBPD_CUDA_TRY(cudaMemcpyAsync(&ne, d.slice_ptr + ns, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(st));
+    S->ne = ne;
+    phase.mark("sort, slices");
+
+    // entry streams: padding slots stay zero (the critical stretch stream
+    // holds the law's sc there)
+    TRY(S->alloc((uint32_t **)&d.colw, (size_t)ne));
+    if (S->wide) TRY(S->alloc((uint32_t **)&d.cid, (size_t)ne));
+    else TRY(S->alloc((uint16_t **)&d.cid, (size_t)ne));
+    TRY(S->alloc(&d.st, (size_t)ne));
+    TRY(S->alloc(&d.bsf, (size_t)ne));
+    const size_t ne1 = (size_t)std::max<int64_t>(ne, 1);
+    BBPD_CUDA_TRY(cudaMemsetAsync((void *)d.colw, 0, 4 * ne1, st));
+    BBPD_CUDA_TRY(cudaMemsetAsync((void *)d.cid, 0, (S->wide ? 4 : 2) * ne1, st));
+    BBPD_CUDA_TRY(cudaMemsetAsync(d.st, 0, ne1, st));
+    BBPD_CUDA_TRY(cudaMemsetAsync(d.bsf, 0, 8 * ne1, st));
+    if (pb->s0) {
+        TRY(S->alloc((double **)&d.s0e, (size_t)ne));
+        BBPD_CUDA_TRY(cudaMemsetAsync((void *)d.s0e, 0, 8 * ne1, st));
+    }
+    if (pb->s1) {
+        TRY(S->alloc((double **)&d.s1e, (size_t)ne));
+        BBPD_CUDA_TRY(cudaMemsetAsync((void *)d.s1e, 0, 8 * ne1, st));
+    }
+    if (pb->sc || S->wide) {   // 32-bit-index instances always read a stream
+        TRY(S->alloc((double **)&d.sce, (size_t)ne));
+        k_fill<<<grid_for(ne), 256, 0, st>>>((double *)d.sce, ne, prm->sc);
+        BBPD_CUDA_TRY(cudaGetLastError());
+    }
+    S->ent32 = ne < ((int64_t)1 << 32);
+    if (S->ent32) TRY(S->alloc((uint32_t **)&S->d_ent, (size_t)n2));
+    else TRY(S->alloc((int64_t **)&S->d_ent, (size_t)n2));
+    phase.mark("entry streams");
+    if (n2 > 0) {
+        a.skey = skey;
+        a.sval = sval;
+        a.first = first;
+        a.sptr = d.slice_ptr;
+        a.colw = (uint32_t *)d.colw;
+        a.cid = (void *)d.cid;
+        a.st = d.st;
+        a.s0e = (double *)d.s0e;
+        a.s1e = (double *)d.s1e;
+        a.sce = (double *)d.sce;
+        a.ent = S->d_ent;
+        a.ent32 = S->ent32 ? 1 : 0;
+        k_layout_scatter<<<grid_for(n2), 256, 0, st>>>(a);
+        BBPD_CUDA_TRY(cudaGetLastError());
+    }
+    phase.mark("scatter");
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int device,
+                           bbpd_solver **out)
+{
+    clear_error();
+    if (!pb || !prm || !out) return fail(BBPD_ERR_ARG, "null argument");
+    *out = nullptr;
+    TRY(require_device());
+    PhaseTimer phase;
+    const int64_t nN = pb->n_nodes, nB = pb->n_bonds;
+    if (nN < 1 || nB < 0) return fail(BBPD_ERR_ARG, "n_nodes must be >= 1 and n_bonds >= 0");
+    if (nN >= MAX_NODES) return fail(BBPD_ERR_UNSUPPORTED, "at most %lld nodes per solver", (long long)MAX_NODES - 1);
+    if (nB >= ((int64_t)1 << 31)) return fail(BBPD_ERR_UNSUPPORTED, "at most 2^31 - 1 bonds per solver");
+    if (!pb->undeformed_coordinates || (nB && (!pb->bondlist || !pb->undeformed_length ||
+        !pb->bond_stiffness || !pb->volume_correction)))
+        return fail(BBPD_ERR_ARG, "missing coordinates or bond arrays");
+    if (prm->law < 0 || prm->law > 3 || prm->scheme < 0 || prm->scheme > 1 || prm->precision < 0 ||
+        prm->precision > 1 || prm->n_chunks < 1 || prm->n_chunks > 4096)
+        return fail(BBPD_ERR_ARG, "bad law/scheme/precision/n_chunks");
+    if (!(prm->failure_functionality == 0.0 || prm->failure_functionality == 1.0))
+        return fail(BBPD_ERR_UNSUPPORTED, "failure_functionality must be 0 or 1");
+    if (prm->scheme == BBPD_SCHEME_ADR && !pb->mass) return fail(BBPD_ERR_ARG, "ADR needs mass");
+    if (prm->scheme == BBPD_SCHEME_EULERCROMER && !pb->density) return fail(BBPD_ERR_ARG, "Euler-Cromer needs density");
+    if (prm->amplitude == BBPD_AMP_SMOOTHSTEP && prm->n_time_steps < 2)
+        return fail(BBPD_ERR_ARG, "smooth step needs n_time_steps >= 2");
+    TRY(validate_01(pb->fail, nB, "fail"));
+    TRY(validate_01(pb->constraint_flag, 3 * nN, "CONSTRAINTFLAG"));
+    TRY(validate_01(pb->prescribed_flag, 3 * nN, "prescribed flag"));
+    if (pb->bond_type) {
+        const double *bt = pb->bond_type;
+        const int64_t k = first_bad(nB, [&](int64_t q) { return !(bt[q] == 0 || bt[q] == 1 || bt[q] == 2); });
+        if (k >= 0) return fail(BBPD_ERR_ARG, "BONDTYPE[%lld] = %g", (long long)k, bt[k]);
+    }
+    if (pb->stretch_plastic) {
+        const double *sp = pb->stretch_plastic;
+        if (first_bad(nB, [&](int64_t q) { return sp[q] != 0; }) >= 0)
+            return fail(BBPD_ERR_UNSUPPORTED, "non-zero stretchPlastic (steel plasticity) is not on this path");
+    }
+    const double *bl = pb->bondlist;
+    {
+        const int64_t k = first_bad(nB, [&](int64_t q) {
+            const double a = bl[q], b = bl[nB + q];
+            return !(a >= 1 && b >= 1 && a <= (double)nN && b <= (double)nN && a == std::floor(a) &&
+                     b == std::floor(b) && a != b);
+        });
+        if (k >= 0)
+            return fail(BBPD_ERR_ARG, "BONDLIST row %lld = (%g, %g) is not a pair of distinct node ids", (long long)k + 1,
+                        bl[k], bl[nB + k]);
+    }
+
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(BBPD_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+    }
+    auto *S = new bbpd_solver;
+    std::unique_ptr<bbpd_solver> guard_(S);
+    S->device = device;
+    S->prm = *prm;
+    S->nN = nN;
+    S->nB = nB;
+    S->has_density = pb->density != nullptr;
+
+    phase.mark("validate");
+    // node order
+    S->perm.resize(nN);
+    S->inv.resize(nN);
+    std::iota(S->perm.begin(), S->perm.end(), 0);
+    if (prm->node_order == BBPD_ORDER_MORTON || prm->node_order == BBPD_ORDER_TILED) {
+        const double *X = pb->undeformed_coordinates;
+        double lo[3], hi[3];
+        for (int c = 0; c < 3; c++) {
+            lo[c] = *std::min_element(X + c * nN, X + (c + 1) * nN);
+            hi[c] = *std::max_element(X + c * nN, X + (c + 1) * nN);
+        }
+        // Quantize on the shortest bond length when that resolves the domain
+        // in 21 bits per axis: a regular lattice then maps to its integer
+        // indices and aligned Morton blocks are exact bricks (a 512-node tile
+        // is an 8 x 8 x 8 brick). Otherwise scale each axis to 21 bits.
+        double h = 0;
+        for (int64_t k = 0; k < nB; k++) {
+            const double l = pb->undeformed_length[k];
+            if (l > 0 && std::isfinite(l) && (h == 0 || l < h)) h = l;
+        }
+        bool lattice = h > 0;
+        for (int c = 0; c < 3 && lattice; c++) lattice = (hi[c] - lo[c]) / h < 2097000.0;
+        std::vector<uint64_t> key(nN);
+        for (int64_t i = 0; i < nN; i++) {
+            uint32_t q[3];
+            for (int c = 0; c < 3; c++) {
+                const double span = hi[c] - lo[c];
+                if (lattice) q[c] = (uint32_t)std::floor((X[i + c * nN] - lo[c]) / h + 0.5);
+                else q[c] = span > 0 ? (uint32_t)((X[i + c * nN] - lo[c]) / span * 2097151.0) : 0;
+            }
+            key[i] = morton3(q[0], q[1], q[2]);
+        }
+        std::stable_sort(S->perm.begin(), S->perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    }
+    for (int64_t p = 0; p < nN; p++) S->inv[S->perm[p]] = (int32_t)p;
+    const int32_t *inv = S->inv.data();
+
+    phase.mark("node order");
+    // Dictionary of the distinct bond constants. The FP32 form keys every
+    // directed entry by (L0, VCF, BONDSTIFFNESS, bond vector in FP32) and is
+    // kept when those keys fit 16-bit ids; otherwise the key is (L0, VCF,
+    // BONDSTIFFNESS), and irregular inputs whose keys do not fit 16 bits get one
+    // entry per bond (32-bit ids). Ids follow the sorted order of the keys'
+    // bits. One pass over the bonds: each host thread numbers the keys of its
+    // bond range in a local map and records every bond's local id; the local
+    // ids are remapped to dictionary ids while the bonds are laid out.
+    const double *X = pb->undeformed_coordinates;
+    auto keyx = [&](int64_t k) {   // forward copy: bond vector X[second] - X[first]
+        const int64_t a = (int64_t)bl[k] - 1, b = (int64_t)bl[nB + k] - 1;
+        const float fx = (float)(X[b] - X[a]), fy = (float)(X[b + nN] - X[a + nN]),
+                    fz = (float)(X[b + 2 * nN] - X[a + 2 * nN]);
+        return KeyX{bits_of(pb->undeformed_length[k]), bits_of(pb->volume_correction[k]),
+                    bits_of(pb->bond_stiffness[k]), fbits(fx), fbits(fy), fbits(fz)};
     };
-    auto perm1 = [&](const double *src, std::vector<double> &dst) {
-        dst.assign(nN, 0.0);
-        if (src)
-            for (int64_t p = 0; p < nN; p++) dst[p] = src[S->perm[p]];
+    auto key3 = [&](int64_t k) {
+        return Key3{bits_of(pb->undeformed_length[k]), bits_of(pb->volume_correction[k]),
+                    bits_of(pb->bond_stiffness[k])};
     };
-    std::vector<double> X3, mass, rho, u0(3 * nN, 0.0), x0(3 * nN, 0.0);
-    perm3(pb->undeformed_coordinates, X3);
-    perm1(pb->mass, mass);
-    perm1(pb->density, rho);
-    std::vector<uint8_t> nflag(nN, 0);
+    constexpr size_t kLocalMax = 65536;   // local ids are 16-bit; more keys overflow the dictionary anyway
+    const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
+    std::vector<int64_t> rhi(HT);         // bond range of host thread t: [rhi[t-1], rhi[t])
+    for (int t = 0; t < HT; t++) rhi[t] = nB * (t + 1) / HT;
+    std::unique_ptr<uint16_t[]> lid(new uint16_t[std::max<int64_t>(nB, 1)]);
+    std::vector<std::vector<uint32_t>> remap(HT);   // local id -> dictionary id, per thread
+    std::vector<uint32_t> negid;
+    std::vector<DictEntry> dict;
+    std::vector<float4> dictx;
+    // one pass: local maps and local ids; false when some thread overflowed
+    auto collect = [&](auto key, auto &local) {
+        std::vector<char> over(HT, 0);
+        host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
+            auto &m = local[t];
+            for (int64_t k = lo; k < hi; k++) {
+                const uint32_t v = m.insert(key(k), (uint32_t)m.count);
+                if (m.count > kLocalMax) {
+                    over[t] = 1;
+                    return;
+                }
+                lid[k] = (uint16_t)v;
+            }
+        });
+        for (char o : over)
+            if (o) return false;
+        return true;
+    };
+    S->prec = kP64;
+    if (prm->precision == BBPD_PREC_FP32) {
+        // The reverse copy's key is the forward key with the bond vector
+        // negated (IEEE subtraction is sign-symmetric; a +0 component stays
+        // +0), so only forward keys are collected and the reverse ids come from
+        // the negation of each dictionary key.
+        auto negx = [](uint32_t f) { return (f & 0x7FFFFFFFu) ? (f ^ 0x80000000u) : f; };
+        auto neg = [&](const KeyX &q) { return KeyX{q.a, q.b, q.c, negx(q.x), negx(q.y), negx(q.z)}; };
+        std::vector<FlatMap<KeyX, KeyXHash>> local(HT);
+        bool ok = collect(keyx, local);
+        FlatMap<KeyX, KeyXHash> idx;
+        for (int t = 0; t < HT && ok; t++) {
+            local[t].for_each([&](const KeyX &q, uint32_t) {
+                idx.insert(q, 0u);
+                idx.insert(neg(q), 0u);
+            });
+            ok = idx.count <= 65535;
+        }
+        if (ok) {
+            std::vector<KeyX> keys;
+            keys.reserve(idx.count);
+            idx.for_each([&](const KeyX &q, uint32_t) { keys.push_back(q); });
+            std::sort(keys.begin(), keys.end());
+            for (size_t q = 0; q < keys.size(); q++) idx.set(keys[q], (uint32_t)q);
+            for (int t = 0; t < HT; t++) {
+                remap[t].resize(local[t].count);
+                local[t].for_each([&](const KeyX &q, uint32_t v) { remap[t][v] = idx.find(q); });
+            }
+            negid.resize(keys.size());
+            for (size_t q = 0; q < keys.size(); q++) negid[q] = idx.find(neg(keys[q]));
+            dict.resize(keys.size());
+            dictx.resize(2 * keys.size());
+            for (size_t q = 0; q < keys.size(); q++) {
+                double l0, vcf, bs;
+                std::memcpy(&l0, &keys[q].a, 8);
+                std::memcpy(&vcf, &keys[q].b, 8);
+                std::memcpy(&bs, &keys[q].c, 8);
+                dict[q] = make_entry(l0, vcf, bs);
+                float xf, yf, zf;
+                std::memcpy(&xf, &keys[q].x, 4);
+                std::memcpy(&yf, &keys[q].y, 4);
+                std::memcpy(&zf, &keys[q].z, 4);
+                const double c0 = ((double)xf * xf + (double)yf * yf + (double)zf * zf) - l0 * l0;
+                dictx[2 * q] = make_float4(xf, yf, zf, (float)l0);
+                dictx[2 * q + 1] = make_float4((float)(bs * prm->cell_volume * vcf), (float)c0,
+                                               dict[q].rl0 > 0 ? 1.f : 0.f, 0.f);
+            }
+            S->prec = kP32X;
+        }
+    }
+    phase.mark("fp32 dictionary");
+    if (S->prec != kP32X) {
+        std::vector<FlatMap<Key3, Key3Hash>> local(HT);
+        bool ok = collect(key3, local);
+        FlatMap<Key3, Key3Hash> id3;
+        for (int t = 0; t < HT && ok; t++) {
+            local[t].for_each([&](const Key3 &q, uint32_t) { id3.insert(q, 0u); });
+            ok = id3.count <= 65535;
+        }
+        if (ok) {
+            std::vector<Key3> keys;
+            keys.reserve(id3.count);
+            id3.for_each([&](const Key3 &q, uint32_t) { keys.push_back(q); });
+            std::sort(keys.begin(), keys.end());
+            for (size_t q = 0; q < keys.size(); q++) id3.set(keys[q], (uint32_t)q);
+            for (int t = 0; t < HT; t++) {
+                remap[t].resize(local[t].count);
+                local[t].for_each([&](const Key3 &q, uint32_t v) { remap[t][v] = id3.find(q); });
+            }
+            dict.resize(keys.size());
+            for (size_t q = 0; q < keys.size(); q++) {
+                double l0, vcf, bs;
+                std::memcpy(&l0, &keys[q].a, 8);
+                std::memcpy(&vcf, &keys[q].b, 8);
+                std::memcpy(&bs, &keys[q].c, 8);
+                dict[q] = make_entry(l0, vcf, bs);
+            }
+        } else {
+            // irregular input: one dictionary entry per bond, 32-bit ids
+            S->wide = true;
+            lid.reset();
+            dict.resize(nB);
+            host_parallel_for(nB, [&](int64_t k) {
+                dict[k] = make_entry(pb->undeformed_length[k], pb->volume_correction[k], pb->bond_stiffness[k]);
+            });
+        }
+        if (dict.empty()) dict.push_back(make_entry(1.0, 0.0, 0.0));
+    }
+    S->ndict = (int64_t)dict.size();
+    // Dictionary ids of the copies of bond k in the list of its first node
+    // (the copy in its second node's list has negid[] of it in the FP32 form,
+    // the same id otherwise), for bonds k0 .. k0 + cnt - 1.
+    auto fwd_ids = [&](int64_t k0, int64_t cnt, auto *out) {
+        if (S->wide) {
+            for (int64_t i = 0; i < cnt; i++) out[i] = (uint32_t)(k0 + i);
+            return;
+        }
+        int t = (int)(std::upper_bound(rhi.begin(), rhi.end(), k0) - rhi.begin());
+        for (int64_t i = 0; i < cnt; i++) {
+            const int64_t k = k0 + i;
+            while (k >= rhi[t]) t++;
+            out[i] = remap[t][lid[k]];
+        }
+    };
+
+    phase.mark("dictionary");
+    const int64_t ns = (nN + 31) / 32;
+    S->ns = ns;
+    Dev &d = S->d;
+    d.n_nodes = nN;
+    d.n_slices = ns;
+    d.colw = nullptr;
+    d.jw = nullptr;
+    d.halo_ptr = nullptr;
+    d.halo = nullptr;
+    d.s0e = d.s1e = d.sce = nullptr;
+    BBPD_CUDA_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    if (prm->node_order == BBPD_ORDER_TILED) TRY(host_layout(S, pb, inv, fwd_ids, negid, dict, dictx, phase));
+    else TRY(device_layout(S, pb, inv, fwd_ids, negid, phase));
+    lid.reset();
+
+    // node arrays in device order, staged; the initial displacement and
+    // positions are formed on the device (k_node_init)
+    const int32_t *perm = S->perm.data();
+    bool identity = true;
+    for (int64_t p = 0; p < nN && identity; p++) identity = perm[p] == p;
+    auto stage_nodes = [&](double *dst, const double *src, int ncomp) -> int {
+        if (!src) {
+            BBPD_CUDA_TRY(cudaMemsetAsync(dst, 0, sizeof(double) * ncomp * nN, S->stream));
+            return BBPD_OK;
+        }
+        if (identity) return staging::upload_copy(dst, src, ncomp * nN, S->stream);
+        return staging::upload(dst, ncomp * nN, S->stream, [&](int64_t e0, int64_t cnt, double *out) {
+            int64_t c = e0 / nN, p = e0 - c * nN;
+            for (int64_t i = 0; i < cnt; i++) {
+                out[i] = src[perm[p] + c * nN];
+                if (++p == nN) p = 0, c++;
+            }
+        });
+    };
+    TRY(S->alloc((double **)&d.X, (size_t)(3 * nN)));
+    TRY(stage_nodes((double *)d.X, pb->undeformed_coordinates, 3));
+    TRY(S->alloc((double **)&d.mass, (size_t)nN));
+    TRY(stage_nodes((double *)d.mass, pb->mass, 1));
+    TRY(S->alloc((double **)&d.rho, (size_t)nN));
+    TRY(stage_nodes((double *)d.rho, pb->density, 1));
+    {
+        std::vector<uint8_t> nflag(nN);
+        host_parallel_for(nN, [&](int64_t p) {
+            const int64_t i = perm[p];
+            uint8_t f = 0;
+            for (int c = 0; c < 3; c++) {
+                const bool cf = pb->constraint_flag && pb->constraint_flag[i + c * nN] == 1;
+                const bool pf = pb->prescribed_flag && pb->prescribed_flag[i + c * nN] == 1;
+                if (cf || pf) f |= (uint8_t)(1 << c);
+                if (pf) f |= (uint8_t)(8 << c);
+            }
+            nflag[p] = f;
+        });
+        TRY(S->put((uint8_t **)&d.nflag, nflag));
+    }
+    phase.mark("node staging");
     double U1;
     if (prm->amplitude == BBPD_AMP_SMOOTHSTEP) {
         // prescribed value at step 1, same arithmetic as the device
@@ -2276,76 +2759,38 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     } else {
         U1 = prm->rate * 1.0;
     }
-    for (int64_t p = 0; p < nN; p++) {
-        int64_t i = S->perm[p];
-        uint8_t f = 0;
-        for (int c = 0; c < 3; c++) {
-            bool cf = pb->constraint_flag && pb->constraint_flag[i + c * nN] == 1;
-            bool pf = pb->prescribed_flag && pb->prescribed_flag[i + c * nN] == 1;
-            if (cf || pf) f |= (uint8_t)(1 << c);
-            if (pf) { f |= (uint8_t)(8 << c); u0[p + c * nN] = U1; }
-            x0[p + c * nN] = X3[p + c * nN] + u0[p + c * nN];
-        }
-        nflag[p] = f;
+    const size_t b3 = sizeof(double) * 3 * (size_t)nN;
+    TRY(S->alloc(&d.xb0, (size_t)(3 * nN)));
+    TRY(S->alloc(&d.xb1, (size_t)(3 * nN)));
+    TRY(S->alloc(&d.u, (size_t)(3 * nN)));
+    TRY(S->alloc(&d.v, (size_t)(3 * nN)));
+    TRY(S->alloc(&d.F0, (size_t)(3 * nN)));
+    TRY(S->alloc(&d.F1, (size_t)(3 * nN)));
+    BBPD_CUDA_TRY(cudaMemsetAsync(d.v, 0, b3, S->stream));
+    BBPD_CUDA_TRY(cudaMemsetAsync(d.F0, 0, b3, S->stream));
+    BBPD_CUDA_TRY(cudaMemsetAsync(d.F1, 0, b3, S->stream));
+    d.a = nullptr;
+    if (prm->scheme == BBPD_SCHEME_EULERCROMER) {
+        TRY(S->alloc(&d.a, (size_t)(3 * nN)));
+        BBPD_CUDA_TRY(cudaMemsetAsync(d.a, 0, b3, S->stream));
     }
-
-    phase.mark("node arrays");
-    // device buffers
-    Dev &d = S->d;
-    d.n_nodes = nN;
-    d.n_slices = ns;
-    TRY(S->put((int64_t **)&d.slice_ptr, sptr));
-    TRY(S->put((int32_t **)&d.deg, deg));
-    TRY(S->put((int32_t **)&d.slice_len, slen));
-    d.colw = nullptr;
-    d.jw = nullptr;
-    d.halo_ptr = nullptr;
-    d.halo = nullptr;
-    if (S->tiled) {
-        TRY(S->put((uint16_t **)&d.jw, jw));
-        TRY(S->put((int64_t **)&d.halo_ptr, hptr));
-        TRY(S->put((uint32_t **)&d.halo, halo));
-    } else {
-        TRY(S->put((uint32_t **)&d.colw, colw.get(), (size_t)ne));
-    }
-    colw.reset();
-    std::vector<uint16_t>().swap(jw);
-    if (S->wide) TRY(S->put((uint32_t **)&d.cid, cid32.get(), (size_t)ne));
-    else TRY(S->put((uint16_t **)&d.cid, cid16.get(), (size_t)ne));
-    TRY(S->put(&d.st, st.get(), (size_t)ne));
-    TRY(S->alloc(&d.bsf, (size_t)ne));
-    BBPD_CUDA_TRY(cudaMemset(d.bsf, 0, sizeof(double) * std::max<int64_t>(ne, 1)));
-    TRY(S->put((DictEntry **)&d.dict, dict));
-    d.dictx = nullptr;
     d.urh0 = d.urh1 = nullptr;
     d.url0 = d.url1 = nullptr;
     if (S->prec == kP32X) {
-        TRY(S->put((float4 **)&d.dictx, dictx));
-        std::vector<float4> uh;
-        std::vector<float2> ul;
-        split_record(u0.data(), nN, uh, ul);
-        TRY(S->put(&d.urh0, uh));
-        TRY(S->put(&d.urh1, uh));
-        TRY(S->put(&d.url0, ul));
-        TRY(S->put(&d.url1, ul));
+        TRY(S->alloc(&d.urh0, (size_t)nN));
+        TRY(S->alloc(&d.urh1, (size_t)nN));
+        TRY(S->alloc(&d.url0, (size_t)nN));
+        TRY(S->alloc(&d.url1, (size_t)nN));
     }
-    d.s0e = d.s1e = d.sce = nullptr;
-    if (pb->s0) TRY(S->put((double **)&d.s0e, s0e));
-    if (pb->s1) TRY(S->put((double **)&d.s1e, s1e));
-    if (pb->sc || S->wide) TRY(S->put((double **)&d.sce, sce));
-    TRY(S->put((double **)&d.X, X3));
-    TRY(S->put(&d.xb0, x0));
-    TRY(S->put(&d.xb1, x0));
-    TRY(S->put(&d.u, u0));
-    std::vector<double> zeros3(3 * nN, 0.0);
-    TRY(S->put(&d.v, zeros3));
-    TRY(S->put(&d.F0, zeros3));
-    TRY(S->put(&d.F1, zeros3));
-    d.a = nullptr;
-    if (prm->scheme == BBPD_SCHEME_EULERCROMER) TRY(S->put(&d.a, zeros3));
-    TRY(S->put((double **)&d.mass, mass));
-    TRY(S->put((double **)&d.rho, rho));
-    TRY(S->put((uint8_t **)&d.nflag, nflag));
+    TRY(S->alloc(&d.sticky, 1));
+    BBPD_CUDA_TRY(cudaMemsetAsync(d.sticky, 0, sizeof(unsigned), S->stream));
+    k_node_init<<<grid_for(nN), 256, 0, S->stream>>>(d, U1);
+    BBPD_CUDA_TRY(cudaGetLastError());
+    phase.mark("node arrays");
+
+    TRY(S->put((DictEntry **)&d.dict, dict));
+    d.dictx = nullptr;
+    if (S->prec == kP32X) TRY(S->put((float4 **)&d.dictx, dictx));
     {
         // levels of the reduction tree: level 1 has one value per slice,
         // level L+1 one per group of 32 values of level L
@@ -2384,10 +2829,6 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     TRY(S->put(&d.work, work));
     std::vector<int> err(1, 0);
     TRY(S->put(&d.err, err));
-    std::vector<unsigned> sticky(1, 0u);
-    for (int64_t e = 0; e < 3 * nN; e++)
-        if (!coord_safe(x0[e])) sticky[0] = 1u;
-    TRY(S->put(&d.sticky, sticky));
 
     phase.mark("uploads");
     // scalars
@@ -2429,7 +2870,6 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     if (occ < 1) return fail(BBPD_ERR_CUDA, "kernel cannot be resident");
     int64_t want = (ns * 32 + kBlock - 1) / kBlock;   // one warp per slice at most
     S->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * occ, want));
-    BBPD_CUDA_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
     BBPD_CUDA_TRY(cudaEventCreate(&S->ev0));
     BBPD_CUDA_TRY(cudaEventCreate(&S->ev1));
 
@@ -2443,9 +2883,11 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
                           : (24 + 4 + 24 * 3 + 8 + 1 /*x v u X rho flag*/ + 24 * 5 /*F a v u x w*/);
         S->bytes_per_step = 2.0 * (double)nB * per_entry + (double)nN * node;
     }
-    // the uploads above ran on the legacy default stream; wait for them only,
-    // not for other solvers' launches on their own streams
+    // the layout and staged copies ran on this solver's stream, the small
+    // uploads on the legacy default stream; wait for those only, not for
+    // other solvers' launches on their own streams
     phase.mark("kernel setup");
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
     BBPD_CUDA_TRY(cudaStreamSynchronize(0));
     *out = guard_.release();
     return BBPD_OK;
@@ -2574,11 +3016,14 @@ extern "C" int bbpd_get(bbpd_solver *S, int field, double *out)
     double *src = field_ptr(S, field, nodal);
     if (nodal) {
         if (!src) return fail(BBPD_ERR_ARG, "field %d not held by this scheme", field);
-        std::vector<double> h(3 * nN);
-        BBPD_CUDA_TRY(cudaMemcpy(h.data(), src, sizeof(double) * 3 * nN, cudaMemcpyDeviceToHost));
-        for (int c = 0; c < 3; c++)
-            for (int64_t p = 0; p < nN; p++) out[S->perm[p] + c * nN] = h[p + c * nN];
-        return BBPD_OK;
+        const int32_t *perm = S->perm.data();
+        return staging::download(src, 3 * nN, S->stream, [&](int64_t e0, int64_t cnt, const double *in) {
+            int64_t c = e0 / nN, p = e0 - c * nN;
+            for (int64_t i = 0; i < cnt; i++) {
+                out[perm[p] + c * nN] = in[i];
+                if (++p == nN) p = 0, c++;
+            }
+        });
     }
     if (field != BBPD_FIELD_BSF && field != BBPD_FIELD_FLAG && field != BBPD_FIELD_FAIL)
         return fail(BBPD_ERR_ARG, "unknown field %d", field);
@@ -2592,15 +3037,14 @@ extern "C" int bbpd_get(bbpd_solver *S, int field, double *out)
             k_bond_gather_bits<uint32_t><<<blocks, 256, 0, S->stream>>>((const uint32_t *)S->d_ent, nB, S->d.st, field, tb);
         else
             k_bond_gather_bits<int64_t><<<blocks, 256, 0, S->stream>>>((const int64_t *)S->d_ent, nB, S->d.st, field, tb);
-        std::unique_ptr<uint8_t[]> hb(new uint8_t[nB]);
         cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpyAsync(hb.get(), tb, (size_t)nB, cudaMemcpyDeviceToHost, S->stream);
+        int rc = e == cudaSuccess ? BBPD_OK : fail(BBPD_ERR_CUDA, "get field %d: %s", field, cudaGetErrorString(e));
+        if (rc == BBPD_OK)
+            rc = staging::download(tb, nB, S->stream, [&](int64_t k0, int64_t cnt, const uint8_t *in) {
+                for (int64_t i = 0; i < cnt; i++) out[k0 + i] = (double)in[i];
+            });
         cudaFreeAsync(tb, S->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
-        if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "get field %d: %s", field, cudaGetErrorString(e));
-        const uint8_t *b = hb.get();
-        host_parallel_for(nB, [&](int64_t k) { out[k] = (double)b[k]; });
-        return BBPD_OK;
+        return rc;
     }
     double *tmp = nullptr;
     BBPD_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(double) * (size_t)nB, S->stream));
@@ -2609,11 +3053,10 @@ extern "C" int bbpd_get(bbpd_solver *S, int field, double *out)
     else
         k_bond_gather<int64_t><<<blocks, 256, 0, S->stream>>>((const int64_t *)S->d_ent, nB, S->d.bsf, S->d.st, field, tmp);
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, sizeof(double) * (size_t)nB, cudaMemcpyDeviceToHost, S->stream);
+    int rc = e == cudaSuccess ? BBPD_OK : fail(BBPD_ERR_CUDA, "get field %d: %s", field, cudaGetErrorString(e));
+    if (rc == BBPD_OK) rc = staging::download_copy(out, tmp, nB, S->stream);
     cudaFreeAsync(tmp, S->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
-    if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "get field %d: %s", field, cudaGetErrorString(e));
-    return BBPD_OK;
+    return rc;
 }
 
 extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
@@ -2660,9 +3103,14 @@ extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
     TRY(upload_entry_map(S));
     double *tmp = nullptr;
     BBPD_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(double) * (size_t)nB, S->stream));
-    cudaError_t e = cudaMemcpyAsync(tmp, in, sizeof(double) * (size_t)nB, cudaMemcpyHostToDevice, S->stream);
+    const int rc = staging::upload_copy(tmp, in, nB, S->stream);
+    if (rc) {
+        cudaFreeAsync(tmp, S->stream);
+        return rc;
+    }
+    cudaError_t e = cudaSuccess;
     const int blocks = (int)std::min<int64_t>((nB + 255) / 256, 148 * 32);
-    if (e == cudaSuccess) {
+    {
         if (S->ent32)
             k_bond_scatter<uint32_t><<<blocks, 256, 0, S->stream>>>((const uint32_t *)S->d_ent, nB, tmp, field, S->d.bsf, S->d.st);
         else

@@ -433,10 +433,13 @@ def main():
             dist.barrier()
         t0 = time.perf_counter()
         s2 = bb.Solver(inp, device=dev, **kw)
+        t1 = time.perf_counter()
         s2.step(args.steps)
+        t2 = time.perf_counter()
         outs = [s2.get(f) for f in ("displacement", "force", "bsf", "flag", "fail")]
         torch.cuda.synchronize()
         te = time.perf_counter() - t0
+        parts = {"create_s": t1 - t0, "steps_s": t2 - t1, "download_s": te - (t2 - t0)}
         s2.close()
         te = max_over_ranks(te, dist, "cuda")
         h2d = sum(inp[k].nbytes for k in ("undeformedCoordinates", "BONDLIST", "UNDEFORMEDLENGTH",
@@ -445,7 +448,8 @@ def main():
         d2h = sum(o.nbytes for o in outs)
         e2e = {"value": replica_rate(nB, args.steps, world, te), "unit": unit,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "seconds": te, "includes": "upload of the reference arrays, layout build, K steps, download of state"}
+               "seconds": te, **{k: round(v, 4) for k, v in parts.items()},
+               "includes": "upload of the reference arrays, layout build, K steps, download of state"}
 
     if rank != 0:
         if dist:

@@ -169,6 +169,43 @@ def test_morton_order_identical(small):
         assert same(a.get(f), b.get(f)), f
 
 
+@pytest.fixture(scope="module")
+def medium():
+    """40 000 nodes, 2.4M bonds: the bond arrays cross the host-device boundary
+    in several staged chunks per host thread, and the device-built layout (input
+    and Morton orders) meets the host-built one (tiled order) at scale."""
+    return bb.beam.build(bb.beam.small(nx=100, ny=20, nz=20))
+
+
+@pytest.mark.parametrize("law", ["trilinear", "exponential"])
+def test_layouts_identical_at_scale(medium, law):
+    nB = medium["nBonds"]
+    rng = np.random.default_rng(11)
+    inp = dict(medium)
+    inp["fail"] = (rng.random(nB) > 0.02).astype(np.float64)        # 2 % of the bonds start broken
+    if law == "exponential":
+        inp["BONDTYPE"] = rng.integers(0, 3, nB).astype(np.float64)
+    kw = dict(LAWKW[law], scheme="adr", rate=-2e-6)
+    runs = [bb.Solver(inp, node_order=o, **kw) for o in ("input", "morton", "tiled")]
+    for s in runs:
+        s.step(40)
+    for f in NODAL + BOND:
+        ref = runs[0].get(f)
+        for s in runs[1:]:
+            assert same(ref, s.get(f)), f
+    assert np.array_equal(runs[0].get("fail"), np.where(inp["fail"] == 0, 0.0, runs[0].get("fail")))
+    # per-bond fields round-trip through the staged copies
+    v = rng.random(nB)
+    v[rng.random(nB) < 0.5] = 0.0
+    runs[1].set("bsf", v)
+    assert same(runs[1].get("bsf"), v)
+    flags = (rng.random(nB) < 0.3).astype(np.float64)
+    runs[2].set("flag", flags)
+    assert same(runs[2].get("flag"), flags)
+    for s in runs:
+        s.close()
+
+
 def test_split_launches_identical(small):
     kw = dict(LAWKW["bilinear"], scheme="adr", rate=-2e-6)
     a, b = bb.Solver(small, **kw), bb.Solver(small, **kw)
