@@ -8,11 +8,12 @@ This package is the host-side mirror of the reference's MATLAB calls:
     Batch      many solvers stepped by one persistent launch (batching form)
     serving    continuous batching of beam solves under an HBM budget
     beam       synthetic beams like the reference's input scripts
+    builder    the reference's input module (horizons, notch, bond data) on the GPU
 """
-from . import _native, beam, routines, serving
+from . import _native, beam, builder, routines, serving
 from ._native import BBPDError, device_count
 from .batch import Batch
 from .solver import Solver, make_params
 
-__all__ = ["Solver", "Batch", "make_params", "beam", "routines", "serving", "BBPDError", "device_count",
+__all__ = ["Solver", "Batch", "make_params", "beam", "builder", "routines", "serving", "BBPDError", "device_count",
            "_native"]

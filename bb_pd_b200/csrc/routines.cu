@@ -15,6 +15,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <cmath>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -281,6 +282,26 @@ __global__ void k_damage_final(const double *__restrict__ nfam, int64_t nN, doub
     damage[i] = 1 - (damage[i] / nfam[i]);
 }
 
+// calculatedamageenergy.m:34-62: energy dissipated by each bond, never
+// decreasing. shape = 2k - 2e^k + alpha k - alpha k e^k + 2 and den =
+// 2k (e^k - 1)(1 + alpha) are formed once on the host; every product keeps the
+// reference's left-to-right order.
+__global__ void k_damageenergy(const double *__restrict__ BS, const double *__restrict__ s0,
+                               const double *__restrict__ sc, const double *__restrict__ L0,
+                               const double *__restrict__ stretch, double shape, double den, double V2,
+                               double *energy, int64_t nB)
+{
+    GRID_STRIDE(k, nB)
+    {
+        const double s = stretch[k], a = s0[k], c = sc[k];
+        double de = 0.0;
+        if ((a < s) && (s <= c)) de = (((((BS[k] * a) * L0[k]) * (a - s)) * shape) / den) * V2;
+        else if (s > c) de = (((((BS[k] * a) * L0[k]) * (a - c)) * shape) / den) * V2;
+        const double e = energy[k];
+        energy[k] = isnan(e) ? de : (de > e ? de : e);   // MATLAB's max ignores NaN
+    }
+}
+
 // ---- nodal force plan ----
 
 __global__ void k_plan_keys(const double *__restrict__ bl, int64_t nB, int64_t nN,
@@ -450,6 +471,22 @@ extern "C" int bbpd_dev_calculatedamage(const double *bl, const double *fail_, c
     if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "damage: %s", cudaGetErrorString(e));
     if (h) return fail(BBPD_ERR_ARG, "BONDLIST holds node ids outside [1, nNodes]");
     return BBPD_OK;
+}
+
+extern "C" int bbpd_dev_calculatedamageenergy(const double *BS, const double *s0, const double *sc,
+        const double *L0, const double *stretch, double k, double alpha, double cellVolume,
+        double *damageEnergy, int64_t nB, void *stream)
+{
+    if (nB < 0) return fail(BBPD_ERR_ARG, "negative size");
+    if (nB == 0) return BBPD_OK;
+    int rc = require_device();
+    if (rc) return rc;
+    const double ek = std::exp(k);
+    const double den = 2 * k * (ek - 1) * (1 + alpha);
+    const double shape = (2 * k) - (2 * ek) + (alpha * k) - (alpha * k * ek) + 2;
+    k_damageenergy<<<blocks_for(nB), kThreads, 0, as_stream(stream)>>>(BS, s0, sc, L0, stretch, shape, den,
+                                                                        cellVolume * cellVolume, damageEnergy, nB);
+    return launch_check();
 }
 
 extern "C" int bbpd_dev_calculatebondforces(double *fX, double *fY, double *fZ,
@@ -771,6 +808,22 @@ extern "C" int bbpd_calculatedamage(const double *bl, const double *fail_, const
     TRY(bbpd_dev_calculatedamage(dbl, dfa, dnf, nB, nN, ddm, nullptr));
     TRY(finish());
     TRY(download(damage, ddm, n));
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_calculatedamageenergy(const double *BS, const double *s0, const double *sc,
+        const double *L0, const double *stretch, double k, double alpha, double cellVolume,
+        double *damageEnergy, int64_t nB)
+{
+    TRY(require_device());
+    std::lock_guard<std::mutex> lk(g_mu);
+    const size_t b = sizeof(double) * (size_t)nB;
+    double *dBS, *ds0, *dsc, *dL, *ds, *dE;
+    MIRROR_IN(BS, b, dBS); MIRROR_IN(s0, b, ds0); MIRROR_IN(sc, b, dsc); MIRROR_IN(L0, b, dL);
+    MIRROR_IN(stretch, b, ds); MIRROR_IN(damageEnergy, b, dE);
+    TRY(bbpd_dev_calculatedamageenergy(dBS, ds0, dsc, dL, ds, k, alpha, cellVolume, dE, nB, nullptr));
+    TRY(finish());
+    TRY(download(damageEnergy, dE, b));
     return BBPD_OK;
 }
 

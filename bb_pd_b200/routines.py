@@ -47,6 +47,7 @@ def _sig():
     L.bbpd_calculatedampingcoefficient.argtypes = [p, p, p, d, p, p, i64, p]
     L.bbpd_timeintegrationADR.argtypes = [i64, d, p, p, p, d, p, p, p, i64]
     L.bbpd_calculatedamage.argtypes = [p, p, p, i64, i64, p]
+    L.bbpd_calculatedamageenergy.argtypes = [p, p, p, p, p, d, d, d, p, i64]
     return L
 
 
@@ -195,3 +196,14 @@ def timeintegrationADR(iTimeStep, DT, nodalVelocityForwardHalf, nodalForce, mass
         _arr(nodalDisplacement, "nodalDisplacement", True), _arr(CONSTRAINTFLAG, "CONSTRAINTFLAG"),
         _rows(nodalForce)))
     return nodalDisplacement, nodalVelocityForwardHalf
+
+
+def calculatedamageenergy(BONDSTIFFNESS, s0, sc, UNDEFORMEDLENGTH, stretch, k, alpha, cellVolume,
+                          damageEnergy) -> np.ndarray:
+    """calculatedamageenergy.m:1 on the GPU: the energy dissipated by every bond,
+    never decreasing (damageEnergy updated in place and returned)."""
+    N.check(_lib().bbpd_calculatedamageenergy(
+        _arr(BONDSTIFFNESS, "BONDSTIFFNESS"), _arr(s0, "s0"), _arr(sc, "sc"),
+        _arr(UNDEFORMEDLENGTH, "UNDEFORMEDLENGTH"), _arr(stretch, "stretch"), float(k), float(alpha),
+        float(cellVolume), _arr(damageEnergy, "damageEnergy", True), _rows(damageEnergy)))
+    return damageEnergy

@@ -207,6 +207,99 @@ int bbpd_dev_calculatedamage(const double *bondlist, const double *fail,
 int bbpd_calculatedamage(const double *bondlist, const double *fail,
         const double *nFAMILYMEMBERS, int64_t nBonds, int64_t nNodes, double *damage);
 
+/* replaces calculatedamageenergy.m:1 (energy dissipated by every bond,
+ * :34-62): for s0 < stretch <= sc the bond's energy is BONDSTIFFNESS s0
+ * UNDEFORMEDLENGTH (s0 - stretch) shape / den cellVolume^2, above sc the same
+ * with sc in place of the stretch, else 0, with shape = 2k - 2e^k + alpha k -
+ * alpha k e^k + 2 and den = 2k (e^k - 1)(1 + alpha); damageEnergy keeps the
+ * larger of its value and this one (damageEnergy in place, nBonds entries).
+ * The drivers pass k = 25, alpha = 0.25
+ * (dynamicsolverdisplacementcontrolled.m:121). */
+int bbpd_dev_calculatedamageenergy(const double *BONDSTIFFNESS, const double *s0,
+        const double *sc, const double *UNDEFORMEDLENGTH, const double *stretch,
+        double k, double alpha, double cellVolume, double *damageEnergy,
+        int64_t nBonds, void *stream);
+int bbpd_calculatedamageenergy(const double *BONDSTIFFNESS, const double *s0,
+        const double *sc, const double *UNDEFORMEDLENGTH, const double *stretch,
+        double k, double alpha, double cellVolume, double *damageEnergy, int64_t nBonds);
+
+/* ---- input builder (the reference's input module, on the GPU) ----
+ * Host-pointer calls copy their inputs to the device and their outputs back;
+ * the bbpd_dev_ forms take device pointers and a stream (NULL: the default
+ * stream) and return once their results are complete. Arrays follow the
+ * reference's layouts: column-major, node ids 1-based doubles. */
+
+/* replaces buildhorizons.m:1 (families and bond list, :13-97). Node j is in
+ * node i's family when sqrt(((xi-xj)^2 + (yi-yj)^2) + (zi-zj)^2) <= horizon,
+ * j != i (found with a cell list instead of rangesearch; families are listed
+ * by ascending node id, rangesearch lists them by distance). BONDLIST rows are
+ * (i, j) with i < j, by i then j; UNDEFORMEDLENGTH is the same square root.
+ * *nBonds always receives the bond count; nFAMILYMEMBERS and
+ * NODEFAMILYPOINTERS (nNodes entries, 1-based) are written when not NULL;
+ * BONDLIST (nBonds x 2), UNDEFORMEDLENGTH and NODEFAMILY (2 nBonds entries) are
+ * written when capacity >= nBonds (call with capacity 0 to size them). */
+int bbpd_buildhorizons(const double *undeformedCoordinates, int64_t nNodes,
+        double horizonRadius, int64_t capacity, int64_t *nBonds,
+        double *nFAMILYMEMBERS, double *NODEFAMILYPOINTERS, double *NODEFAMILY,
+        double *BONDLIST, double *UNDEFORMEDLENGTH);
+int bbpd_dev_buildhorizons(const double *undeformedCoordinates, int64_t nNodes,
+        double horizonRadius, int64_t capacity, int64_t *nBonds,
+        double *nFAMILYMEMBERS, double *NODEFAMILYPOINTERS, double *NODEFAMILY,
+        double *BONDLIST, double *UNDEFORMEDLENGTH, void *stream);
+
+/* replaces buildnotch.m:1 (:13-119 with determineintersection.m:59-150): the
+ * bonds whose segment meets the rectangle x = xlocation DX, y from the least
+ * to the largest y coordinate, z from the least z coordinate to depth DX are
+ * removed; the kept rows keep their order. *nBondsOut receives their count;
+ * BONDLISTout (written nBondsOut x 2, room for nBonds x 2), UNDEFORMEDLENGTHout
+ * (room for nBonds), nFAMILYMEMBERS and NODEFAMILYPOINTERS (nNodes) and
+ * NODEFAMILY (room for 2 nBonds; every family in bond order of the reduced
+ * list) may each be NULL. */
+int bbpd_buildnotch(const double *undeformedCoordinates, int64_t nNodes,
+        const double *BONDLIST, const double *UNDEFORMEDLENGTH, int64_t nBonds,
+        double DX, double xlocation, double depth, int64_t *nBondsOut,
+        double *BONDLISTout, double *UNDEFORMEDLENGTHout, double *nFAMILYMEMBERS,
+        double *NODEFAMILYPOINTERS, double *NODEFAMILY);
+int bbpd_dev_buildnotch(const double *undeformedCoordinates, int64_t nNodes,
+        const double *BONDLIST, const double *UNDEFORMEDLENGTH, int64_t nBonds,
+        double DX, double xlocation, double depth, int64_t *nBondsOut,
+        double *BONDLISTout, double *UNDEFORMEDLENGTHout, double *nFAMILYMEMBERS,
+        double *NODEFAMILYPOINTERS, double *NODEFAMILY, void *stream);
+
+/* replaces calculatevolumecorrectionfactors.m:1 (:16-34): 1 for L <= horizon -
+ * RADIJ, (horizon + RADIJ - L) / (2 RADIJ) up to the horizon, else 0. */
+int bbpd_calculatevolumecorrectionfactors(const double *UNDEFORMEDLENGTH,
+        int64_t nBonds, double horizon, double RADIJ, double *VOLUMECORRECTIONFACTORS);
+int bbpd_dev_calculatevolumecorrectionfactors(const double *UNDEFORMEDLENGTH,
+        int64_t nBonds, double horizon, double RADIJ, double *VOLUMECORRECTIONFACTORS,
+        void *stream);
+
+/* replaces buildbonddata.m:1 (:16-71): BONDTYPE 0 concrete-concrete, 1
+ * concrete-steel (either way), 2 steel-steel from MATERIALFLAG (NULL: all
+ * concrete; values other than 0 or 1 are rejected); stiffeningFactor =
+ * 2 neighbourhoodVolume / (nFAM_i cellVolume + nFAM_j cellVolume);
+ * BONDSTIFFNESS = stiffeningFactor x the concrete or steel constant;
+ * BFMULTIPLIER 3 for BONDTYPE 1, else 1. BONDTYPE, BFMULTIPLIER and
+ * stiffeningFactor may be NULL. The reference's VOLUMECORRECTIONFACTORS
+ * argument is unused there and absent here. */
+int bbpd_buildbonddata(const double *BONDLIST, int64_t nBonds, int64_t nNodes,
+        const double *nFAMILYMEMBERS, const double *MATERIALFLAG,
+        double bondStiffnessConcrete, double bondStiffnessSteel, double cellVolume,
+        double neighbourhoodVolume, double *BONDSTIFFNESS, double *BONDTYPE,
+        double *BFMULTIPLIER, double *stiffeningFactor);
+int bbpd_dev_buildbonddata(const double *BONDLIST, int64_t nBonds, int64_t nNodes,
+        const double *nFAMILYMEMBERS, const double *MATERIALFLAG,
+        double bondStiffnessConcrete, double bondStiffnessSteel, double cellVolume,
+        double neighbourhoodVolume, double *BONDSTIFFNESS, double *BONDTYPE,
+        double *BFMULTIPLIER, double *stiffeningFactor, void *stream);
+
+/* replaces buildmassmatrix.m:1 (:32-40): the ADR mass of every node,
+ * 0.25 DT^2 (nFAM DX^2)(bondStiffnessConcrete / DX). */
+int bbpd_buildmassmatrix(int64_t nNodes, double DX, double bondStiffnessConcrete,
+        double DT, const double *nFAMILYMEMBERS, double *massVector);
+int bbpd_dev_buildmassmatrix(int64_t nNodes, double DX, double bondStiffnessConcrete,
+        double DT, const double *nFAMILYMEMBERS, double *massVector, void *stream);
+
 /* Free the device mirrors and cached plan of the host-pointer entry points
  * (the gateways register it with mexAtExit). */
 int bbpd_release_mirrors(void);

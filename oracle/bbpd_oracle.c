@@ -342,6 +342,29 @@ void orc_damage(const double *bl, const double *fail, const double *nFamily,
     for (int64_t i = 0; i < nNodes; i++) damage[i] = 1 - (damage[i] / nFamily[i]);
 }
 
+void orc_damageenergy(const double *BS, const double *s0, const double *sc, const double *L0,
+                      const double *stretch, double k, double alpha, double cellVolume,
+                      double *damageEnergy, int64_t nBonds)
+{
+    const double denominator = 2 * k * (exp(k) - 1) * (1 + alpha);                         /* :36 */
+    const double shape = (2 * k) - (2 * exp(k)) + (alpha * k) - (alpha * k * exp(k)) + 2;  /* :47, :54 */
+    const double V2 = cellVolume * cellVolume;
+    for (int64_t b = 0; b < nBonds; b++) {
+        const double s = stretch[b];
+        double de = 0.0;
+        if ((s0[b] < s) && (s <= sc[b])) {                                                  /* :43 */
+            const double numerator = BS[b] * s0[b] * L0[b] * (s0[b] - s) * shape;
+            de = (numerator / denominator) * V2;
+        } else if (s > sc[b]) {                                                             /* :50 */
+            const double numerator = BS[b] * s0[b] * L0[b] * (s0[b] - sc[b]) * shape;
+            de = (numerator / denominator) * V2;
+        }
+        /* :61 max(damageEnergy, de), NaN entries ignored as MATLAB's max does */
+        const double e = damageEnergy[b];
+        damageEnergy[b] = (e != e) ? de : ((de > e) ? de : e);
+    }
+}
+
 /* calculatecontactforce.m:29-80 (literal: distances from the positions at
  * entry, then the nodes inside the radius in family order). */
 double orc_contact(const orc_penetrator *pen, double *cz, const double *X,
@@ -611,4 +634,184 @@ void orc_run(const orc_problem *p, orc_state *st, const orc_kernels *k,
         st->step = n + 1;
     }
     free(CFe);
+}
+
+/* ---- input builder ---- */
+
+int64_t orc_buildhorizons(const double *X, int64_t nNodes, double horizon, int64_t capacity,
+                          double *nFamily, double *famPtr, double *family, double *bl,
+                          double *L0)
+{
+    const int64_t n = nNodes;
+    int64_t nb = 0, nf = 0;
+    for (int64_t i = 0; i < n; i++) {
+        int64_t c = 0;
+        for (int64_t j = 0; j < n; j++) {
+            if (j == i) continue;
+            const double e0 = X[i] - X[j], e1 = X[i + n] - X[j + n], e2 = X[i + 2 * n] - X[j + 2 * n];
+            if (sqrt(e0 * e0 + e1 * e1 + e2 * e2) <= horizon) {
+                c++;
+                if (j > i) nb++;
+            }
+        }
+        if (nFamily) nFamily[i] = (double)c;
+        if (famPtr) famPtr[i] = (double)(nf + 1);     /* buildhorizons.m:36-44 */
+        nf += c;
+    }
+    if (capacity < nb) return nb;
+    int64_t k = 0, f = 0;
+    for (int64_t i = 0; i < n; i++)
+        for (int64_t j = 0; j < n; j++) {
+            if (j == i) continue;
+            const double e0 = X[i] - X[j], e1 = X[i + n] - X[j + n], e2 = X[i + 2 * n] - X[j + 2 * n];
+            const double L = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+            if (L > horizon) continue;
+            if (family) family[f++] = (double)(j + 1);
+            if (j > i) {                                /* :64-76 */
+                bl[k] = (double)(i + 1);
+                bl[k + nb] = (double)(j + 1);
+                L0[k] = L;                              /* :88-97 */
+                k++;
+            }
+        }
+    return nb;
+}
+
+void orc_volumecorrection(const double *L0, int64_t nBonds, double horizon, double radij,
+                          double *VCF)
+{
+    for (int64_t k = 0; k < nBonds; k++) {
+        const double UL = L0[k];
+        if (UL <= (horizon - radij)) VCF[k] = 1;                                   /* :23-25 */
+        else if ((UL > (horizon - radij)) && (UL <= horizon)) VCF[k] = (horizon + radij - UL) / (2 * radij);
+        else VCF[k] = 0;
+    }
+}
+
+int orc_bonddata(const double *bl, int64_t nBonds, const double *nFamily,
+                 const double *materialFlag, double bsConcrete, double bsSteel,
+                 double cellVolume, double neighbourhoodVolume, double *BS, double *BT,
+                 double *BFM, double *stiffening)
+{
+    for (int64_t k = 0; k < nBonds; k++) {
+        const int64_t i = (int64_t)bl[k] - 1, j = (int64_t)bl[nBonds + k] - 1;
+        const double mi = materialFlag ? materialFlag[i] : 0.0, mj = materialFlag ? materialFlag[j] : 0.0;
+        double bst;
+        if (mi == 0 && mj == 0) { bst = bsConcrete; BT[k] = 0; }                 /* :33-38 */
+        else if (mi == 0 && mj == 1) { bst = bsConcrete; BT[k] = 1; }            /* :40-45 */
+        else if (mi == 1 && mj == 0) { bst = bsConcrete; BT[k] = 1; }            /* :47-52 */
+        else if (mi == 1 && mj == 1) { bst = bsSteel; BT[k] = 2; }               /* :54-59 */
+        else return -1;
+        const double vi = nFamily[i] * cellVolume, vj = nFamily[j] * cellVolume;    /* :62-63 */
+        const double sf = (2 * neighbourhoodVolume) / ((vi + vj));                /* :64 */
+        if (stiffening) stiffening[k] = sf;
+        BS[k] = sf * bst;                                                          /* :65 */
+        BFM[k] = BT[k] == 1 ? 3 : 1;                                               /* :70-71 */
+    }
+    return 0;
+}
+
+void orc_massmatrix(int64_t nNodes, double dx, double bsConcrete, double dt,
+                    const double *nFamily, double *mass)
+{
+    for (int64_t i = 0; i < nNodes; i++) {
+        const double Kij = (nFamily[i] * (dx * dx)) * (bsConcrete / dx);              /* :36 */
+        mass[i] = 0.25 * (dt * dt) * Kij;                                          /* :37-38 */
+    }
+}
+
+static double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+static void cross3(const double *a, const double *b, double *c)
+{
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* determineintersection.m:59-86 with plane_line_intersect :126-150 */
+static int notch_hit(const double *A, const double *B, const double *D, const double *nrm,
+                     const double *P0, const double *P1)
+{
+    double AB[3], AD[3], u[3], w[3], I[3];
+    for (int c = 0; c < 3; c++) {
+        AB[c] = B[c] - A[c];
+        AD[c] = D[c] - A[c];
+        u[c] = P1[c] - P0[c];
+        w[c] = P0[c] - A[c];
+    }
+    const double Dn = dot3(nrm, u), N = -dot3(nrm, w);
+    if (fabs(Dn) < 1e-7) return 0;                 /* parallel: check 2 or 0, no hit */
+    const double sI = N / Dn;
+    for (int c = 0; c < 3; c++) I[c] = P0[c] + (sI * u[c]);
+    if (sI < 0 || sI > 1) return 0;                /* check 3 */
+    return (dot3(A, AB) <= dot3(I, AB)) && (dot3(I, AB) <= dot3(B, AB)) && (dot3(A, AD) <= dot3(I, AD)) &&
+           (dot3(I, AD) <= dot3(D, AD));
+}
+
+int64_t orc_buildnotch(const double *X, int64_t nNodes, const double *bl, const double *L0,
+                       int64_t nBonds, double DX, double xlocation, double depth,
+                       double *blOut, double *L0Out, double *nFamily, double *famPtr,
+                       double *family)
+{
+    const int64_t n = nNodes;
+    double lo[3], hi[3];
+    for (int c = 0; c < 3; c++) {
+        lo[c] = hi[c] = X[c * n];
+        for (int64_t i = 1; i < n; i++) {
+            const double v = X[i + c * n];
+            if (v < lo[c]) lo[c] = v;
+            if (v > hi[c]) hi[c] = v;
+        }
+    }
+    const double A[3] = {xlocation * DX, lo[1], lo[2]}, B[3] = {xlocation * DX, hi[1], lo[2]};   /* :52-55 */
+    const double D[3] = {xlocation * DX, lo[1], depth * DX};
+    double AB[3], AD[3], cr[3], nrm[3];
+    for (int c = 0; c < 3; c++) {
+        AB[c] = B[c] - A[c];
+        AD[c] = D[c] - A[c];
+    }
+    cross3(AB, AD, cr);
+    const double len = sqrt(dot3(cr, cr));
+    for (int c = 0; c < 3; c++) nrm[c] = cr[c] / len;
+    char *keep = (char *)malloc((size_t)(nBonds > 0 ? nBonds : 1));
+    int64_t m = 0;
+    for (int64_t k = 0; k < nBonds; k++) {
+        const int64_t i = (int64_t)bl[k] - 1, j = (int64_t)bl[nBonds + k] - 1;
+        const double P0[3] = {X[i], X[i + n], X[i + 2 * n]}, P1[3] = {X[j], X[j + n], X[j + 2 * n]};
+        keep[k] = !notch_hit(A, B, D, nrm, P0, P1);
+        m += keep[k];
+    }
+    int64_t r = 0;
+    for (int64_t k = 0; k < nBonds; k++)
+        if (keep[k]) {
+            blOut[r] = bl[k];
+            blOut[r + m] = bl[nBonds + k];
+            L0Out[r] = L0[k];
+            r++;
+        }
+    free(keep);
+    /* :90-119 families from the reduced list, in bond order */
+    for (int64_t i = 0; i < n; i++) nFamily[i] = 0;
+    for (int64_t k = 0; k < m; k++) {
+        nFamily[(int64_t)blOut[k] - 1] += 1;
+        nFamily[(int64_t)blOut[k + m] - 1] += 1;
+    }
+    double acc = 1;
+    for (int64_t i = 0; i < n; i++) {
+        famPtr[i] = acc;
+        acc += nFamily[i];
+    }
+    if (family) {
+        double *cnt = (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+        for (int64_t k = 0; k < m; k++) {
+            const int64_t i = (int64_t)blOut[k] - 1, j = (int64_t)blOut[k + m] - 1;
+            family[(int64_t)(famPtr[i] + cnt[i]) - 1] = (double)(j + 1);
+            family[(int64_t)(famPtr[j] + cnt[j]) - 1] = (double)(i + 1);
+            cnt[i] += 1;
+            cnt[j] += 1;
+        }
+        free(cnt);
+    }
+    return m;
 }

@@ -121,6 +121,49 @@ void orc_adr_integrate(int64_t iTimeStep, double dt, double *vh, const double *F
 void orc_damage(const double *bl, const double *fail, const double *nFamily,
                 int64_t nBonds, int64_t nNodes, double *damage);
 
+/* calculatedamageenergy.m:34-62 (energy dissipated by every bond, never
+ * decreasing; k and alpha as the drivers pass them, 25 and 0.25). */
+void orc_damageenergy(const double *BS, const double *s0, const double *sc, const double *L0,
+                      const double *stretch, double k, double alpha, double cellVolume,
+                      double *damageEnergy, int64_t nBonds);
+
+/* ---- input builder (the reference's input module) ---- */
+
+/* buildhorizons.m:13-97 by brute force: node j is in node i's family when
+ * sqrt(((xi - xj)^2 + (yi - yj)^2) + (zi - zj)^2) <= horizon, j != i. Families
+ * are listed by ascending node id (the reference's rangesearch lists them by
+ * distance); BONDLIST rows (i, j), i < j, by i then j, 1-based doubles.
+ * Returns nBonds; the arrays are written when capacity >= nBonds
+ * (NODEFAMILY then needs 2 nBonds entries). */
+int64_t orc_buildhorizons(const double *X, int64_t nNodes, double horizon, int64_t capacity,
+                          double *nFamily, double *famPtr, double *family, double *bl,
+                          double *L0);
+
+/* calculatevolumecorrectionfactors.m:16-34 */
+void orc_volumecorrection(const double *L0, int64_t nBonds, double horizon, double radij,
+                          double *VCF);
+
+/* buildbonddata.m:16-66 (materialFlag null: every node concrete). Returns 0,
+ * or -1 when a material flag is neither 0 nor 1. */
+int orc_bonddata(const double *bl, int64_t nBonds, const double *nFamily,
+                 const double *materialFlag, double bsConcrete, double bsSteel,
+                 double cellVolume, double neighbourhoodVolume, double *BS, double *BT,
+                 double *BFM, double *stiffening);
+
+/* buildmassmatrix.m:32-40 */
+void orc_massmatrix(int64_t nNodes, double dx, double bsConcrete, double dt,
+                    const double *nFamily, double *mass);
+
+/* buildnotch.m:13-119 with determineintersection.m:59-150: bonds whose segment
+ * meets the rectangle x = xlocation DX, y in [min y, max y], z in [min z,
+ * depth DX] are removed, families rebuilt from the reduced list. Writes the
+ * kept rows (col-major with leading dimension = the returned count) and
+ * returns the number kept. */
+int64_t orc_buildnotch(const double *X, int64_t nNodes, const double *bl, const double *L0,
+                       int64_t nBonds, double DX, double xlocation, double depth,
+                       double *blOut, double *L0Out, double *nFamily, double *famPtr,
+                       double *family);
+
 /* smoothstepdata.m:40-42 */
 double orc_smoothstep(double t, double t0, double t1, double v0, double v1);
 

@@ -92,6 +92,16 @@ def lib() -> C.CDLL:
         L.orc_bsf_bilinear.argtypes = [_P, _P, C.c_int, _P, C.c_int, _P, _P, _P, C.c_int64]
         L.orc_bondfailure.argtypes = [_P, C.c_double, _P, _P, _P, C.c_int, C.c_double, C.c_int64]
         L.orc_damage.argtypes = [_P, _P, _P, C.c_int64, C.c_int64, _P]
+        L.orc_buildhorizons.argtypes = [_P, C.c_int64, C.c_double, C.c_int64, _P, _P, _P, _P, _P]
+        L.orc_buildhorizons.restype = C.c_int64
+        L.orc_volumecorrection.argtypes = [_P, C.c_int64, C.c_double, C.c_double, _P]
+        L.orc_bonddata.argtypes = [_P, C.c_int64, _P, _P, C.c_double, C.c_double, C.c_double, C.c_double,
+                                   _P, _P, _P, _P]
+        L.orc_massmatrix.argtypes = [C.c_int64, C.c_double, C.c_double, C.c_double, _P, _P]
+        L.orc_buildnotch.argtypes = [_P, C.c_int64, _P, _P, C.c_int64, C.c_double, C.c_double, C.c_double,
+                                     _P, _P, _P, _P, _P]
+        L.orc_buildnotch.restype = C.c_int64
+        L.orc_damageenergy.argtypes = [_P, _P, _P, _P, _P, C.c_double, C.c_double, C.c_double, _P, C.c_int64]
         L.orc_bondforces.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_double, _P, _P, C.c_int64]
         L.orc_nodalforces_chunked.argtypes = [C.c_int64, C.c_int64, _P, _P, _P, _P, _P, C.c_int]
         L.orc_eulercromer.argtypes = [_P, _P, C.c_double, _P, _P, _P, C.c_double, _P, _P, _P, C.c_int64, C.c_int]

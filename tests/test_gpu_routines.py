@@ -218,3 +218,24 @@ def test_damage_vs_oracle():
     with pytest.raises(bb.BBPDError) as e:
         R.calculatedamage(bad, fail, nfam)
     assert e.value.status == bb._native.ERR_ARG
+
+
+def test_damageenergy_vs_oracle():
+    """calculatedamageenergy.m on the GPU, bit for bit with the oracle over
+    stretches on both sides of s0 and sc (and on them), over repeated steps."""
+    rng = np.random.default_rng(9)
+    n = 200_003
+    bs = rng.uniform(1e18, 4e18, n)
+    L0 = rng.uniform(1e-3, 4e-3, n)
+    s0 = np.full(n, 1e-4)
+    sc = np.exp(rng.normal(np.log(2e-3), 0.1, n))
+    e_gpu, e_orc = np.zeros(n), np.zeros(n)
+    for step in range(4):
+        st = rng.uniform(-1e-3, 4e-3, n)
+        st[:1000] = s0[:1000]
+        st[1000:2000] = sc[1000:2000]
+        st[2000:2100] = np.nan
+        R.calculatedamageenergy(bs, s0, sc, L0, st, 25, 0.25, 1.5625e-8, e_gpu)
+        po.lib().orc_damageenergy(P(bs), P(s0), P(sc), P(L0), P(st), 25.0, 0.25, 1.5625e-8, P(e_orc), n)
+        assert same(e_gpu, e_orc), step
+    assert (e_gpu > 0).mean() > 0.5

@@ -322,3 +322,115 @@ def test_damage_known_answers():
     dmg = np.zeros(4)
     po.lib().orc_damage(po.P(bl), po.P(fail), po.P(nfam), 4, 4, po.P(dmg))
     assert list(dmg) == [0.5, 0.0, 1 - 2 / 3, 0.5]
+
+
+def _energy_formula(bs, s0, sc, L0, s, k, alpha, V):
+    """calculatedamageenergy.m:36-55 for one bond, written out again."""
+    den = 2 * k * (np.exp(k) - 1) * (1 + alpha)
+    shape = (2 * k) - (2 * np.exp(k)) + (alpha * k) - (alpha * k * np.exp(k)) + 2
+    if s0 < s <= sc:
+        return (bs * s0 * L0 * (s0 - s) * shape / den) * V ** 2
+    if s > sc:
+        return (bs * s0 * L0 * (s0 - sc) * shape / den) * V ** 2
+    return 0.0
+
+
+def test_damageenergy_known_answers():
+    """calculatedamageenergy.m:34-62: nothing below s0, growing with the
+    stretch in the softening range, the value at sc above it, and never
+    lower than the energy already dissipated (unloading keeps it; a NaN
+    stretch adds nothing)."""
+    k, alpha, V = 25.0, 0.25, 1.25e-7
+    s0, sc = 1e-4, 2e-3
+    s = np.array([0.0, 1e-4, 1.5e-4, 1e-3, 2e-3, 5e-3, np.nan])
+    n = s.size
+    bs, L0 = np.full(n, 3.1e18), np.full(n, 2.5e-3)
+    S0, SC = np.full(n, s0), np.full(n, sc)
+    e = np.zeros(n)
+    po.lib().orc_damageenergy(po.P(bs), po.P(S0), po.P(SC), po.P(L0), po.P(s), k, alpha, V, po.P(e), n)
+    want = [_energy_formula(bs[0], s0, sc, L0[0], x, k, alpha, V) for x in s]
+    np.testing.assert_allclose(e, want, rtol=1e-14, atol=0)
+    assert e[0] == 0 and e[1] == 0 and e[6] == 0
+    assert 0 < e[2] < e[3] < e[4] and e[4] == e[5]
+    # unloading: a smaller stretch leaves the dissipated energy unchanged
+    before = e.copy()
+    s2 = np.full(n, 1.2e-4)
+    po.lib().orc_damageenergy(po.P(bs), po.P(S0), po.P(SC), po.P(L0), po.P(s2), k, alpha, V, po.P(e), n)
+    assert np.array_equal(e[:6], np.maximum(before[:6], e[:6])) and np.array_equal(e[3:6], before[3:6])
+    assert e[0] > 0 and e[0] == e[1] == e[6]
+
+
+def _builder_case(**kw):
+    from bb_pd_b200 import beam
+    return beam.build(beam.small(nx=12, ny=4, nz=5, **kw))
+
+
+def test_builder_oracle_matches_lattice_builder():
+    """The brute-force restatement of buildhorizons.m, the volume correction,
+    buildbonddata.m and buildmassmatrix.m gives the lattice builder's arrays
+    bit for bit (both list families by node id)."""
+    inp = _builder_case()
+    X, n, nb = inp["undeformedCoordinates"], inp["nNodes"], inp["nBonds"]
+    L = po.lib()
+    fam, fptr = np.zeros(n), np.zeros(n)
+    assert L.orc_buildhorizons(po.P(X), n, inp["horizon"], 0, po.P(fam), po.P(fptr), None, None, None) == nb
+    bl, L0, family = np.zeros((nb, 2), order="F"), np.zeros(nb), np.zeros(2 * nb)
+    assert L.orc_buildhorizons(po.P(X), n, inp["horizon"], nb, po.P(fam), po.P(fptr), po.P(family),
+                               po.P(bl), po.P(L0)) == nb
+    assert np.array_equal(bl, inp["BONDLIST"]) and np.array_equal(L0, inp["UNDEFORMEDLENGTH"])
+    assert np.array_equal(fam, inp["nFAMILYMEMBERS"])
+    assert fptr[0] == 1 and np.array_equal(np.diff(fptr), fam[:-1])
+    for i in (0, n // 2, n - 1):                  # families by ascending node id, bonds both ways
+        f = family[int(fptr[i]) - 1:int(fptr[i] + fam[i]) - 1]
+        assert np.all(np.diff(f) > 0)
+        mine = np.concatenate([bl[bl[:, 0] == i + 1, 1], bl[bl[:, 1] == i + 1, 0]])
+        assert np.array_equal(np.sort(mine), f)
+    vcf = np.zeros(nb)
+    L.orc_volumecorrection(po.P(L0), nb, inp["horizon"], 5e-3 / 2, po.P(vcf))
+    assert np.array_equal(vcf, inp["VOLUMECORRECTIONFACTORS"])
+    VH = (4.0 / 3.0) * np.pi * inp["horizon"] ** 3
+    bs, bt, bfm, sf = (np.zeros(nb) for _ in range(4))
+    assert L.orc_bonddata(po.P(bl), nb, po.P(fam), None, inp["bondStiffnessConcrete"], 0.0, inp["cellVolume"],
+                          VH, po.P(bs), po.P(bt), po.P(bfm), po.P(sf)) == 0
+    assert np.array_equal(bs, inp["BONDSTIFFNESS"]) and not bt.any() and np.all(bfm == 1)
+    mass = np.zeros(n)
+    L.orc_massmatrix(n, 5e-3, inp["bondStiffnessConcrete"], inp["DT"], po.P(fam), po.P(mass))
+    assert np.array_equal(mass, inp["massVector"])
+
+
+def test_builder_oracle_bond_types_and_notch():
+    """buildbonddata.m's material table (concrete, interface x3, steel) and
+    buildnotch.m's removal of the bonds crossing the notch rectangle, checked
+    against the lattice builder's notch and a direct segment test."""
+    L = po.lib()
+    inp = _builder_case()
+    X, n, nb, bl = inp["undeformedCoordinates"], inp["nNodes"], inp["nBonds"], inp["BONDLIST"]
+    fam = inp["nFAMILYMEMBERS"]
+    mat = (X[:, 2] > 0.016).astype(np.float64)
+    bs, bt, bfm, sf = (np.zeros(nb) for _ in range(4))
+    assert L.orc_bonddata(po.P(bl), nb, po.P(fam), po.P(mat), 2.0, 7.0, 1.0, 1.0, po.P(bs), po.P(bt),
+                          po.P(bfm), po.P(sf)) == 0
+    mi, mj = mat[bl[:, 0].astype(int) - 1], mat[bl[:, 1].astype(int) - 1]
+    assert np.array_equal(bt, mi + mj) and np.array_equal(bfm, np.where(bt == 1, 3.0, 1.0))
+    assert np.array_equal(bs, sf * np.where(bt == 2, 7.0, 2.0))
+    bad = mat.copy()
+    bad[3] = 0.5
+    assert L.orc_bonddata(po.P(bl), nb, po.P(fam), po.P(bad), 2.0, 7.0, 1.0, 1.0, po.P(bs), po.P(bt),
+                          po.P(bfm), po.P(sf)) == -1
+    # notch at x = 6.5 dx, 2.3 dx deep: the lattice builder's rectangle runs
+    # from the bottom node layer (z = dx) to dx/2 + depth
+    dx = 5e-3
+    notched = _builder_case(notch_x=6.5 * dx, notch_depth=1.8 * dx)
+    blo, L0o = np.zeros((nb, 2), order="F"), np.zeros(nb)
+    famo, fptr, family = np.zeros(n), np.zeros(n), np.zeros(2 * nb)
+    m = L.orc_buildnotch(po.P(X), n, po.P(bl), po.P(inp["UNDEFORMEDLENGTH"]), nb, dx, 6.5, 2.3,
+                         po.P(blo), po.P(L0o), po.P(famo), po.P(fptr), po.P(family))
+    assert m == notched["nBonds"] < nb
+    assert np.array_equal(blo.ravel(order="F")[:2 * m], notched["BONDLIST"].ravel(order="F"))
+    assert np.array_equal(L0o[:m], notched["UNDEFORMEDLENGTH"])
+    assert np.array_equal(famo, notched["nFAMILYMEMBERS"])
+    i0 = int(np.argmax(famo))                       # family of a node in bond order of the reduced list
+    f = family[int(fptr[i0]) - 1:int(fptr[i0] + famo[i0]) - 1]
+    blm = np.asfortranarray(blo.ravel(order="F")[:2 * m].reshape((m, 2), order="F"))
+    want = [b if a == i0 + 1 else a for a, b in blm if a == i0 + 1 or b == i0 + 1]
+    assert list(f) == want
