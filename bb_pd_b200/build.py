@@ -27,7 +27,7 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CUDA_SOURCES = ["common.cu", "routines.cu", "solver.cu", "selftest.cu", "damping_noalloc.cu", "builder.cu",
-                "beam.cpp"]
+                "static.cu", "beam.cpp"]
 
 # Gateways: (output name, gateway macro). Names are the reference MEX files.
 GATEWAYS = [

@@ -367,6 +367,41 @@ typedef struct bbpd_problem {
     const double *prescribed_flag;        /* nNodes x 3 in {0,1}, or NULL */
 } bbpd_problem;
 
+/* ---- static (implicit) solver ----
+ * replaces the displacement-controlled Newton-Raphson of
+ * solvers/scripts/static/newtonraphsondisplacementcontrolled.m:56-160 with its
+ * tangent from buildstiffnessmatrixCSCformat.m (NOD = 3). Each step moves the
+ * prescribed DOFs (prescribed_flag) by `increment`; supports
+ * (constraint_flag) stay; then Newton iterations update every bond
+ * (calculatedeformedlength, the law of params.law with params.s0/s1/sc,
+ * calculatebondfailure with params.sc and params.sc_steel), form the bond
+ * forces of calculatebondforces.m (BFMULTIPLIER from BONDTYPE: 3 for type 1)
+ * and their nodal sum in bond order times cellVolume, and move the free nodes
+ * by the solution of K delta = F. K is the sum over intact bonds of
+ * BFM (BS / L^3) VCF cellVolume^2 (1 - BSF) [c c^T, -c c^T; -c c^T, c c^T].
+ * The linear solves are a block-Jacobi preconditioned conjugate gradient to a
+ * relative residual of cg_tol (the reference calls MATLAB's bicgstabl and
+ * lsqr). A step ends when ||F on free DOFs|| <= tol ||F on held DOFs|| (the
+ * reference uses 0.5 % of the net internal force), or after max_newton
+ * solves with stats->converged = 0. Per-bond s0/s1/sc arrays are rejected. */
+typedef struct bbpd_static bbpd_static;
+typedef struct bbpd_static_stats {
+    int32_t newton_iterations;   /* linear solves of the step */
+    int32_t cg_iterations;       /* conjugate-gradient iterations, all solves */
+    double residual;             /* ||nodal force on free DOFs|| at the end */
+    double reaction;             /* ||nodal force on held DOFs|| at the end */
+    int32_t converged;           /* 1 when residual <= tol * reaction */
+    int32_t reserved;
+} bbpd_static_stats;
+int bbpd_static_create(const bbpd_problem *problem, const bbpd_params *params, int device,
+        bbpd_static **out);
+int bbpd_static_step(bbpd_static *solver, double increment, double tol, int max_newton,
+        double cg_tol, int max_cg, bbpd_static_stats *stats);
+/* BBPD_FIELD_DISPLACEMENT, _DEFORMED, _FORCE (nodal force times cellVolume,
+ * as the driver forms it), _BSF, _FLAG, _FAIL */
+int bbpd_static_get(bbpd_static *solver, int field, double *out);
+int bbpd_static_destroy(bbpd_static *solver);
+
 typedef struct bbpd_solver bbpd_solver;
 
 /* Validate, lay out (per-node bond lists in bond order, sliced by 32 nodes)
