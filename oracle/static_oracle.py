@@ -60,7 +60,7 @@ class StaticOracle:
             f[(self.BT == 0) & (s > self.s0)] = 1
             with np.errstate(divide="ignore", invalid="ignore"):
                 bs = ((s - self.s0) / s) * (self.sc / (self.sc - self.s0))
-            cand = bs * f
+                cand = bs * f
             B = np.where(np.isnan(cand), B, np.where(np.isnan(B), cand, np.where(cand > B, cand, B)))
             B = np.where(B > 1, 1.0, B)
             B = np.where(np.isnan(B), 0.0, B)
