@@ -741,3 +741,272 @@ extern "C" int bbpd_static_destroy(bbpd_static *S)
     delete S;
     return BBPD_OK;
 }
+
+// ---- buildstiffnessmatrixCSCformat.m as a routine ----
+
+namespace {
+
+struct CooBonds {
+    const double *X;            // nodal coordinates, nNodes x NOD
+    const double *bl, *VCF, *BS, *BFM, *fail, *BSF;
+    int64_t n, nB;
+    int NOD;
+    double V;
+};
+
+// Local stiffness of bond k: its scale rig and bond vector (NOD components);
+// false for a failed bond (buildstiffnessmatrixCSCformat.m:72, :110).
+__device__ __forceinline__ bool coo_local(const CooBonds &q, int64_t k, double &rig, double c[3], int64_t &i,
+                                          int64_t &j)
+{
+    if (q.fail[k] != 1) return false;
+    i = (int64_t)q.bl[k] - 1;
+    j = (int64_t)q.bl[q.nB + k] - 1;
+    double L2 = 0;
+    for (int u = 0; u < q.NOD; u++) {
+        c[u] = q.X[j + u * q.n] - q.X[i + u * q.n];
+        L2 = u == 0 ? c[u] * c[u] : L2 + c[u] * c[u];
+    }
+    const double L = sqrt(L2);
+    if (q.NOD == 3)   // :116
+        rig = q.BFM[k] * ((q.BS[k] / (L * L * L)) * q.VCF[k] * (q.V * q.V)) * (1 - q.BSF[k]);
+    else              // :78
+        rig = q.BFM[k] * (q.BS[k] / (L * L * L)) * q.VCF[k] * (q.V * q.V);
+    return true;
+}
+
+// entry (r, s) of the 2 NOD x 2 NOD local matrix rig [A -A; -A A], A = c c^T
+__device__ __forceinline__ double coo_entry(double rig, const double *c, int NOD, int r, int s)
+{
+    const double m = c[r % NOD] * c[s % NOD];
+    return ((r < NOD) == (s < NOD)) ? rig * m : rig * (-m);
+}
+
+// nonzero count and norm(Klocal) of every bond; norm = 2 |rig| |c|^2, the
+// largest singular value of rig [A -A; -A A]
+__global__ void k_coo_count(CooBonds q, int64_t *cnt, double *nrm)
+{
+    GRID_STRIDE(k, q.nB + 1)
+    {
+        if (k == q.nB) {
+            cnt[k] = 0;
+            continue;
+        }
+        double rig, c[3];
+        int64_t i, j;
+        int64_t z = 0;
+        double nm = 0;
+        if (coo_local(q, k, rig, c, i, j)) {
+            const int D = 2 * q.NOD;
+            for (int s = 0; s < D; s++)
+                for (int r = 0; r < D; r++) z += coo_entry(rig, c, q.NOD, r, s) != 0;
+            double L2 = 0;
+            for (int u = 0; u < q.NOD; u++) L2 = u == 0 ? c[u] * c[u] : L2 + c[u] * c[u];
+            nm = 2 * fabs(rig) * L2;
+        }
+        cnt[k] = z;
+        nrm[k] = nm;
+    }
+}
+
+// nonzeros of every bond in MATLAB find order (column-major), with 1-based
+// global DOFs NOD (node - 1) + 1 .. NOD node (:91-100, :129-138)
+__global__ void k_coo_write(CooBonds q, const int64_t *__restrict__ off, double *rows, double *cols, double *vals)
+{
+    GRID_STRIDE(k, q.nB)
+    {
+        double rig, c[3];
+        int64_t i, j;
+        if (!coo_local(q, k, rig, c, i, j)) continue;
+        const int D = 2 * q.NOD;
+        int64_t o = off[k];
+        for (int s = 0; s < D; s++)
+            for (int r = 0; r < D; r++) {
+                const double v = coo_entry(rig, c, q.NOD, r, s);
+                if (v == 0) continue;
+                const int64_t gr = (r < q.NOD ? q.NOD * i : q.NOD * j) + (r % q.NOD) + 1;
+                const int64_t gc = (s < q.NOD ? q.NOD * i : q.NOD * j) + (s % q.NOD) + 1;
+                rows[o] = (double)gr;
+                cols[o] = (double)gc;
+                vals[o] = v;
+                o++;
+            }
+    }
+}
+
+__global__ void k_node_sum(const int64_t *__restrict__ off, const uint32_t *__restrict__ ent, int64_t n,
+                           const double *__restrict__ v, double *out)
+{
+    GRID_STRIDE(i, n)
+    {
+        double a = 0;
+        for (int64_t e = off[i]; e < off[i + 1]; e++) a = a + v[ent[e] >> 1];
+        out[i] = a;
+    }
+}
+
+__global__ void k_bl_nodes(const double *__restrict__ bl, int64_t nB, int64_t n, uint32_t *a, uint32_t *b, int *bad)
+{
+    GRID_STRIDE(k, nB)
+    {
+        const double x = bl[k], y = bl[nB + k];
+        if (!(x >= 1 && y >= 1 && x <= (double)n && y <= (double)n)) {
+            *bad = 1;
+            a[k] = b[k] = 0;
+            continue;
+        }
+        a[k] = (uint32_t)(x - 1);
+        b[k] = (uint32_t)(y - 1);
+    }
+}
+
+}  // namespace
+
+extern "C" int bbpd_dev_buildstiffnessmatrix(const double *X, int64_t nNodes, int NOD, const double *BONDLIST,
+        const double *VCF, double VOLUME, const double *BS, const double *BFM, const double *failFlag, const double *BSF,
+        int64_t nBonds, int64_t capacity, int64_t *nnz, double *rowIndex, double *columnIndex, double *values,
+        double *massVector, void *stream)
+{
+    if (!nnz) return fail(BBPD_ERR_ARG, "null nnz");
+    if (NOD != 2 && NOD != 3) return fail(BBPD_ERR_ARG, "NOD must be 2 or 3");
+    if (nNodes < 1 || nNodes >= ((int64_t)1 << 31) || nBonds < 0 || nBonds >= ((int64_t)1 << 31))
+        return fail(BBPD_ERR_ARG, "need 1 <= nNodes < 2^31 and 0 <= nBonds < 2^31");
+    if (!X || (nBonds && (!BONDLIST || !VCF || !BS || !BFM || !failFlag || !BSF))) return fail(BBPD_ERR_ARG, "null array");
+    TRY(require_device());
+    cudaStream_t st = as_stream(stream);
+    const int64_t n = nNodes, nB = nBonds, m = 2 * nB;
+    CooBonds q{X, BONDLIST, VCF, BS, BFM, failFlag, BSF, n, nB, NOD, VOLUME};
+    std::vector<void *> tmp;
+    auto get = [&](void **p, size_t bytes) -> int {
+        BBPD_CUDA_TRY(cudaMallocAsync(p, std::max<size_t>(bytes, 8), st));
+        tmp.push_back(*p);
+        return BBPD_OK;
+    };
+    struct Free {
+        std::vector<void *> &t;
+        cudaStream_t s;
+        ~Free()
+        {
+            for (void *p : t) cudaFreeAsync(p, s);
+        }
+    } freer{tmp, st};
+    uint32_t *a = nullptr, *b = nullptr, *key = nullptr, *skey = nullptr, *val = nullptr, *ent = nullptr;
+    int64_t *cnt = nullptr, *off = nullptr, *first = nullptr, *last = nullptr, *ncnt = nullptr, *noff = nullptr;
+    double *nrm = nullptr;
+    int *bad = nullptr;
+    TRY(get((void **)&a, 4 * nB));
+    TRY(get((void **)&b, 4 * nB));
+    TRY(get((void **)&bad, sizeof(int)));
+    TRY(get((void **)&cnt, 8 * (nB + 1)));
+    TRY(get((void **)&off, 8 * (nB + 1)));
+    TRY(get((void **)&nrm, 8 * nB));
+    BBPD_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), st));
+    k_bl_nodes<<<blocks_for(nB), kThreads, 0, st>>>(BONDLIST, nB, n, a, b, bad);
+    k_coo_count<<<blocks_for(nB + 1), kThreads, 0, st>>>(q, cnt, nrm);
+    TRY(launch_check());
+    size_t tb = 0;
+    BBPD_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, nB + 1, st));
+    void *t1 = nullptr;
+    TRY(get(&t1, tb));
+    BBPD_CUDA_TRY(cub::DeviceScan::ExclusiveSum(t1, tb, cnt, off, nB + 1, st));
+    int64_t total = 0;
+    int hbad = 0;
+    BBPD_CUDA_TRY(cudaMemcpyAsync(&total, off + nB, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    BBPD_CUDA_TRY(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(st));
+    if (hbad) return fail(BBPD_ERR_ARG, "BONDLIST holds node ids outside [1, nNodes]");
+    *nnz = total;
+    if (capacity >= total && total > 0 && rowIndex && columnIndex && values) {
+        k_coo_write<<<blocks_for(nB), kThreads, 0, st>>>(q, off, rowIndex, columnIndex, values);
+        TRY(launch_check());
+    }
+    if (massVector) {
+        // massVector(i) accumulates norm(Klocal) of its intact bonds in bond order
+        TRY(get((void **)&key, 4 * m));
+        TRY(get((void **)&skey, 4 * m));
+        TRY(get((void **)&val, 4 * m));
+        TRY(get((void **)&ent, 4 * m));
+        TRY(get((void **)&first, 8 * n));
+        TRY(get((void **)&last, 8 * n));
+        TRY(get((void **)&ncnt, 8 * (n + 1)));
+        TRY(get((void **)&noff, 8 * (n + 1)));
+        BBPD_CUDA_TRY(cudaMemsetAsync(first, 0, 8 * n, st));
+        BBPD_CUDA_TRY(cudaMemsetAsync(last, 0, 8 * n, st));
+        int bits = 1;
+        while (bits < 32 && ((int64_t)1 << bits) < n) bits++;
+        if (m > 0) {
+            k_entry_keys<<<blocks_for(m), kThreads, 0, st>>>(a, b, nB, key);
+            k_iota<<<blocks_for(m), kThreads, 0, st>>>(val, m);
+            BBPD_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, val, ent, m, 0, bits, st));
+            void *t2 = nullptr;
+            TRY(get(&t2, tb));
+            BBPD_CUDA_TRY(cub::DeviceRadixSort::SortPairs(t2, tb, key, skey, val, ent, m, 0, bits, st));
+            k_run_bounds<<<blocks_for(m), kThreads, 0, st>>>(skey, m, first, last);
+        }
+        k_counts<<<blocks_for(n + 1), kThreads, 0, st>>>(first, last, n, ncnt);
+        BBPD_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, ncnt, noff, n + 1, st));
+        void *t3 = nullptr;
+        TRY(get(&t3, tb));
+        BBPD_CUDA_TRY(cub::DeviceScan::ExclusiveSum(t3, tb, ncnt, noff, n + 1, st));
+        k_node_sum<<<blocks_for(n), kThreads, 0, st>>>(noff, ent, n, nrm, massVector);
+        TRY(launch_check());
+    }
+    BBPD_CUDA_TRY(cudaStreamSynchronize(st));
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_buildstiffnessmatrix(const double *X, int64_t nNodes, int NOD, const double *BONDLIST,
+        const double *VCF, double VOLUME, const double *BS, const double *BFM, const double *failFlag, const double *BSF,
+        int64_t nBonds, int64_t capacity, int64_t *nnz, double *rowIndex, double *columnIndex, double *values,
+        double *massVector)
+{
+    if (!nnz) return fail(BBPD_ERR_ARG, "null nnz");
+    if (NOD != 2 && NOD != 3) return fail(BBPD_ERR_ARG, "NOD must be 2 or 3");
+    if (nNodes < 1 || nBonds < 0) return fail(BBPD_ERR_ARG, "bad sizes");
+    if (!X || (nBonds && (!BONDLIST || !VCF || !BS || !BFM || !failFlag || !BSF))) return fail(BBPD_ERR_ARG, "null array");
+    TRY(require_device());
+    cudaStream_t st = nullptr;
+    BBPD_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct Own {
+        cudaStream_t s;
+        std::vector<void *> p;
+        ~Own()
+        {
+            for (void *q : p) cudaFreeAsync(q, s);
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    } own{st, {}};
+    auto up = [&](const double *h, int64_t cnt, double **d) -> int {
+        BBPD_CUDA_TRY(cudaMallocAsync((void **)d, sizeof(double) * std::max<int64_t>(cnt, 1), st));
+        own.p.push_back(*d);
+        return h ? staging::upload_copy(*d, h, cnt, st) : BBPD_OK;
+    };
+    const int64_t nB = nBonds;
+    double *dX, *dbl, *dV, *dBS, *dBFM, *dfail, *dBSF, *dm = nullptr;
+    TRY(up(X, NOD * nNodes, &dX));
+    TRY(up(BONDLIST, 2 * nB, &dbl));
+    TRY(up(VCF, nB, &dV));
+    TRY(up(BS, nB, &dBS));
+    TRY(up(BFM, nB, &dBFM));
+    TRY(up(failFlag, nB, &dfail));
+    TRY(up(BSF, nB, &dBSF));
+    if (massVector) TRY(up(nullptr, nNodes, &dm));
+    TRY(bbpd_dev_buildstiffnessmatrix(dX, nNodes, NOD, dbl, dV, VOLUME, dBS, dBFM, dfail, dBSF, nB, 0, nnz, nullptr,
+                                      nullptr, nullptr, dm, st));
+    const int64_t total = *nnz;
+    if (capacity >= total && total > 0 && rowIndex && columnIndex && values) {
+        double *dr, *dc, *dv;
+        TRY(up(nullptr, total, &dr));
+        TRY(up(nullptr, total, &dc));
+        TRY(up(nullptr, total, &dv));
+        int64_t again = 0;
+        TRY(bbpd_dev_buildstiffnessmatrix(dX, nNodes, NOD, dbl, dV, VOLUME, dBS, dBFM, dfail, dBSF, nB, total, &again,
+                                          dr, dc, dv, nullptr, st));
+        TRY(staging::download_copy(rowIndex, dr, total, st));
+        TRY(staging::download_copy(columnIndex, dc, total, st));
+        TRY(staging::download_copy(values, dv, total, st));
+    }
+    if (dm) TRY(staging::download_copy(massVector, dm, nNodes, st));
+    return BBPD_OK;
+}

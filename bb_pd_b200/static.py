@@ -88,3 +88,32 @@ class StaticSolver:
             self.close()
         except Exception:
             pass
+
+
+def buildstiffnessmatrixCSCformat(nodalCoordinates, BONDLIST, VOLUMECORRECTIONFACTORS, VOLUME, BONDSTIFFNESS,
+                                  BFMULTIPLIER, fail, bondSofteningFactor, UNDEFORMEDLENGTH=None):
+    """buildstiffnessmatrixCSCformat.m:1 on the GPU -> (globalRowIndex,
+    globalColumnIndex, globalNonZeroValues, massVector)."""
+    X = np.asfortranarray(nodalCoordinates, dtype=np.float64)
+    n, nod = X.shape
+    bl = np.asfortranarray(BONDLIST, dtype=np.float64)
+    arrs = [np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+            for a in (VOLUMECORRECTIONFACTORS, BONDSTIFFNESS, BFMULTIPLIER, fail, bondSofteningFactor)]
+    nB = bl.shape[0]
+    if bl.ndim != 2 or bl.shape[1] != 2 or any(a.size != nB for a in arrs):
+        raise ValueError("need an nBonds x 2 BONDLIST and nBonds entries in every per-bond array")
+    L = N.lib()
+    p, i64 = C.c_void_p, C.c_int64
+    L.bbpd_buildstiffnessmatrix.argtypes = [p, i64, C.c_int, p, p, C.c_double, p, p, p, p, i64, i64,
+                                            C.POINTER(i64), p, p, p, p]
+    P = lambda a: None if a is None else a.ctypes.data_as(p)
+    nnz = C.c_int64()
+    mass = np.zeros(n)
+    vcf, bs, bfm, fl, bsf = arrs
+    N.check(L.bbpd_buildstiffnessmatrix(P(X), n, nod, P(bl), P(vcf), float(VOLUME), P(bs), P(bfm), P(fl), P(bsf), nB,
+                                        0, C.byref(nnz), None, None, None, P(mass)))
+    m = nnz.value
+    rows, cols, vals = np.zeros(m), np.zeros(m), np.zeros(m)
+    N.check(L.bbpd_buildstiffnessmatrix(P(X), n, nod, P(bl), P(vcf), float(VOLUME), P(bs), P(bfm), P(fl), P(bsf), nB,
+                                        m, C.byref(nnz), P(rows), P(cols), P(vals), None))
+    return rows, cols, vals, mass

@@ -402,6 +402,31 @@ int bbpd_static_step(bbpd_static *solver, double increment, double tol, int max_
 int bbpd_static_get(bbpd_static *solver, int field, double *out);
 int bbpd_static_destroy(bbpd_static *solver);
 
+/* replaces buildstiffnessmatrixCSCformat.m:1 (NOD 2 or 3): the triplets of the
+ * global stiffness matrix, bond by bond (intact bonds only, fail == 1), each
+ * bond's nonzeros in MATLAB find order (column-major over its local matrix
+ * rig [c c^T, -c c^T; -c c^T, c c^T], rows and columns its 1-based global
+ * DOFs), with rig = BFMULTIPLIER ((BONDSTIFFNESS / L^3) VCF VOLUME^2)
+ * (1 - bondSofteningFactor) for NOD = 3 and without the softening factor for
+ * NOD = 2, c the bond vector at the given coordinates and L its length (L^3 is
+ * formed as L L L). massVector (nNodes, or NULL) accumulates norm(Klocal) =
+ * 2 |rig| |c|^2 of every intact bond at both ends, in bond order (MATLAB's
+ * norm computes the same value by an SVD, to rounding). *nnz always receives
+ * the triplet count; the triplets are written when capacity >= *nnz. The
+ * reference's UNDEFORMEDLENGTH argument is unused there and absent here. */
+int bbpd_buildstiffnessmatrix(const double *nodalCoordinates, int64_t nNodes, int NOD,
+        const double *BONDLIST, const double *VOLUMECORRECTIONFACTORS, double VOLUME,
+        const double *BONDSTIFFNESS, const double *BFMULTIPLIER, const double *fail,
+        const double *bondSofteningFactor, int64_t nBonds, int64_t capacity, int64_t *nnz,
+        double *globalRowIndex, double *globalColumnIndex, double *globalNonZeroValues,
+        double *massVector);
+int bbpd_dev_buildstiffnessmatrix(const double *nodalCoordinates, int64_t nNodes, int NOD,
+        const double *BONDLIST, const double *VOLUMECORRECTIONFACTORS, double VOLUME,
+        const double *BONDSTIFFNESS, const double *BFMULTIPLIER, const double *fail,
+        const double *bondSofteningFactor, int64_t nBonds, int64_t capacity, int64_t *nnz,
+        double *globalRowIndex, double *globalColumnIndex, double *globalNonZeroValues,
+        double *massVector, void *stream);
+
 typedef struct bbpd_solver bbpd_solver;
 
 /* Validate, lay out (per-node bond lists in bond order, sliced by 32 nodes)

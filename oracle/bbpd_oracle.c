@@ -815,3 +815,46 @@ int64_t orc_buildnotch(const double *X, int64_t nNodes, const double *bl, const 
     }
     return m;
 }
+
+int64_t orc_stiffness_coo(const double *X, int64_t nNodes, int NOD, const double *bl,
+                          const double *VCF, double V, const double *BS, const double *BFM,
+                          const double *fail, const double *BSF, int64_t nBonds,
+                          int64_t capacity, double *rows, double *cols, double *vals,
+                          double *mass)
+{
+    const int64_t n = nNodes;
+    if (mass)
+        for (int64_t i = 0; i < n; i++) mass[i] = 0.0;
+    int64_t cnt = 0;
+    for (int64_t k = 0; k < nBonds; k++) {
+        if (fail[k] != 1) continue;                                      /* :72, :110 */
+        const int64_t i = (int64_t)bl[k] - 1, j = (int64_t)bl[nBonds + k] - 1;
+        double c[3], L2 = 0;
+        for (int u = 0; u < NOD; u++) {
+            c[u] = X[j + u * n] - X[i + u * n];                          /* :76-77, :114-116 */
+            L2 = u == 0 ? c[u] * c[u] : L2 + c[u] * c[u];
+        }
+        const double L = sqrt(L2);
+        const double rig = NOD == 3 ? BFM[k] * ((BS[k] / (L * L * L)) * VCF[k] * (V * V)) * (1 - BSF[k])   /* :118 */
+                                    : BFM[k] * (BS[k] / (L * L * L)) * VCF[k] * (V * V);                     /* :79 */
+        const int D = 2 * NOD;
+        for (int s = 0; s < D; s++)                                      /* find: column-major */
+            for (int r = 0; r < D; r++) {
+                const double m = c[r % NOD] * c[s % NOD];
+                const double v = ((r < NOD) == (s < NOD)) ? rig * m : rig * (-m);
+                if (v == 0) continue;
+                if (cnt < capacity) {
+                    rows[cnt] = (double)((r < NOD ? NOD * i : NOD * j) + (r % NOD) + 1);
+                    cols[cnt] = (double)((s < NOD ? NOD * i : NOD * j) + (s % NOD) + 1);
+                    vals[cnt] = v;
+                }
+                cnt++;
+            }
+        if (mass) {
+            const double nm = 2 * fabs(rig) * L2;                        /* norm(Klocal) */
+            mass[i] = mass[i] + nm;
+            mass[j] = mass[j] + nm;
+        }
+    }
+    return cnt;
+}

@@ -164,6 +164,16 @@ int64_t orc_buildnotch(const double *X, int64_t nNodes, const double *bl, const 
                        double *blOut, double *L0Out, double *nFamily, double *famPtr,
                        double *family);
 
+/* buildstiffnessmatrixCSCformat.m:57-150 (NOD 2 or 3), literal: the
+ * nonzeros of every intact bond's local matrix in MATLAB find order and
+ * massVector += norm(Klocal) at both ends, the norm taken as 2 |rig| |c|^2.
+ * Returns the triplet count; writes the triplets when capacity allows. */
+int64_t orc_stiffness_coo(const double *X, int64_t nNodes, int NOD, const double *bl,
+                          const double *VCF, double V, const double *BS, const double *BFM,
+                          const double *fail, const double *BSF, int64_t nBonds,
+                          int64_t capacity, double *rows, double *cols, double *vals,
+                          double *mass);
+
 /* smoothstepdata.m:40-42 */
 double orc_smoothstep(double t, double t0, double t1, double v0, double v1);
 

@@ -101,6 +101,9 @@ def lib() -> C.CDLL:
         L.orc_buildnotch.argtypes = [_P, C.c_int64, _P, _P, C.c_int64, C.c_double, C.c_double, C.c_double,
                                      _P, _P, _P, _P, _P]
         L.orc_buildnotch.restype = C.c_int64
+        L.orc_stiffness_coo.argtypes = [_P, C.c_int64, C.c_int, _P, _P, C.c_double, _P, _P, _P, _P, C.c_int64,
+                                        C.c_int64, _P, _P, _P, _P]
+        L.orc_stiffness_coo.restype = C.c_int64
         L.orc_damageenergy.argtypes = [_P, _P, _P, _P, _P, C.c_double, C.c_double, C.c_double, _P, C.c_int64]
         L.orc_bondforces.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_double, _P, _P, C.c_int64]
         L.orc_nodalforces_chunked.argtypes = [C.c_int64, C.c_int64, _P, _P, _P, _P, _P, C.c_int]
