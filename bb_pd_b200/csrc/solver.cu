@@ -54,6 +54,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <thread>
 #include <unordered_map>
@@ -2279,6 +2280,26 @@ struct TempBufs {
 
 inline int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
 
+// The layout build's temporaries (gigabytes for large problems) come from the
+// device's default stream-ordered pool. With the pool's default release
+// threshold of zero, every synchronisation returns the freed memory to the
+// driver and the next build maps it again; keeping up to 8 GB reserved lets
+// consecutive builds (a serving loop) reuse it. Set once per device.
+static void keep_layout_pool(int device)
+{
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> g(mu);
+    if (std::find(done.begin(), done.end(), device) != done.end()) return;
+    done.push_back(device);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = (uint64_t)8 << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+}
+
 // Layout built on the device, for the input and Morton node orders. The host
 // converts the per-bond arrays while staging them (node ids to device
 // positions, dictionary ids, fail and BONDTYPE packed in a byte); the sort of
@@ -2293,6 +2314,7 @@ static int device_layout(bbpd_solver *S, const bbpd_problem *pb, const int32_t *
     const double *bl = pb->bondlist;
     cudaStream_t st = S->stream;
     Dev &d = S->d;
+    keep_layout_pool(S->device);
     TempBufs tmp(st);
 
     // staged per-bond inputs

@@ -435,6 +435,7 @@ struct bbpd_static {
     uint8_t *skip = nullptr;
     SBonds b{};
     SNodes g{};
+    cudaGraphExec_t cg_exec = nullptr;   // kCgBlock conjugate-gradient iterations, captured once
     template <class T>
     int alloc(T **q, size_t count)
     {
@@ -445,12 +446,52 @@ struct bbpd_static {
     ~bbpd_static()
     {
         if (st) cudaStreamSynchronize(st);
+        if (cg_exec) cudaGraphExecDestroy(cg_exec);
         for (void *q : allocs) cudaFree(q);
         if (st) cudaStreamDestroy(st);
     }
 };
 
 namespace {
+
+constexpr int kCgBlock = 8;   // iterations between convergence checks
+
+// `iters` conjugate-gradient iterations; the step sizes live in device memory,
+// so nothing here waits for the host
+void enqueue_cg(bbpd_static *S, int iters)
+{
+    cudaStream_t st = S->st;
+    const int64_t n = S->n;
+    for (int c = 0; c < iters; c++) {
+        k_static_spmv<<<kRedBlocks, kThreads, 0, st>>>(S->g, S->b.a, S->b.b, S->b.rig, S->b.c, S->p, S->Kp, S->part);
+        k_reduce<<<1, 32, 0, st>>>(S->part, kRedBlocks, 1, S->scal + 2);
+        k_cg_update<<<kRedBlocks, kThreads, 0, st>>>(n, S->skip, S->Minv, S->scal, S->p, S->Kp, S->d, S->r, S->z,
+                                                     S->part);
+        k_reduce<<<1, 32, 0, st>>>(S->part, kRedBlocks, 2, S->rzn);
+        k_cg_direction<<<blocks_for(3 * n), kThreads, 0, st>>>(n, S->z, S->p, S->rzn, S->scal);
+        k_roll<<<1, 32, 0, st>>>(S->scal, S->rzn);
+    }
+}
+
+// kCgBlock iterations as one graph launch (the 6 kernels of an iteration are
+// launch-bound on small problems); captured on first use
+int run_cg_block(bbpd_static *S)
+{
+    if (!S->cg_exec) {
+        cudaGraph_t gr = nullptr;
+        BBPD_CUDA_TRY(cudaStreamBeginCapture(S->st, cudaStreamCaptureModeThreadLocal));
+        enqueue_cg(S, kCgBlock);
+        cudaError_t e = cudaStreamEndCapture(S->st, &gr);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&S->cg_exec, gr, 0);
+        if (gr) cudaGraphDestroy(gr);
+        if (e != cudaSuccess) {
+            S->cg_exec = nullptr;
+            return fail(BBPD_ERR_CUDA, "conjugate-gradient graph: %s", cudaGetErrorString(e));
+        }
+    }
+    BBPD_CUDA_TRY(cudaGraphLaunch(S->cg_exec, S->st));
+    return BBPD_OK;
+}
 
 int read_scalars(bbpd_static *S, const double *src, int cnt, double *out)
 {
@@ -681,23 +722,17 @@ extern "C" int bbpd_static_step(bbpd_static *S, double increment, double tol, in
         TRY(read_scalars(S, S->scal, 2, s01));
         const double rr0 = s01[1];
         if (rr0 > 0) {
-            for (int c = 1; c <= max_cg; c++) {
-                k_static_spmv<<<kRedBlocks, kThreads, 0, st>>>(S->g, S->b.a, S->b.b, S->b.rig, S->b.c, S->p, S->Kp,
-                                                               S->part);
-                k_reduce<<<1, 32, 0, st>>>(S->part, kRedBlocks, 1, S->scal + 2);
-                k_cg_update<<<kRedBlocks, kThreads, 0, st>>>(n, S->skip, S->Minv, S->scal, S->p, S->Kp, S->d, S->r,
-                                                             S->z, S->part);
-                k_reduce<<<1, 32, 0, st>>>(S->part, kRedBlocks, 2, S->rzn);
-                stats->cg_iterations++;
-                if (c % 8 == 0 || c == max_cg) {
-                    TRY(launch_check());
-                    double rz[2];
-                    TRY(read_scalars(S, S->rzn, 2, rz));
-                    if (!std::isfinite(rz[1])) return fail(BBPD_ERR_NONFINITE, "conjugate gradient diverged");
-                    if (rz[1] <= cg_tol * cg_tol * rr0) break;
-                }
-                k_cg_direction<<<blocks_for(3 * n), kThreads, 0, st>>>(n, S->z, S->p, S->rzn, S->scal);
-                k_roll<<<1, 32, 0, st>>>(S->scal, S->rzn);
+            for (int done = 0; done < max_cg;) {
+                const int blk = std::min(kCgBlock, max_cg - done);
+                if (blk == kCgBlock) TRY(run_cg_block(S));
+                else enqueue_cg(S, blk);
+                TRY(launch_check());
+                done += blk;
+                stats->cg_iterations += blk;
+                double rz[2];
+                TRY(read_scalars(S, S->rzn, 2, rz));
+                if (!std::isfinite(rz[1])) return fail(BBPD_ERR_NONFINITE, "conjugate gradient diverged");
+                if (rz[1] <= cg_tol * cg_tol * rr0) break;
             }
         }
         k_move<<<blocks_for(3 * n), kThreads, 0, st>>>(3 * n, S->x, S->d);
