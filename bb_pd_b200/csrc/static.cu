@@ -174,20 +174,23 @@ __global__ void k_static_nodal(SNodes g, const double *__restrict__ f, double V,
     }
 }
 
-// y = K p on the free DOFs (held DOFs: y = 0, p taken as 0), and a partial of p.y
+// y = K p on the free DOFs (held DOFs: y = 0, p taken as 0), and a partial of
+// p.y. One warp per node: the lanes take its entries 32 apart and the sums
+// meet in a fixed butterfly, so the product is deterministic.
 __global__ void k_static_spmv(SNodes g, const uint32_t *__restrict__ a, const uint32_t *__restrict__ b,
                               const double *__restrict__ rig, const double *__restrict__ cv,
                               const double *__restrict__ p, double *y, double *part)
 {
     __shared__ double sh[kThreads / 32];
+    const int lane = threadIdx.x & 31;
     double acc = 0;
     const int64_t n = g.n, nB = g.nB;
-    GRID_STRIDE(i, n)
-    {
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         double pi[3];
         for (int c = 0; c < 3; c++) pi[c] = g.held[i + c * n] ? 0.0 : p[i + c * n];
         double yi[3] = {0, 0, 0};
-        for (int64_t e = g.off[i]; e < g.off[i + 1]; e++) {
+        for (int64_t e = g.off[i] + lane; e < g.off[i + 1]; e += 32) {
             const uint32_t q = g.ent[e];
             const int64_t k = q >> 1;
             const double r = rig[k];
@@ -201,14 +204,16 @@ __global__ void k_static_spmv(SNodes g, const uint32_t *__restrict__ a, const ui
             yi[1] += t * c1;
             yi[2] += t * c2;
         }
-        for (int c = 0; c < 3; c++) {
-            const double v = g.held[i + c * n] ? 0.0 : yi[c];
-            y[i + c * n] = v;
-            acc += pi[c] * v;
-        }
+        for (int o = 16; o > 0; o >>= 1)
+            for (int c = 0; c < 3; c++) yi[c] += __shfl_xor_sync(0xffffffffu, yi[c], o);
+        if (lane == 0)
+            for (int c = 0; c < 3; c++) {
+                const double v = g.held[i + c * n] ? 0.0 : yi[c];
+                y[i + c * n] = v;
+                acc += pi[c] * v;
+            }
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    if (lane == 0) sh[threadIdx.x >> 5] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
         double s = 0;
