@@ -139,6 +139,7 @@ struct Dev {
     const double *s0e, *s1e, *sce;   // per-entry law stretches or null
     const double *X;
     double *xb0, *xb1;               // positions: step n reads xb[(n-1)&1], writes xb[n&1]
+    double4 *xa0, *xa1;              // the same positions as (x, y, z, 0) per node: one 32-byte load per neighbour gather
     double *u, *v, *a;
     double *F0, *F1;                 // F of step n lives in F[n&1]
     const double *mass, *rho;
@@ -557,6 +558,14 @@ __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fe
     return entry_general<LAW, PREC>(d, e, f.w, f.sv, f.g, f.sc, xi, yi, zi, f.xj, f.yj, f.zj);
 }
 
+// A node's (x, y, z) from its 32-byte position record in one 256-bit load.
+__device__ __forceinline__ void load_pos(const double4 *p, double &x, double &y, double &z)
+{
+    double w;
+    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(x), "=d"(y), "=d"(z), "=d"(w) : "l"(p));
+    (void)w;
+}
+
 // Forces of the 32 nodes of one slice (FP64 form).
 // Lane `lane` owns node sl*32+lane and walks its entries in bond order, a group
 // of 4 at a time: the next group's streams load while the current group's 12
@@ -564,7 +573,7 @@ __device__ __forceinline__ double3 entry_force(const Dev &d, int64_t e, const Fe
 // node's force summed in the reference's order.
 template <int LAW, int PREC, class CID, int SCE>
 __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane, bool safe,
-                                             const double *xs, double &tx, double &ty,
+                                             const double *xs, const double4 *xa, double &tx, double &ty,
                                              double &tz)
 {
     const int64_t nN = d.n_nodes;
@@ -591,7 +600,7 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
         for (int q = 0; q < 4; q++) {
             if (q < nq) {
                 const uint32_t j = group_w(Gc, q) & COL_MASK;
-                xj[q] = x0[j]; yj[q] = x1[j]; zj[q] = x2[j];
+                load_pos(xa + j, xj[q], yj[q], zj[q]);
             } else {   // unused slot: finite values for the branch-free pass
                 xj[q] = xi + 1.0; yj[q] = yi; zj[q] = zi;
             }
@@ -788,6 +797,8 @@ struct StepBufs {
     double *Fc;
     const double *Fp, *xs;
     double *xn;
+    const double4 *xas;
+    double4 *xan;
     const float4 *urhs;
     const float2 *urls;
     float4 *urhn;
@@ -803,6 +814,8 @@ __device__ __forceinline__ StepBufs step_bufs(const Dev &d, int64_t n)
     b.Fp = (n & 1) ? d.F0 : d.F1;
     b.xs = ((n - 1) & 1) ? d.xb1 : d.xb0;
     b.xn = (n & 1) ? d.xb1 : d.xb0;
+    b.xas = ((n - 1) & 1) ? d.xa1 : d.xa0;
+    b.xan = (n & 1) ? d.xa1 : d.xa0;
     b.urhs = ((n - 1) & 1) ? d.urh1 : d.urh0;
     b.urls = ((n - 1) & 1) ? d.url1 : d.url0;
     b.urhn = (n & 1) ? d.urh1 : d.urh0;
@@ -926,6 +939,7 @@ __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, in
                 bad |= !isfinite(un[dof]) || !isfinite(vn[dof]);
                 far |= coord_out_of_range(xn3[dof]);
             }
+            b.xan[i] = make_double4(xn3[0], xn3[1], xn3[2], 0.0);
             if (PREC == kP32X) {
                 b.urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
                 b.urln[i] = make_float2(ul[1], ul[2]);
@@ -1005,6 +1019,7 @@ __device__ __forceinline__ void adr_update_slice(const Dev &d, const StepBufs &b
             bad |= !isfinite(un[dof]) || !isfinite(vn[dof]);
             far |= coord_out_of_range(xn3[dof]);
         }
+        b.xan[i] = make_double4(xn3[0], xn3[1], xn3[2], 0.0);
         if (PREC == kP32X) {
             b.urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
             b.urln[i] = make_float2(ul[1], ul[2]);
@@ -1052,7 +1067,7 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
             prefetch_slice_head<CID, SCE>(d, sl_next, lane);
             double tx, ty, tz;
             if (PREC == kP32X) slice_forces_x<LAW, CID, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
-            else slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, b.xs, tx, ty, tz);
+            else slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, b.xs, b.xas, tx, ty, tz);
             finish_slice<SCHEME, PREC>(d, b, sl, lane, tx, ty, tz, it);
             sl = sl_next;
         }
@@ -1427,7 +1442,7 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
                 const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
                 double tx, ty, tz;
                 if (PREC == kP32X) slice_forces_x<LAW, uint16_t, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
-                else slice_forces<LAW, PREC, uint16_t, SCE>(d, sl, lane, safe, b.xs, tx, ty, tz);
+                else slice_forces<LAW, PREC, uint16_t, SCE>(d, sl, lane, safe, b.xs, b.xas, tx, ty, tz);
                 finish_slice<BBPD_SCHEME_ADR, PREC>(d, b, sl, lane, tx, ty, tz, it);
             }
             gi = gnext;
@@ -1638,6 +1653,7 @@ __global__ void k_node_init(Dev d, double U1)
         const uint8_t f = d.nflag[p];
         bool far = false;
         float uh[3], ul[3];
+        double xr[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const int64_t e = p + c * nN;
@@ -1646,16 +1662,25 @@ __global__ void k_node_init(Dev d, double U1)
             d.u[e] = u;
             d.xb0[e] = x;
             d.xb1[e] = x;
+            xr[c] = x;
             far |= coord_out_of_range(x);
             uh[c] = (float)u;
             ul[c] = (float)(u - (double)uh[c]);
         }
+        d.xa0[p] = d.xa1[p] = make_double4(xr[0], xr[1], xr[2], 0.0);
         if (d.urh0) {
             d.urh0[p] = d.urh1[p] = make_float4(uh[0], uh[1], uh[2], ul[0]);
             d.url0[p] = d.url1[p] = make_float2(ul[1], ul[2]);
         }
         if (far) atomicOr(d.sticky, 1u);
     }
+}
+
+// Position records (x, y, z, 0) from the SoA position buffer.
+__global__ void k_pack_positions(const double *__restrict__ x, int64_t nN, double4 *xa)
+{
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nN; p += (int64_t)gridDim.x * blockDim.x)
+        xa[p] = make_double4(x[p], x[p + nN], x[p + 2 * nN], 0.0);
 }
 
 typedef void (*kernel_t)(Dev, int64_t, int64_t);
@@ -2784,6 +2809,8 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     const size_t b3 = sizeof(double) * 3 * (size_t)nN;
     TRY(S->alloc(&d.xb0, (size_t)(3 * nN)));
     TRY(S->alloc(&d.xb1, (size_t)(3 * nN)));
+    TRY(S->alloc(&d.xa0, (size_t)nN));
+    TRY(S->alloc(&d.xa1, (size_t)nN));
     TRY(S->alloc(&d.u, (size_t)(3 * nN)));
     TRY(S->alloc(&d.v, (size_t)(3 * nN)));
     TRY(S->alloc(&d.F0, (size_t)(3 * nN)));
@@ -3109,6 +3136,13 @@ extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
         if (field == BBPD_FIELD_DEFORMED) {
             // both position buffers: the next step reads the one of its parity
             BBPD_CUDA_TRY(cudaMemcpy(dst == S->d.xb0 ? S->d.xb1 : S->d.xb0, h.data(), sizeof(double) * 3 * nN, cudaMemcpyHostToDevice));
+            // the position records follow, ordered after those copies on the
+            // legacy stream
+            const int blocks = (int)std::min<int64_t>((nN + 255) / 256, 148 * 32);
+            k_pack_positions<<<blocks, 256, 0, 0>>>(S->d.xb0, nN, S->d.xa0);
+            k_pack_positions<<<blocks, 256, 0, 0>>>(S->d.xb1, nN, S->d.xa1);
+            BBPD_CUDA_TRY(cudaGetLastError());
+            BBPD_CUDA_TRY(cudaStreamSynchronize(0));
             bool far = false;
             for (double x : h) far |= !coord_safe(x);
             if (far) {   // sticky: from now on the kernels divide with IEEE division
@@ -3168,6 +3202,7 @@ extern "C" int bbpd_set_step(bbpd_solver *S, int64_t step, double cn)
     if (((step - S->step) & 1) != 0) {
         std::swap(S->d.F0, S->d.F1);
         std::swap(S->d.xb0, S->d.xb1);
+        std::swap(S->d.xa0, S->d.xa1);
         std::swap(S->d.urh0, S->d.urh1);
         std::swap(S->d.url0, S->d.url1);
     }
