@@ -343,14 +343,20 @@ constexpr int kPrefetch = BBPD_PREFETCH_GROUPS;
 
 __device__ __forceinline__ DictEntry ldg_dict(const DictEntry *t, uint32_t c)
 {
-    const double2 *p = reinterpret_cast<const double2 *>(t + c);
-    const double2 a = __ldg(p), b = __ldg(p + 1);
+    // the table is read-only for the whole launch: one 256-bit read-only load
     DictEntry e;
-    e.l0 = a.x;
-    e.rl0 = a.y;
-    e.vcf = b.x;
-    e.bs = b.y;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(e.l0), "=d"(e.rl0), "=d"(e.vcf), "=d"(e.bs)
+        : "l"(t + c));
     return e;
+}
+
+// FP32 form: the two float4 of dictionary entry c in one 256-bit read-only load.
+__device__ __forceinline__ void ldg_dictx(const float4 *t, uint32_t c, float4 &A, float4 &B)
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(A.x), "=f"(A.y), "=f"(A.z), "=f"(A.w), "=f"(B.x), "=f"(B.y), "=f"(B.z), "=f"(B.w)
+        : "l"(t + 2 * (size_t)c));
 }
 
 // Per-entry data, fetched before the arithmetic of the entry. sc is the
@@ -725,7 +731,8 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
             const int64_t e = e0 + q;
             const uint32_t w = group_w(Gc, q), c = valid ? Gc.cid(q) : 0u, sv = (Gc.s >> (8 * q)) & 0xFFu;
             const int bt = (w >> BT_SHIFT) & 3;
-            const float4 A = __ldg(&d.dictx[2 * c]), Bv = __ldg(&d.dictx[2 * c + 1]);
+            float4 A, Bv;
+            ldg_dictx(d.dictx, c, A, Bv);
             const float etx = (uj[q].x - ui.x) + (uj[q].w - ui.w);
             const float ety = (uj[q].y - ui.y) + (lj[q].x - li.x);
             const float etz = (uj[q].z - ui.z) + (lj[q].y - li.y);
