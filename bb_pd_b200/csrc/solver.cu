@@ -48,6 +48,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -2049,6 +2050,19 @@ static int validate_01(const double *a, int64_t n, const char *name)
     return BBPD_OK;
 }
 
+// BONDLIST row q holds two distinct node ids in [1, nN]
+inline bool bond_row_ok(const double *bl, int64_t nB, int64_t nN, int64_t q)
+{
+    const double a = bl[q], b = bl[nB + q];
+    return a >= 1 && b >= 1 && a <= (double)nN && b <= (double)nN && a == std::floor(a) && b == std::floor(b) && a != b;
+}
+
+static int bad_bond_row(const double *bl, int64_t nB, int64_t k)
+{
+    return fail(BBPD_ERR_ARG, "BONDLIST row %lld = (%g, %g) is not a pair of distinct node ids", (long long)k + 1, bl[k],
+                bl[nB + k]);
+}
+
 // Phases of bbpd_create, printed to stderr when BBPD_TIMING is set (each
 // phase then also waits for the device work it queued).
 struct PhaseTimer {
@@ -2352,12 +2366,23 @@ static int device_layout(bbpd_solver *S, const bbpd_problem *pb, const int32_t *
     // staged per-bond inputs
     uint32_t *key = nullptr;
     TRY(tmp.get(&key, (size_t)n2));
+    // rows are checked on the way (bond_row_ok); the first bad row fails the create
+    std::atomic<int64_t> bad_row(nB);
     TRY(staging::upload(key, n2, st, [&](int64_t q0, int64_t cnt, uint32_t *out) {
+        int64_t bad = nB;
         for (int64_t i = 0; i < cnt; i++) {
-            const int64_t q = q0 + i;
-            out[i] = (uint32_t)inv[(int64_t)bl[(q & 1) * nB + (q >> 1)] - 1];
+            const int64_t q = q0 + i, k = q >> 1;
+            if (!bond_row_ok(bl, nB, nN, k)) {
+                bad = std::min(bad, k);
+                out[i] = 0;
+                continue;
+            }
+            out[i] = (uint32_t)inv[(int64_t)bl[(q & 1) * nB + k] - 1];
+        }
+        for (int64_t cur = bad_row.load(); bad < cur && !bad_row.compare_exchange_weak(cur, bad);) {
         }
     }));
+    if (bad_row.load() < nB) return bad_bond_row(bl, nB, bad_row.load());
     LayoutArgs a{};
     a.nB = nB;
     a.T = prm->n_chunks;
@@ -2534,15 +2559,13 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
             return fail(BBPD_ERR_UNSUPPORTED, "non-zero stretchPlastic (steel plasticity) is not on this path");
     }
     const double *bl = pb->bondlist;
-    {
-        const int64_t k = first_bad(nB, [&](int64_t q) {
-            const double a = bl[q], b = bl[nB + q];
-            return !(a >= 1 && b >= 1 && a <= (double)nN && b <= (double)nN && a == std::floor(a) &&
-                     b == std::floor(b) && a != b);
-        });
-        if (k >= 0)
-            return fail(BBPD_ERR_ARG, "BONDLIST row %lld = (%g, %g) is not a pair of distinct node ids", (long long)k + 1,
-                        bl[k], bl[nB + k]);
+    // The FP64 form with a device-built layout checks BONDLIST while staging it
+    // (the only earlier pass over it); every other configuration reads it
+    // before then and checks it here.
+    const bool late_bl_check = prm->node_order != BBPD_ORDER_TILED && prm->precision != BBPD_PREC_FP32;
+    if (!late_bl_check) {
+        const int64_t k = first_bad(nB, [&](int64_t q) { return !bond_row_ok(bl, nB, nN, q); });
+        if (k >= 0) return bad_bond_row(bl, nB, k);
     }
 
     if (cudaSetDevice(device) != cudaSuccess) {

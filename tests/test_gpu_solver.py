@@ -206,6 +206,21 @@ def test_layouts_identical_at_scale(medium, law):
         s.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_bad_bondlist_first_row_reported(medium, precision):
+    """BONDLIST rows are checked while they are staged (FP64) or before the
+    dictionary pass (FP32): either way the first bad row is the one reported."""
+    nN = medium["nNodes"]
+    bl = medium["BONDLIST"].copy(order="F")
+    bl[2_000_000, 0] = nN + 1          # out of range
+    bl[1_234_567, 1] = 2.5             # not an integer
+    bad = dict(medium, BONDLIST=bl)
+    with pytest.raises(bb.BBPDError) as e:
+        bb.Solver(bad, **LAWKW["trilinear"], scheme="adr", precision=precision)
+    assert e.value.status == bb._native.ERR_ARG
+    assert "row 1234568 " in str(e.value), str(e.value)
+
+
 def test_split_launches_identical(small):
     kw = dict(LAWKW["bilinear"], scheme="adr", rate=-2e-6)
     a, b = bb.Solver(small, **kw), bb.Solver(small, **kw)
