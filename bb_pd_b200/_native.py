@@ -23,7 +23,7 @@ PREC_FP64, PREC_FP32 = range(2)
 AMP_LINEAR, AMP_SMOOTHSTEP = range(2)
 ORDER_INPUT, ORDER_MORTON, ORDER_TILED = range(3)
 FIELD = {"displacement": 0, "velocity": 1, "force": 2, "deformed": 3, "force_prev": 4,
-         "acceleration": 5, "bsf": 16, "flag": 17, "fail": 18}
+         "acceleration": 5, "bsf": 16, "flag": 17, "fail": 18, "damage_energy": 19}
 LAWS = {"linear": LAW_LINEAR, "bilinear": LAW_BILINEAR, "trilinear": LAW_TRILINEAR,
         "exponential": LAW_EXPONENTIAL}
 
@@ -132,6 +132,7 @@ def lib() -> C.CDLL:
         L.bbpd_selftest_wait_timeout.argtypes = [C.c_double]
         L.bbpd_selftest_division.argtypes = [C.c_int64, C.c_uint64] + [C.POINTER(C.c_int64)] * 3 + [_P]
         L.bbpd_get_reaction.argtypes = [C.c_void_p, C.c_int64, _P]
+        L.bbpd_track_damage_energy.argtypes = [C.c_void_p]
         L.bbpd_set_contact.argtypes = [C.c_void_p, C.c_int, C.POINTER(Penetrator)]
         L.bbpd_set_probes.argtypes = [C.c_void_p, C.c_int, _P, C.POINTER(C.c_int32)]
         L.bbpd_get_probes.argtypes = [C.c_void_p, C.c_int64, _P]

@@ -138,6 +138,7 @@ struct Dev {
     float4 *urh0, *urh1;             // FP32 form: per node (uh_x, uh_y, uh_z, ul_x), ping-pong like positions
     float2 *url0, *url1;             // FP32 form: per node (ul_y, ul_z); uh + ul is the FP32 split of u
     const double *s0e, *s1e, *sce;   // per-entry law stretches or null
+    double *smax;                    // damage-energy tracking: largest stretch of each concrete entry past s0, or null
     const double *X;
     double *xb0, *xb1;               // positions: step n reads xb[(n-1)&1], writes xb[n&1]
     double4 *xa0, *xa1;              // the same positions as (x, y, z, 0) per node: one 32-byte load per neighbour gather
@@ -494,6 +495,9 @@ __device__ BBPD_GENERAL_ATTR double3 entry_general(const Dev &d, int64_t e, uint
             L = (double)Lf;
         }
     }
+    // damage-energy tracking: every step in which a concrete bond's stretch
+    // exceeds s0 comes here (the fast path requires s <= s0)
+    if (d.smax && bt == 0 && s > s0b && s > d.smax[e]) d.smax[e] = s;
     // law and damage (calculatebsf*.m / calculatebondfailureMex.c)
     const double B0 = (sv & ST_DAMAGED) ? d.bsf[e] : 0.0;
     double B = B0;
@@ -1512,6 +1516,27 @@ __global__ void k_bond_gather(const IDX *__restrict__ ent, int64_t nB, const dou
             const uint8_t w = st[pos];
             out[k] = field == BBPD_FIELD_FLAG ? ((w & ST_SOFT) ? 1.0 : 0.0) : ((w & ST_BROKEN) ? 0.0 : 1.0);
         }
+    }
+}
+
+// calculatedamageenergy.m:34-62 for every bond from the largest stretch its
+// entries recorded (the energy is a non-decreasing function of the stretch, so
+// this equals the reference's running maximum over steps); bonds never past s0
+// have recorded 0 and get 0.
+template <class IDX, class CID>
+__global__ void k_bond_energy(const IDX *__restrict__ ent, int64_t nB, const double *__restrict__ smax,
+                              const CID *__restrict__ cid, const DictEntry *__restrict__ dict,
+                              const double *__restrict__ s0e, const double *__restrict__ sce, double s0, double sc,
+                              double shape, double den, double V2, double *out)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nB; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pos = (int64_t)ent[k];
+        const double s = smax[pos], a = s0e ? s0e[pos] : s0, c = sce ? sce[pos] : sc;
+        const DictEntry g = dict[cid[pos]];
+        double de = 0.0;
+        if ((a < s) && (s <= c)) de = (((((g.bs * a) * g.l0) * (a - s)) * shape) / den) * V2;
+        else if (s > c) de = (((((g.bs * a) * g.l0) * (a - c)) * shape) / den) * V2;
+        out[k] = de;
     }
 }
 
@@ -2782,6 +2807,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     d.halo_ptr = nullptr;
     d.halo = nullptr;
     d.s0e = d.s1e = d.sce = nullptr;
+    d.smax = nullptr;
     BBPD_CUDA_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
     if (prm->node_order == BBPD_ORDER_TILED) TRY(host_layout(S, pb, inv, fwd_ids, negid, dict, dictx, phase));
     else TRY(device_layout(S, pb, inv, fwd_ids, negid, phase));
@@ -3104,6 +3130,38 @@ extern "C" int bbpd_get(bbpd_solver *S, int field, double *out)
             }
         });
     }
+    if (field == BBPD_FIELD_DAMAGE_ENERGY) {
+        if (!S->d.smax) return fail(BBPD_ERR_ARG, "damage energy is not tracked (bbpd_track_damage_energy)");
+        if (nB == 0) return BBPD_OK;
+        TRY(upload_entry_map(S));
+        // calculatedamageenergy.m:36 and its shape factor, formed once with the host's exp
+        const double k = S->prm.k_exp, alpha = S->prm.alpha_exp, V = S->prm.cell_volume;
+        const double ek = std::exp(k);
+        const double den = 2 * k * (ek - 1) * (1 + alpha);
+        const double shape = (2 * k) - (2 * ek) + (alpha * k) - (alpha * k * ek) + 2;
+        const Dev &d = S->d;
+        const int blocks = (int)std::min<int64_t>((nB + 255) / 256, 148 * 32);
+        double *tmp = nullptr;
+        BBPD_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(double) * (size_t)nB, S->stream));
+        const void *ent = S->d_ent;
+        if (S->ent32 && !S->wide)
+            k_bond_energy<uint32_t, uint16_t><<<blocks, 256, 0, S->stream>>>((const uint32_t *)ent, nB, d.smax,
+                (const uint16_t *)d.cid, d.dict, d.s0e, d.sce, d.P.s0, d.P.sc, shape, den, V * V, tmp);
+        else if (S->ent32)
+            k_bond_energy<uint32_t, uint32_t><<<blocks, 256, 0, S->stream>>>((const uint32_t *)ent, nB, d.smax,
+                (const uint32_t *)d.cid, d.dict, d.s0e, d.sce, d.P.s0, d.P.sc, shape, den, V * V, tmp);
+        else if (!S->wide)
+            k_bond_energy<int64_t, uint16_t><<<blocks, 256, 0, S->stream>>>((const int64_t *)ent, nB, d.smax,
+                (const uint16_t *)d.cid, d.dict, d.s0e, d.sce, d.P.s0, d.P.sc, shape, den, V * V, tmp);
+        else
+            k_bond_energy<int64_t, uint32_t><<<blocks, 256, 0, S->stream>>>((const int64_t *)ent, nB, d.smax,
+                (const uint32_t *)d.cid, d.dict, d.s0e, d.sce, d.P.s0, d.P.sc, shape, den, V * V, tmp);
+        cudaError_t e = cudaGetLastError();
+        int rc = e == cudaSuccess ? BBPD_OK : fail(BBPD_ERR_CUDA, "damage energy: %s", cudaGetErrorString(e));
+        if (rc == BBPD_OK) rc = staging::download_copy(out, tmp, nB, S->stream);
+        cudaFreeAsync(tmp, S->stream);
+        return rc;
+    }
     if (field != BBPD_FIELD_BSF && field != BBPD_FIELD_FLAG && field != BBPD_FIELD_FAIL)
         return fail(BBPD_ERR_ARG, "unknown field %d", field);
     if (nB == 0) return BBPD_OK;
@@ -3206,6 +3264,20 @@ extern "C" int bbpd_set(bbpd_solver *S, int field, const double *in)
     cudaFreeAsync(tmp, S->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
     if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "set field %d: %s", field, cudaGetErrorString(e));
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_track_damage_energy(bbpd_solver *S)
+{
+    if (!S) return fail(BBPD_ERR_ARG, "null solver");
+    if (S->prm.law == BBPD_LAW_LINEAR)
+        return fail(BBPD_ERR_UNSUPPORTED, "damage energy is tracked for the softening laws only");
+    if (S->batch) TRY(batch_member_changed(S->batch));
+    BBPD_CUDA_TRY(cudaSetDevice(S->device));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    if (!S->d.smax) TRY(S->alloc(&S->d.smax, (size_t)S->ne));
+    BBPD_CUDA_TRY(cudaMemsetAsync(S->d.smax, 0, sizeof(double) * (size_t)std::max<int64_t>(S->ne, 1), S->stream));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));
     return BBPD_OK;
 }
 

@@ -131,6 +131,11 @@ class Solver:
         N.check(N.lib().bbpd_get_step(self._h, C.byref(st), C.byref(cn)))
         return float(cn.value)
 
+    def track_damage_energy(self) -> None:
+        """Record, from now on, what calculatedamageenergy.m needs at every step;
+        get("damage_energy") then returns the energy dissipated per bond."""
+        N.check(N.lib().bbpd_track_damage_energy(self._h))
+
     def set_step(self, step: int, cn: float = 0.0) -> None:
         N.check(N.lib().bbpd_set_step(self._h, step, cn))
 

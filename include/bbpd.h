@@ -449,7 +449,8 @@ enum { BBPD_FIELD_DISPLACEMENT = 0,  /* nodalDisplacement, nNodes x 3 */
        BBPD_FIELD_ACCELERATION = 5,  /* nodalAcceleration (Euler-Cromer) */
        BBPD_FIELD_BSF = 16,          /* bondSofteningFactor, nBonds */
        BBPD_FIELD_FLAG = 17,         /* flagBondSoftening, nBonds */
-       BBPD_FIELD_FAIL = 18          /* fail, nBonds */ };
+       BBPD_FIELD_FAIL = 18,         /* fail, nBonds */
+       BBPD_FIELD_DAMAGE_ENERGY = 19 /* damageEnergy, nBonds (after bbpd_track_damage_energy) */ };
 
 /* Copy a field to host memory (reference layout and node order). */
 int bbpd_get(bbpd_solver *s, int field, double *host_out);
@@ -457,6 +458,20 @@ int bbpd_get(bbpd_solver *s, int field, double *host_out);
  * FORCE_PREV included). Bond fields set both directed copies of each bond. */
 int bbpd_set(bbpd_solver *s, int field, const double *host_in);
 /* Next step to run (1-based) and last ADR damping coefficient. */
+/* replaces the per-step calculatedamageenergy.m call of the drivers
+ * (dynamicsolverdisplacementcontrolled.m:121, :34-62 of the function) for the
+ * fused solver. From this call on, every launch records the largest stretch
+ * of each concrete bond (BONDTYPE 0) once it exceeds s0, and
+ * bbpd_get(BBPD_FIELD_DAMAGE_ENERGY) returns the energy dissipated per bond:
+ * the formula evaluated at that stretch, which equals the reference's running
+ * maximum over steps because the energy never decreases with the stretch. k
+ * and alpha come from params.k_exp and params.alpha_exp (25 and 0.25, the
+ * values the drivers pass); other bonds report 0. Softening laws only (the
+ * linear law: BBPD_ERR_UNSUPPORTED). A second call starts the record afresh;
+ * the record takes 8 bytes per directed entry and is not part of a checkpoint.
+ * The FP32 form records its FP32 stretch outside the guard band. */
+int bbpd_track_damage_energy(bbpd_solver *s);
+
 int bbpd_get_step(bbpd_solver *s, int64_t *step, double *cn);
 int bbpd_set_step(bbpd_solver *s, int64_t step, double cn);
 

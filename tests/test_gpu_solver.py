@@ -221,6 +221,52 @@ def test_bad_bondlist_first_row_reported(medium, precision):
     assert "row 1234568 " in str(e.value), str(e.value)
 
 
+@pytest.mark.parametrize("law", ["trilinear", "bilinear", "exponential"])
+def test_damage_energy_tracking_vs_oracle(small, law):
+    """The fused solver's damage energy against the oracle's loop with
+    calculatedamageenergy.m applied to every step's stretch (the drivers'
+    order): bit-identical for the FP64 laws without exp, within 1e-9 relative
+    for the exponential law (CUDA's and glibc's exp may differ in the last bit)."""
+    kw = dict(LAWKW[law], scheme="adr", rate=-4e-6)
+    s = bb.Solver(small, **kw)
+    s.track_damage_energy()
+    r = po.Run(small, **kw)
+    nB = small["nBonds"]
+    s0 = np.full(nB, kw.get("s0", 1e-4))
+    sc = np.full(nB, kw["sc"])
+    E = np.zeros(nB)
+    bs, L0, V = small["BONDSTIFFNESS"], small["UNDEFORMEDLENGTH"], small["cellVolume"]
+    P = po.P
+    for step in range(90):
+        r.step(1)
+        st = r.get("stretch")
+        po.lib().orc_damageenergy(P(bs), P(s0), P(sc), P(L0), P(st), 25.0, 0.25, V, P(E), nB)
+    s.step(40)
+    s.step(50)
+    got = s.get("damage_energy")
+    assert (E > 0).any()
+    if law == "exponential":
+        np.testing.assert_allclose(got, E, rtol=1e-9, atol=1e-9 * np.abs(E).max())
+    else:
+        assert same(got, E)
+    s.track_damage_energy()                    # restart: nothing recorded yet
+    assert not s.get("damage_energy").any()
+    s.close()
+
+
+def test_damage_energy_tracking_rejections(small):
+    s = bb.Solver(small, **LAWKW["trilinear"], scheme="adr")
+    with pytest.raises(bb.BBPDError) as e:
+        s.get("damage_energy")
+    assert e.value.status == bb._native.ERR_ARG
+    s.close()
+    s = bb.Solver(small, **LAWKW["linear"], scheme="adr")
+    with pytest.raises(bb.BBPDError) as e:
+        s.track_damage_energy()
+    assert e.value.status == bb._native.ERR_UNSUPPORTED
+    s.close()
+
+
 def test_split_launches_identical(small):
     kw = dict(LAWKW["bilinear"], scheme="adr", rate=-2e-6)
     a, b = bb.Solver(small, **kw), bb.Solver(small, **kw)
