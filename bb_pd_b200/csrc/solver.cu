@@ -2088,15 +2088,16 @@ static int bad_bond_row(const double *bl, int64_t nB, int64_t k)
                 bl[nB + k]);
 }
 
-// Phases of bbpd_create, printed to stderr when BBPD_TIMING is set (each
-// phase then also waits for the device work it queued).
+// Phases of bbpd_create, printed to stderr when BBPD_TIMING is set; each
+// phase also waits for the device work it queued unless BBPD_TIMING=nosync.
 struct PhaseTimer {
     bool on = std::getenv("BBPD_TIMING") != nullptr;
+    bool sync = on && std::strcmp(std::getenv("BBPD_TIMING"), "nosync") != 0;
     std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
     void mark(const char *name)
     {
         if (!on) return;
-        cudaDeviceSynchronize();
+        if (sync) cudaDeviceSynchronize();
         const auto now = std::chrono::steady_clock::now();
         std::fprintf(stderr, "bbpd_create %-16s %8.1f ms\n", name,
                      std::chrono::duration<double, std::milli>(now - t).count());
