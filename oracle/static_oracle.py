@@ -3,9 +3,11 @@
 
 It follows solvers/scripts/static/newtonraphsondisplacementcontrolled.m:56-160:
 the prescribed DOFs move by the increment. Each Newton iteration then updates
-the bonds: calculatedeformedlength.m, the bilinear law of
-calculatebondsofteningfactor.m:159-165 (or no softening for the linear law),
-and calculatebondfailure with the law's sc. It forms the bond forces of
+the bonds: calculatedeformedlength.m, the law (the bilinear law of
+calculatebondsofteningfactor.m:159-165 restated here; the trilinear and
+exponential laws through the oracle's C routines orc_bsf_trilinear and
+orc_bsf_exponential; no softening for the linear law), and calculatebondfailure
+with the law's sc. It forms the bond forces of
 calculatebondforces.m:9-17 (BFMULTIPLIER included) and sums them over nodes in
 bond order (calculatenodalforces.m:25-35), times cellVolume (driver :111).
 The free nodes move by the solution of K delta = F, with K assembled as in
@@ -23,10 +25,12 @@ import scipy.sparse.linalg as spla
 
 class StaticOracle:
     def __init__(self, inp: dict, law: str = "bilinear", s0: float = 1e-4, sc: float = 2e-3,
-                 sc_steel: float = 1.0, failure_functionality: float = 0.0, cell_volume: float | None = None):
-        if law not in ("bilinear", "linear"):
-            raise ValueError("the oracle restates the bilinear and linear laws")
+                 sc_steel: float = 1.0, failure_functionality: float = 0.0, cell_volume: float | None = None,
+                 s1: float = 3e-4, beta_tri: float = 0.25, k_exp: float = 25.0, alpha_exp: float = 0.25):
+        if law not in ("bilinear", "linear", "trilinear", "exponential"):
+            raise ValueError("unknown law")
         self.law, self.s0, self.sc, self.sc_steel, self.ff = law, s0, sc, sc_steel, failure_functionality
+        self.s1, self.beta, self.k, self.alpha = s1, beta_tri, k_exp, alpha_exp
         self.n, self.nB = int(inp["nNodes"]), int(inp["nBonds"])
         self.V = float(cell_volume if cell_volume is not None else inp["cellVolume"])
         self.X = np.asfortranarray(inp["undeformedCoordinates"], dtype=np.float64)
@@ -65,6 +69,21 @@ class StaticOracle:
             B = np.where(B > 1, 1.0, B)
             B = np.where(np.isnan(B), 0.0, B)
             self.flag = f
+        elif self.law in ("trilinear", "exponential"):
+            from oracle import pyoracle as po
+            lib, P = po.lib(), po.P
+            s_c = np.ascontiguousarray(s)
+            B = np.ascontiguousarray(B.copy())
+            bt = np.ascontiguousarray(self.BT.astype(np.float64))
+            flag = np.ascontiguousarray(self.flag.copy())
+            s0a, s1a, sca = (np.array([v]) for v in (self.s0, self.s1, self.sc))
+            if self.law == "trilinear":
+                lib.orc_bsf_trilinear(P(s_c), P(s0a), 0, P(s1a), 0, P(sca), 0, self.beta, P(B), P(bt), P(flag), self.nB)
+            else:
+                scratch = np.zeros(self.nB)
+                lib.orc_bsf_exponential(P(s_c), P(s0a), 0, P(sca), 0, self.k, self.alpha, P(scratch), P(B), P(bt),
+                                      P(flag), self.nB)
+            self.flag = flag
         self.bsf = B
         fl = self.fail
         fl = np.where((fl == 1) & (self.BT == 0) & (s > self.sc), self.ff, fl)

@@ -109,3 +109,24 @@ def test_stiffness_triplets_vs_oracle(nod):
     for a, b in ((r, orr), (c, occ), (v, ov), (m, om)):
         assert np.array_equal(a, b)
     assert r.size <= (2 * nod) ** 2 * int(fail.sum())
+
+
+@pytest.mark.parametrize("law,steps", [("trilinear", 4), ("exponential", 3)])
+def test_static_other_laws_vs_oracle(law, steps):
+    """The static solver with the trilinear and exponential laws against the
+    oracle (its C law routines inside the restated Newton loop)."""
+    dx = 5e-3
+    inp = bb.beam.build(bb.beam.small(nx=24, ny=4, nz=8, notch_x=12.5 * dx, notch_depth=3.2 * dx))
+    kw = dict(law=law, s0=1e-4, sc=2e-3)
+    g = StaticSolver(inp, **kw)
+    o = StaticOracle(inp, **kw)
+    for step in range(steps):
+        sg = g.step(-1e-5, tol=1e-6, max_newton=60, **CG)
+        so = o.step(-1e-5, tol=1e-6, max_newton=60)
+        assert sg.converged and so["converged"], step
+        ug, uo = g.get("displacement"), o.get("displacement")
+        assert np.abs(ug - uo).max() <= 1e-6 * np.abs(uo).max(), step
+        assert same_flags(g.get("flag"), o.get("flag")), step
+        assert same_flags(g.get("fail"), o.get("fail")), step
+    assert g.get("flag").sum() > 100
+    g.close()
