@@ -129,3 +129,46 @@ def test_gpu_built_inputs_drive_the_solver():
     b.step(60)
     for f in ("displacement", "force", "bsf", "fail"):
         assert same(a.get(f), b.get(f)), f
+
+
+def test_device_pointer_forms_match_host_forms():
+    """bbpd_dev_buildhorizons / bbpd_dev_buildnotch on device arrays (torch
+    tensors in the reference layouts) give the host-pointer forms' results."""
+    import ctypes as C
+    import torch
+    L = bb._native.lib()
+    p, i64 = C.c_void_p, C.c_int64
+    L.bbpd_dev_buildhorizons.argtypes = [p, i64, C.c_double, i64, C.POINTER(i64), p, p, p, p, p, p]
+    L.bbpd_dev_buildnotch.argtypes = [p, i64, p, p, i64, C.c_double, C.c_double, C.c_double, C.POINTER(i64),
+                                      p, p, p, p, p, p]
+    dx = 5e-3
+    inp = bb.beam.build(bb.beam.small(nx=30, ny=5, nz=8))
+    X = inp["undeformedCoordinates"]
+    n = inp["nNodes"]
+    dev = torch.device("cuda:0")
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(dev)          # column-major n x 3
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    nb = C.c_int64()
+    nfam, fptr = torch.zeros(n, dtype=torch.float64, device=dev), torch.zeros(n, dtype=torch.float64, device=dev)
+    bb._native.check(L.bbpd_dev_buildhorizons(ptr(Xd), n, inp["horizon"], 0, C.byref(nb), ptr(nfam), ptr(fptr),
+                                              None, None, None, None))
+    m = nb.value
+    fam = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+    bl = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+    L0 = torch.zeros(m, dtype=torch.float64, device=dev)
+    bb._native.check(L.bbpd_dev_buildhorizons(ptr(Xd), n, inp["horizon"], m, C.byref(nb), None, None, ptr(fam),
+                                              ptr(bl), ptr(L0), None))
+    hn, hp, hf, hbl, hL = G.buildhorizons(X, inp["horizon"])
+    assert same(nfam.cpu().numpy(), hn) and same(fptr.cpu().numpy(), hp) and same(fam.cpu().numpy(), hf)
+    assert same(bl.cpu().numpy(), hbl.ravel(order="F")) and same(L0.cpu().numpy(), hL)
+    out_n = C.c_int64()
+    blo = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+    Lo = torch.zeros(m, dtype=torch.float64, device=dev)
+    nf2 = torch.zeros(n, dtype=torch.float64, device=dev)
+    bb._native.check(L.bbpd_dev_buildnotch(ptr(Xd), n, ptr(bl), ptr(L0), m, dx, 15.5, 3.7, C.byref(out_n), ptr(blo),
+                                           ptr(Lo), ptr(nf2), None, None, None))
+    k = out_n.value
+    hblo, hLo, hnf, _, _ = G.buildnotch(X, hbl, hL, dx, 15.5, 3.7)
+    assert k == hblo.shape[0] < m
+    assert same(blo.cpu().numpy()[:2 * k], hblo.ravel(order="F")) and same(Lo.cpu().numpy()[:k], hLo)
+    assert same(nf2.cpu().numpy(), hnf)
