@@ -951,7 +951,7 @@ __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, in
                 bad |= !isfinite(un[dof]) || !isfinite(vn[dof]);
                 far |= coord_out_of_range(xn3[dof]);
             }
-            b.xan[i] = make_double4(xn3[0], xn3[1], xn3[2], 0.0);
+            if (PREC != kP32X) b.xan[i] = make_double4(xn3[0], xn3[1], xn3[2], 0.0);   // FP64 gathers only
             if (PREC == kP32X) {
                 b.urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
                 b.urln[i] = make_float2(ul[1], ul[2]);
@@ -1031,7 +1031,7 @@ __device__ __forceinline__ void adr_update_slice(const Dev &d, const StepBufs &b
             bad |= !isfinite(un[dof]) || !isfinite(vn[dof]);
             far |= coord_out_of_range(xn3[dof]);
         }
-        b.xan[i] = make_double4(xn3[0], xn3[1], xn3[2], 0.0);
+        if (PREC != kP32X) b.xan[i] = make_double4(xn3[0], xn3[1], xn3[2], 0.0);   // FP64 gathers only
         if (PREC == kP32X) {
             b.urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
             b.urln[i] = make_float2(ul[1], ul[2]);
