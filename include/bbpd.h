@@ -37,7 +37,7 @@ typedef enum bbpd_status {
     BBPD_ERR_OOM = 3,          /* device allocation failed */
     BBPD_ERR_TIMEOUT = 4,      /* a device-side wait gave up (kernel returned early) */
     BBPD_ERR_NONFINITE = 5,    /* a displacement or velocity became NaN/Inf */
-    BBPD_ERR_UNSUPPORTED = 6,  /* valid input outside what this build implements */
+    BBPD_ERR_UNSUPPORTED = 6,  /* valid input outside what this library implements */
     BBPD_ERR_NO_DEVICE = 7     /* no CUDA device (this library has no CPU path) */
 } bbpd_status;
 
