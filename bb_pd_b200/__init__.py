@@ -9,11 +9,12 @@ This package is the host-side mirror of the reference's MATLAB calls:
     serving    continuous batching of beam solves under an HBM budget
     beam       synthetic beams like the reference's input scripts
     builder    the reference's input module (horizons, notch, bond data) on the GPU
+    static     the static (implicit) Newton-Raphson solver and the stiffness triplets
 """
-from . import _native, beam, builder, routines, serving
+from . import _native, beam, builder, routines, serving, static
 from ._native import BBPDError, device_count
 from .batch import Batch
 from .solver import Solver, make_params
 
-__all__ = ["Solver", "Batch", "make_params", "beam", "builder", "routines", "serving", "BBPDError", "device_count",
+__all__ = ["Solver", "Batch", "make_params", "beam", "builder", "routines", "static", "serving", "BBPDError", "device_count",
            "_native"]
