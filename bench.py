@@ -191,7 +191,11 @@ def run_batch(args):
     batch = bb.Batch(args.form)
     for s in sol:
         batch.add(s)
-    bps, grab = batch.tune(max(1, args.warmup // 3))
+    if args.batch_schedule:   # a fixed schedule instead of the autotuner (profiling one kernel)
+        bps, grab = (int(v) for v in args.batch_schedule.split(","))
+        batch.set_schedule(bps, grab)
+    else:
+        bps, grab = batch.tune(max(1, args.warmup // 3))
     batch.step(args.warmup)
     clocks = Clocks(0)
     clocks.start()
@@ -343,6 +347,7 @@ def main():
                          "persistent batch launch; serve: a Poisson stream of solves, continuous batching")
     ap.add_argument("--members", type=int, default=64, help="batch: beams in the size-effect series")
     ap.add_argument("--dx", type=float, default=5e-3, help="batch: lattice spacing of the series (m)")
+    ap.add_argument("--batch-schedule", default="", help="batch: 'blocks_per_sm,grab' instead of autotuning")
     ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")
     ap.add_argument("--max-nodes", type=float, default=3e5, help="serve: largest beam (nodes)")
     ap.add_argument("--arrival-hz", type=float, default=4.0, help="serve: Poisson arrival rate")
