@@ -7,7 +7,7 @@ Outputs (git-ignored, shipped with the source tree):
     bb_pd_b200/mex/<Name>.mexa64        one gateway per reference MEX routine,
                                         compiled against the stub mex.h here;
                                         with MATLAB, compile mex_gateways.c with
-                                        `mex` instead
+                                        `mex -DGW_<Name> mex_gateways.c -lbbpd`
 """
 from __future__ import annotations
 

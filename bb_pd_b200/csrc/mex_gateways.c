@@ -2,7 +2,7 @@
  * mexFunction gateways: drop-in replacements for the reference's MEX files.
  * Compile once per routine with -DGW_<Name> (bb_pd_b200/build.py does this
  * against the stub mex.h; with MATLAB: `mex -DGW_<Name> mex_gateways.c
- * -lbbpd`). Each gateway keeps the reference's argument
+ * -I<repo>/include -L<repo>/bb_pd_b200/lib -lbbpd`). Each gateway keeps the reference's argument
  * list, argument count check, size source (mxGetM of the same argument) and
  * in-place semantics, and calls libbbpd's host-pointer entry point, which runs
  * the routine on the GPU. Library errors become mexErrMsgTxt calls.

@@ -72,7 +72,7 @@ __device__ __forceinline__ double matlab_max(double a, double b)
     return (b > a) ? b : a;
 }
 
-// Bilinear softening, calculatebondsofteningfactor.m:159-165 for one bond.
+// Bilinear softening, calculatebondsofteningfactor.m:42-48 for one bond.
 __device__ __forceinline__ void law_bilinear(double s, double s0, double sc,
                                              bool concrete, double &BSF, bool &flag)
 {

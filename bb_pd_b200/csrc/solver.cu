@@ -994,7 +994,7 @@ __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, in
     }
 }
 
-// ADR phase B (timeintegrationADR.m:168-197) on the nodes of slice sb.
+// ADR phase B (timeintegrationADR.m:53-80) on the nodes of slice sb.
 template <int PREC>
 __device__ __forceinline__ void adr_update_slice(const Dev &d, const StepBufs &b, int64_t sb, int lane,
                                                  int64_t it)

@@ -42,7 +42,7 @@ typedef enum bbpd_status {
 } bbpd_status;
 
 enum { BBPD_LAW_LINEAR = 0,       /* brittle: calculatebondfailureMex.c:26-44 */
-       BBPD_LAW_BILINEAR = 1,     /* calculatebondsofteningfactor.m:159-165 */
+       BBPD_LAW_BILINEAR = 1,     /* calculatebondsofteningfactor.m:42-48 */
        BBPD_LAW_TRILINEAR = 2,    /* calculatebsftrilinear.m:80-112 */
        BBPD_LAW_EXPONENTIAL = 3   /* calculatebsfexponentialMex.c:26-66 */ };
 enum { BBPD_SCHEME_EULERCROMER = 0, BBPD_SCHEME_ADR = 1 };
@@ -190,7 +190,9 @@ int bbpd_calculatedampingcoefficient(const double *nodalForce,
  * synchronisation. Scratch is a fixed 256 KiB array per device inside the
  * library, so nNodes <= BBPD_DAMPING_NOALLOC_MAX_NODES (larger: BBPD_ERR_ARG).
  * The first call on each device looks up that array's address: make it before
- * any stream capture. Nothing needs zeroing beforehand. Calls that overlap on
+ * any stream capture. The address is kept for the life of the process, so
+ * after cudaDeviceReset on a device, unload and reload the library before the
+ * next call there. Nothing needs zeroing beforehand. Calls that overlap on
  * one device (unordered streams or host threads) race on the shared scratch. */
 #define BBPD_DAMPING_NOALLOC_MAX_NODES 16777216
 int bbpd_dev_calculatedampingcoefficient_noalloc(const double *nodalForce,

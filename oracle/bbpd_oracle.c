@@ -88,7 +88,7 @@ static double matlab_max(double a, double b)
     return (b > a) ? b : a;
 }
 
-/* calculatebondsofteningfactor.m:159-165 */
+/* calculatebondsofteningfactor.m:42-48 */
 void orc_bsf_bilinear(const double *s, const double *s0, int s0_stride,
                       const double *sc, int sc_stride, double *BSF,
                       const double *BT, double *flag, int64_t nBonds)
@@ -306,7 +306,7 @@ double orc_damping_coefficient_tree(const double *F, const double *m,
     return orc_cn_from_sums(cn1, cn2);
 }
 
-/* timeintegrationADR.m:168-197; vh and vhp may alias (element-wise update). */
+/* timeintegrationADR.m:53-80; vh and vhp may alias (element-wise update). */
 void orc_adr_integrate(int64_t iTimeStep, double dt, double *vh, const double *F,
                        const double *m, double cn, const double *vhp, double *u,
                        const double *CF, int64_t nN)

@@ -54,7 +54,7 @@ void orc_bsf_trilinear(const double *s, const double *s0, int s0_stride,
                        int sc_stride, double beta, double *BSF, const double *BT,
                        double *flag, int64_t nBonds);
 
-/* calculatebondsofteningfactor.m:159-165 (MATLAB only, bilinear). */
+/* calculatebondsofteningfactor.m:42-48 (MATLAB only, bilinear). */
 void orc_bsf_bilinear(const double *s, const double *s0, int s0_stride,
                       const double *sc, int sc_stride, double *BSF,
                       const double *BT, double *flag, int64_t nBonds);
@@ -112,7 +112,7 @@ double orc_cn_from_sums(double cn1, double cn2);
  * left. */
 double orc_tree_sum(const double *t, int64_t n);
 
-/* timeintegrationADR.m:168-197 (ADR central-difference half-step update). */
+/* timeintegrationADR.m:53-80 (ADR central-difference half-step update). */
 void orc_adr_integrate(int64_t iTimeStep, double dt, double *vh, const double *F,
                        const double *m, double cn, const double *vhp, double *u,
                        const double *CF, int64_t nNodes);

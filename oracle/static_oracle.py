@@ -4,7 +4,7 @@
 It follows solvers/scripts/static/newtonraphsondisplacementcontrolled.m:56-160:
 the prescribed DOFs move by the increment. Each Newton iteration then updates
 the bonds: calculatedeformedlength.m, the law (the bilinear law of
-calculatebondsofteningfactor.m:159-165 restated here; the trilinear and
+calculatebondsofteningfactor.m:42-48 restated here; the trilinear and
 exponential laws through the oracle's C routines orc_bsf_trilinear and
 orc_bsf_exponential; no softening for the linear law), and calculatebondfailure
 with the law's sc. It forms the bond forces of
