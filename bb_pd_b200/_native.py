@@ -21,7 +21,7 @@ LAW_LINEAR, LAW_BILINEAR, LAW_TRILINEAR, LAW_EXPONENTIAL = range(4)
 SCHEME_EULERCROMER, SCHEME_ADR = range(2)
 PREC_FP64, PREC_FP32 = range(2)
 AMP_LINEAR, AMP_SMOOTHSTEP = range(2)
-ORDER_INPUT, ORDER_MORTON, ORDER_TILED = range(3)
+ORDER_INPUT, ORDER_MORTON, ORDER_TILED, ORDER_LATTICE = range(4)
 FIELD = {"displacement": 0, "velocity": 1, "force": 2, "deformed": 3, "force_prev": 4,
          "acceleration": 5, "bsf": 16, "flag": 17, "fail": 18, "damage_energy": 19}
 LAWS = {"linear": LAW_LINEAR, "bilinear": LAW_BILINEAR, "trilinear": LAW_TRILINEAR,

@@ -71,6 +71,9 @@ constexpr int BT_SHIFT = 25;             // bits 25-26: BONDTYPE
 constexpr uint8_t ST_BROKEN = 1;         // fail == 0
 constexpr uint8_t ST_SOFT = 2;           // flagBondSoftening == 1
 constexpr uint8_t ST_DAMAGED = 4;        // BSF != +0.0 (BSF stored in bsf[])
+constexpr uint8_t ST_MASK = 7;           // the three state bits
+constexpr int LST_BT_SHIFT = 3;          // lattice form: bits 3-4 of the state byte hold BONDTYPE
+constexpr uint8_t LST_ABSENT = 0x80;     // lattice form: no bond in this slot
 constexpr int64_t MAX_NODES = (int64_t)1 << 24;
 
 constexpr int ERR_TIMEOUT = 1;
@@ -159,6 +162,16 @@ struct Dev {
     int pen_react[4];                // 1: force counts toward the reaction
     int64_t pen_off[5];              // family of cylinder p: contact entries [pen_off[p], pen_off[p+1])
     const int32_t *cidx;             // per node: its contact entry, or -1
+    // lattice form (lstep_kernel): bond slot f * n_nodes + lo holds the bond
+    // between node lo and node lo + offset f of the forward stencil
+    const int4 *ltab;                // per chain position: (partner offset in the staged box, f * n_nodes,
+                                     // offset of the slot's lower node from this node, 0)
+    int n_sigma;                     // chain positions, a multiple of 4
+    const uint64_t *lcpos;           // per node: chain positions opening an OpenMP chunk, 8 bits each, 0xFF none
+    int lnx, lny, lnz;               // lattice nodes per axis
+    int lty, ltz, lhalo;             // tile rows per y and z (a tile is 32 nodes long in x), stencil reach
+    int lsx, lsy, lsz;               // staged box per tile: (32 + 2 reach) x (lty + 2 reach) x (ltz + 2 reach)
+    int64_t ltiles[3];               // tiles per axis
     double *cforce;                  // per contact entry: z force of the step, two buffers by step parity
     double *pen_cz;                  // centre z of every cylinder, two buffers by step parity ([2][4])
     int64_t n_contact;
@@ -514,7 +527,9 @@ __device__ BBPD_GENERAL_ATTR double3 entry_general(const Dev &d, int64_t e, uint
         law_linear(s, scb, P, bt, failv);
     }
     const bool dmg = __double_as_longlong(B) != 0;
-    const uint32_t stn = (soft ? ST_SOFT : 0u) | (failv == 0.0 ? ST_BROKEN : 0u) | (dmg ? ST_DAMAGED : 0u);
+    // bits above the three state bits (the lattice form's BONDTYPE) are kept
+    const uint32_t stn = (soft ? ST_SOFT : 0u) | (failv == 0.0 ? ST_BROKEN : 0u) | (dmg ? ST_DAMAGED : 0u) |
+                         (sv & ~(uint32_t)ST_MASK);
     if (stn != sv) d.st[e] = (uint8_t)stn;
     if (__double_as_longlong(B) != __double_as_longlong(B0)) d.bsf[e] = B;
     // bond force (calculatebondforcesMex.c:34-40)
@@ -910,6 +925,88 @@ __device__ __forceinline__ void contact_reaction(const Dev &d, int64_t n, int64_
     if (it < d.react_cap) d.react[it] = r;
 }
 
+// Euler-Cromer (timeintegrationeulercromerMex.c:33-50) on node i once its
+// nodal force (tx, ty, tz) is summed.
+template <int PREC>
+__device__ __forceinline__ void ec_integrate_node(const Dev &d, const StepBufs &b, int64_t i, double tx,
+                                                  double ty, double tz, int64_t it)
+{
+    const int64_t nN = d.n_nodes;
+    const uint8_t fl = d.nflag[i];
+    const double Fv[3] = {tx, ty, tz};
+    double un[3], vn[3], xn3[3];
+#pragma unroll
+    for (int dof = 0; dof < 3; dof++) {
+        const int64_t e = i + nN * dof;
+        b.Fc[e] = Fv[dof];
+        double ae = (Fv[dof] - d.damping * d.v[e]) / d.rho[i];
+        if (fl & (1 << dof)) ae = 0;
+        double ve = d.v[e] + (ae * d.dt);
+        double ue = d.u[e] + (ve * d.dt);
+        double xe = d.X[e] + ue;
+        if (fl & (8 << dof)) { ue = b.Un1; xe = d.X[e] + ue; }
+        if (d.a) d.a[e] = ae;
+        un[dof] = ue; vn[dof] = ve; xn3[dof] = xe;
+    }
+    if (d.n_pen) apply_contact(d, b.n, i, un, vn, xn3);
+    if (d.n_probe) record_probes(d, it, i, un);
+    float uh[3], ul[3];
+    bool bad = false, far = false;
+#pragma unroll
+    for (int dof = 0; dof < 3; dof++) {
+        const int64_t e = i + nN * dof;
+        d.v[e] = vn[dof]; d.u[e] = un[dof]; b.xn[e] = xn3[dof];
+        uh[dof] = (float)un[dof]; ul[dof] = (float)(un[dof] - (double)uh[dof]);
+        bad |= !isfinite(un[dof]) || !isfinite(vn[dof]);
+        far |= coord_out_of_range(xn3[dof]);
+    }
+    if (PREC != kP32X) b.xan[i] = make_double4(xn3[0], xn3[1], xn3[2], 0.0);   // FP64 gathers only
+    if (PREC == kP32X) {
+        b.urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
+        b.urln[i] = make_float2(ul[1], ul[2]);
+    }
+    if (bad) atomicOr(d.err, ERR_NONFINITE);
+    if (far) atomicOr(d.sticky, 1u);
+}
+
+// ADR: calculatedampingcoefficient.m:61-85 terms of the nodes of slice sl
+// (lane's node has force tx, ty, tz) and their share of the reaction (force on
+// the prescribed DOFs), folded over the slice's 32 lanes by the xor butterfly
+// and entered into the tree.
+__device__ __forceinline__ void adr_slice_terms(const Dev &d, const StepBufs &b, int64_t sl, int lane,
+                                                double tx, double ty, double tz, int64_t it)
+{
+    const int64_t nN = d.n_nodes;
+    const int64_t i = sl * 32 + lane;
+    double c1 = 0, c2 = 0, c3 = 0;
+    if (i < nN) {
+        const double m = d.mass[i];
+        const double Fv[3] = {tx, ty, tz};
+        const uint8_t fl = d.nflag[i];
+#pragma unroll
+        for (int dof = 0; dof < 3; dof++)
+            if (fl & (8 << dof)) c3 = c3 + Fv[dof];
+#pragma unroll
+        for (int dof = 0; dof < 3; dof++) {
+            const int64_t e = i + nN * dof;
+            const double vhp = d.v[e], ue = d.u[e];
+            if (vhp != 0) c1 = c1 - ue * ue * ((Fv[dof] / m - b.Fp[e] / m) / (d.dt * vhp));
+        }
+#pragma unroll
+        for (int dof = 0; dof < 3; dof++) {
+            const double ue = d.u[i + nN * dof];
+            c2 = c2 + ue * ue;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
+        c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
+        c3 = c3 + __shfl_xor_sync(0xffffffffu, c3, off);
+    }
+    tree_publish(d, sl, lane, c1, c2, c3, it);
+}
+
 // Work on one slice after its nodal forces (tx, ty, tz of lane's node) are
 // summed: Euler-Cromer integrates the node; ADR stores F, forms the node's
 // Rayleigh-quotient terms, folds them over the slice and enters the tree.
@@ -921,76 +1018,10 @@ __device__ __forceinline__ void finish_slice(const Dev &d, const StepBufs &b, in
     const int64_t i = sl * 32 + lane;
     const bool valid = i < nN;
     if (SCHEME == BBPD_SCHEME_EULERCROMER) {
-        if (valid) {
-            // timeintegrationeulercromerMex.c:33-50 on the node just summed
-            const uint8_t fl = d.nflag[i];
-            const double Fv[3] = {tx, ty, tz};
-            double un[3], vn[3], xn3[3];
-#pragma unroll
-            for (int dof = 0; dof < 3; dof++) {
-                const int64_t e = i + nN * dof;
-                b.Fc[e] = Fv[dof];
-                double ae = (Fv[dof] - d.damping * d.v[e]) / d.rho[i];
-                if (fl & (1 << dof)) ae = 0;
-                double ve = d.v[e] + (ae * d.dt);
-                double ue = d.u[e] + (ve * d.dt);
-                double xe = d.X[e] + ue;
-                if (fl & (8 << dof)) { ue = b.Un1; xe = d.X[e] + ue; }
-                if (d.a) d.a[e] = ae;
-                un[dof] = ue; vn[dof] = ve; xn3[dof] = xe;
-            }
-            if (d.n_pen) apply_contact(d, b.n, i, un, vn, xn3);
-            if (d.n_probe) record_probes(d, it, i, un);
-            float uh[3], ul[3];
-            bool bad = false, far = false;
-#pragma unroll
-            for (int dof = 0; dof < 3; dof++) {
-                const int64_t e = i + nN * dof;
-                d.v[e] = vn[dof]; d.u[e] = un[dof]; b.xn[e] = xn3[dof];
-                uh[dof] = (float)un[dof]; ul[dof] = (float)(un[dof] - (double)uh[dof]);
-                bad |= !isfinite(un[dof]) || !isfinite(vn[dof]);
-                far |= coord_out_of_range(xn3[dof]);
-            }
-            if (PREC != kP32X) b.xan[i] = make_double4(xn3[0], xn3[1], xn3[2], 0.0);   // FP64 gathers only
-            if (PREC == kP32X) {
-                b.urhn[i] = make_float4(uh[0], uh[1], uh[2], ul[0]);
-                b.urln[i] = make_float2(ul[1], ul[2]);
-            }
-            if (bad) atomicOr(d.err, ERR_NONFINITE);
-            if (far) atomicOr(d.sticky, 1u);
-        }
+        if (valid) ec_integrate_node<PREC>(d, b, i, tx, ty, tz, it);
     } else {
-        // calculatedampingcoefficient.m:61-85 terms of this node and its share
-        // of the reaction (force on its prescribed DOFs), then the xor
-        // butterfly over the slice's 32 lanes
-        double c1 = 0, c2 = 0, c3 = 0;
-        if (valid) {
-            b.Fc[i] = tx; b.Fc[i + nN] = ty; b.Fc[i + 2 * nN] = tz;
-            const double m = d.mass[i];
-            const double Fv[3] = {tx, ty, tz};
-            const uint8_t fl = d.nflag[i];
-#pragma unroll
-            for (int dof = 0; dof < 3; dof++)
-                if (fl & (8 << dof)) c3 = c3 + Fv[dof];
-#pragma unroll
-            for (int dof = 0; dof < 3; dof++) {
-                const int64_t e = i + nN * dof;
-                const double vhp = d.v[e], ue = d.u[e];
-                if (vhp != 0) c1 = c1 - ue * ue * ((Fv[dof] / m - b.Fp[e] / m) / (d.dt * vhp));
-            }
-#pragma unroll
-            for (int dof = 0; dof < 3; dof++) {
-                const double ue = d.u[i + nN * dof];
-                c2 = c2 + ue * ue;
-            }
-        }
-#pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) {
-            c1 = c1 + __shfl_xor_sync(0xffffffffu, c1, off);
-            c2 = c2 + __shfl_xor_sync(0xffffffffu, c2, off);
-            c3 = c3 + __shfl_xor_sync(0xffffffffu, c3, off);
-        }
-        tree_publish(d, sl, lane, c1, c2, c3, it);
+        if (valid) { b.Fc[i] = tx; b.Fc[i + nN] = ty; b.Fc[i + 2 * nN] = tz; }
+        adr_slice_terms(d, b, sl, lane, tx, ty, tz, it);
     }
 }
 
@@ -1363,6 +1394,219 @@ __global__ void __launch_bounds__(kBlock, 2) tstep_kernel(Dev d, int64_t step0, 
         if (SCHEME == BBPD_SCHEME_ADR) {
             if (!grid_barrier(d)) return;
             adr_update<PREC>(d, b, lane, gwarp, nwarps, it);
+        }
+        if (!grid_barrier(d)) return;
+        if (d.n_pen && blockIdx.x == 0 && threadIdx.x == 0) contact_reaction(d, b.n, it);
+    }
+}
+
+// ---------------------------------------------------------------- lattice kernel
+//
+// Lattice form, for a regular lattice of nodes in x-fastest order (the order
+// of buildmaterialpointcoordinates.m:38-56) whose bond list gives every node
+// its bonds in one common order of stencil offsets (a bond list ordered by
+// its first node, each node's family in one order: what buildbonddata.m
+// builds on such a lattice). Neighbours are then addressed by the stencil, not
+// stored: each bond has one slot, slot = f * nN + lo for the bond from node lo
+// to node lo + f (f a forward stencil offset), holding a state byte (fail /
+// softening / damaged bits, BONDTYPE, "absent" for offsets that leave the
+// lattice or bonds that are not in the list) and a dictionary id, read by both
+// end nodes. Both ends compute bit-identical stretch and the same law update
+// from the same state, so either may store the new state; the update is
+// idempotent (max, or, and), so the other end computes the same force whether
+// it reads the state before or after the store.
+//
+// A block takes a tile of 32 x lty x ltz nodes, stages the positions of the
+// tile and of the stencil's reach around it in shared memory, and each warp
+// walks one row of 32 nodes, one lane per node. Lanes read their partners at
+// a fixed offset of their own staged position, so the 32 lanes read 32
+// consecutive doubles (no bank conflicts), and the slots of one chain position
+// are consecutive too (coalesced). Each node sums its entries in its bond-list
+// order, with the OpenMP chunk partials of calculatenodalforcesopenmpMex.c.
+// Euler-Cromer integrates each node in the tile; ADR stores the forces, and
+// the Rayleigh-quotient sums run over 32-node slices after a grid barrier, in
+// the same tree as the other kernels.
+
+// Forces of lane's node n (own: its index in the staged box).
+template <int LAW, bool SCE>
+__device__ __forceinline__ void lattice_forces(const Dev &d, int64_t n, bool valid, int own, bool safe,
+                                               const double *sx, const double *sy, const double *sz,
+                                               const int4 *stab, const DictEntry *sdict, int ncache,
+                                               double &tx, double &ty, double &tz)
+{
+    const int64_t nN = d.n_nodes;
+    const uint16_t *cids = reinterpret_cast<const uint16_t *>(d.cid);
+    const double xi = sx[own], yi = sy[own], zi = sz[own];
+    uint64_t cp = valid ? __ldg(d.lcpos + n) : ~0ull;
+    int nextc = (int)(cp & 0xFFu);
+    tx = 0.0; ty = 0.0; tz = 0.0;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    const int nsig = d.n_sigma;
+    // state bytes and dictionary ids of one group of 4 chain positions
+    uint32_t Sc[4], Cc[4], Sn[4], Cn[4];
+    auto fetch = [&](int g, uint32_t *S, uint32_t *Cd) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int4 t = stab[4 * g + q];
+            const int64_t lo = n + t.z;
+            const bool in = valid && (uint64_t)lo < (uint64_t)nN;
+            const int64_t slot = (int64_t)t.y + (in ? lo : 0);
+            S[q] = in ? (uint32_t)__ldcs(d.st + slot) : (uint32_t)LST_ABSENT;
+            Cd[q] = in ? (uint32_t)__ldcs(cids + slot) : 0u;
+        }
+    };
+    const int ng = nsig >> 2;
+    fetch(0, Sc, Cc);
+    for (int g = 0; g < ng; g++) {
+        if (g + 1 < ng) fetch(g + 1, Sn, Cn);
+        double fx[4], fy[4], fz[4];
+        unsigned slow = 0, pres = 0;
+        // pass 1: the fast path of the group's four entries, without branches
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int4 t = stab[4 * g + q];
+            const uint32_t sv = Sc[q];
+            const bool present = !(sv & LST_ABSENT);
+            const int p = own + t.x;
+            // absent entries get finite stand-ins for the branch-free pass
+            const double xj = present ? sx[p] : xi + 1.0;
+            const double yj = present ? sy[p] : yi;
+            const double zj = present ? sz[p] : zi;
+            const uint32_t c = Cc[q];
+            const DictEntry gd = ((int)c < ncache) ? sdict[c] : ldg_dict(d.dict, c);
+            const int64_t slot = (int64_t)t.y + n + t.z;
+            const double scv = SCE ? (present ? __ldcs(d.sce + slot) : d.P.sc) : d.P.sc;
+            const int bt = (sv >> LST_BT_SHIFT) & 3;
+            const double dX = xj - xi, dY = yj - yi, dZ = zj - zi;
+            const double L = sqrt(dX * dX + dY * dY + dZ * dZ);
+            const double s = quot_rn(L - gd.l0, gd.l0, gd.rl0);
+            bool okr;
+            const double rL = recip_rn(L, okr);
+            const bool fast = safe && okr && (sv & ST_MASK) == 0 && gd.rl0 > 0 && L > 0 &&
+                              law_quiet<LAW>(d.P, bt, s, d.P.s0, scv);
+            const double tt = ((gd.bs * s) * d.V) * gd.vcf;
+            fx[q] = tt * quot_rn(dX, L, rL);
+            fy[q] = tt * quot_rn(dY, L, rL);
+            fz[q] = tt * quot_rn(dZ, L, rL);
+            if (present) pres |= 1u << q;
+            if (present && !fast) slow |= 1u << q;
+        }
+        // pass 2: the rare general entries, and the sum in the reference's order
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (pres & (1u << q)) {
+                const int sig = 4 * g + q;
+                double3 r = make_double3(fx[q], fy[q], fz[q]);
+                if (slow & (1u << q)) {
+                    const int4 t = stab[sig];
+                    const int64_t slot = (int64_t)t.y + n + t.z;
+                    const uint32_t sv = Sc[q];
+                    const int p = own + t.x;
+                    const double scv = SCE ? __ldcs(d.sce + slot) : d.P.sc;
+                    const uint32_t w = ((sv >> LST_BT_SHIFT) & 3u) << BT_SHIFT;
+                    r = entry_general<LAW, kP64>(d, slot, w, sv, ldg_dict(d.dict, Cc[q]), scv, xi, yi, zi,
+                                                 sx[p], sy[p], sz[p]);
+                }
+                if (sig == nextc) {   // partial of the previous OpenMP thread is complete
+                    tx = tx + ax; ty = ty + ay; tz = tz + az;
+                    ax = 0.0; ay = 0.0; az = 0.0;
+                    cp >>= 8;
+                    nextc = (int)(cp & 0xFFu);
+                }
+                ax = ax + r.x; ay = ay + r.y; az = az + r.z;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) { Sc[q] = Sn[q]; Cc[q] = Cn[q]; }
+    }
+    tx = tx + ax; ty = ty + ay; tz = tz + az;
+}
+
+// Dynamic shared memory: the dictionary cache (ncache entries of 32 bytes),
+// the chain table (n_sigma int4) and the staged positions of one tile (x, y, z
+// arrays over the lsx * lsy * lsz box).
+template <int LAW, int SCHEME, bool SCE>
+__global__ void __launch_bounds__(kBlock, 2) lstep_kernel(Dev d, int64_t step0, int64_t nsteps)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int64_t s_tile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nN = d.n_nodes, nsl = d.n_slices;
+    const int ncache = d.ncache, nsig = d.n_sigma;
+    const int sxn = d.lsx, syn = d.lsy, szn = d.lsz, H = d.lhalo;
+    const int box = sxn * syn * szn;
+    const int64_t ntx = d.ltiles[0], nty = d.ltiles[1], ntiles = d.ltiles[0] * d.ltiles[1] * d.ltiles[2];
+
+    DictEntry *sdict = reinterpret_cast<DictEntry *>(smem);
+    int4 *stab = reinterpret_cast<int4 *>(smem + (size_t)32 * ncache);
+    double *sx = reinterpret_cast<double *>(stab + nsig), *sy = sx + box, *sz = sy + box;
+
+    for (int c = threadIdx.x; c < ncache; c += blockDim.x) sdict[c] = ldg_dict(d.dict, c);
+    for (int c = threadIdx.x; c < nsig; c += blockDim.x) stab[c] = d.ltab[c];
+
+    // this warp's row in a tile
+    const int wy = warp % d.lty, wz = warp / d.lty;
+    const bool wrow = warp < d.lty * d.ltz;
+    const int own = (lane + H) + sxn * ((wy + H) + syn * (wz + H));
+
+    for (int64_t it = 0; it < nsteps; it++) {
+        const StepBufs b = step_bufs(d, step0 + it);
+        const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
+        if (d.n_pen && blockIdx.x == 0 && threadIdx.x == 0) contact_advance(d, b.n);
+        // tiles from a shared counter; each block stops at its first grab past
+        // the last tile, so a step uses exactly ntiles + gridDim.x values
+        const int64_t base = it * (ntiles + gridDim.x);
+        for (;;) {
+            __syncthreads();   // the previous tile's positions are no longer read
+            if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(d.work, 1ull) - base;
+            __syncthreads();
+            const int64_t tile = s_tile;
+            if (tile >= ntiles) break;
+            const int64_t tz0 = tile / (ntx * nty), rem = tile - tz0 * ntx * nty;
+            const int64_t ty0 = rem / ntx, tx0 = rem - ty0 * ntx;
+            const int x0 = (int)tx0 * 32, y0 = (int)ty0 * d.lty, z0 = (int)tz0 * d.ltz;
+            // stage the tile and its reach; points outside the lattice hold 0
+            for (int l = threadIdx.x; l < box; l += blockDim.x) {
+                const int bz = l / (sxn * syn), r2 = l - bz * sxn * syn;
+                const int by = r2 / sxn, bx = r2 - by * sxn;
+                const int gx = x0 - H + bx, gy = y0 - H + by, gz = z0 - H + bz;
+                double px = 0.0, py = 0.0, pz = 0.0;
+                if (gx >= 0 && gx < d.lnx && gy >= 0 && gy < d.lny && gz >= 0 && gz < d.lnz) {
+                    const int64_t g = gx + (int64_t)d.lnx * (gy + (int64_t)d.lny * gz);
+                    px = b.xs[g]; py = b.xs[g + nN]; pz = b.xs[g + 2 * nN];
+                }
+                sx[l] = px; sy[l] = py; sz[l] = pz;
+            }
+            __syncthreads();
+            if (wrow) {
+                const int gx = x0 + lane, gy = y0 + wy, gz = z0 + wz;
+                const bool valid = gx < d.lnx && gy < d.lny && gz < d.lnz;
+                const int64_t n = valid ? gx + (int64_t)d.lnx * (gy + (int64_t)d.lny * gz) : 0;
+                double tx, ty, tz;
+                lattice_forces<LAW, SCE>(d, n, valid, own, safe, sx, sy, sz, stab, sdict, ncache, tx, ty, tz);
+                if (valid) {
+                    if (SCHEME == BBPD_SCHEME_EULERCROMER) {
+                        ec_integrate_node<kP64>(d, b, n, tx, ty, tz, it);
+                    } else {
+                        b.Fc[n] = tx; b.Fc[n + nN] = ty; b.Fc[n + 2 * nN] = tz;
+                    }
+                }
+            }
+        }
+        if (SCHEME == BBPD_SCHEME_ADR) {
+            if (!grid_barrier(d)) return;
+            // Rayleigh-quotient terms over 32-node slices, in the tree order
+            // of the other kernels
+            for (int64_t sl = gwarp; sl < nsl; sl += nwarps) {
+                const int64_t i = sl * 32 + lane;
+                double fx = 0, fy = 0, fz = 0;
+                if (i < nN) { fx = b.Fc[i]; fy = b.Fc[i + nN]; fz = b.Fc[i + 2 * nN]; }
+                adr_slice_terms(d, b, sl, lane, fx, fy, fz, it);
+            }
+            if (!grid_barrier(d)) return;
+            adr_update<kP64>(d, b, lane, gwarp, nwarps, it);
         }
         if (!grid_barrier(d)) return;
         if (d.n_pen && blockIdx.x == 0 && threadIdx.x == 0) contact_reaction(d, b.n, it);
@@ -1769,6 +2013,24 @@ kernel_t pick_tkernel(int law, int scheme, int prec, bool sce)
     }
 }
 
+template <int LAW>
+kernel_t pick_lscheme(int scheme, bool sce)
+{
+    if (scheme == BBPD_SCHEME_ADR) return sce ? lstep_kernel<LAW, BBPD_SCHEME_ADR, true> : lstep_kernel<LAW, BBPD_SCHEME_ADR, false>;
+    return sce ? lstep_kernel<LAW, BBPD_SCHEME_EULERCROMER, true> : lstep_kernel<LAW, BBPD_SCHEME_EULERCROMER, false>;
+}
+
+// Lattice form: FP64, 16-bit dictionary ids.
+kernel_t pick_lkernel(int law, int scheme, bool sce)
+{
+    switch (law) {
+    case BBPD_LAW_LINEAR: return pick_lscheme<BBPD_LAW_LINEAR>(scheme, sce);
+    case BBPD_LAW_BILINEAR: return pick_lscheme<BBPD_LAW_BILINEAR>(scheme, sce);
+    case BBPD_LAW_TRILINEAR: return pick_lscheme<BBPD_LAW_TRILINEAR>(scheme, sce);
+    default: return pick_lscheme<BBPD_LAW_EXPONENTIAL>(scheme, sce);
+    }
+}
+
 kernel_t pick_kernel(int law, int scheme, int prec, bool wide, bool sce)
 {
     switch (law) {
@@ -2008,6 +2270,7 @@ struct bbpd_solver {
     kernel_t kernel = nullptr;
     int grid = 0;
     bool tiled = false;                 // tiled kernel with shared-memory staging
+    bool lattice = false;               // lattice form (lstep_kernel)
     size_t smem = 0;                    // its dynamic shared memory per block
     bbpd_batch *batch = nullptr;        // batch this solver is a member of
     bool has_density = false;          // DENSITY given (contact needs it)
@@ -2547,6 +2810,336 @@ static int device_layout(bbpd_solver *S, const bbpd_problem *pb, const int32_t *
     return BBPD_OK;
 }
 
+// ---- lattice form: bond slots (see lstep_kernel) ----
+
+// Bond k into its slot: state byte (fail, BONDTYPE), dictionary id, per-bond
+// critical stretch; slot_bond records which bond a slot holds.
+__global__ void k_lattice_scatter(int64_t nB, const uint32_t *__restrict__ slot, const uint8_t *__restrict__ bflag,
+                                  const uint16_t *__restrict__ bcid, const double *__restrict__ bsc, uint8_t *st,
+                                  uint16_t *cid, double *sce, uint32_t *slot_bond)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nB; k += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t q = slot[k];
+        if (slot_bond) slot_bond[q] = (uint32_t)k;
+        if (st) st[q] = bflag ? bflag[k] : (uint8_t)0;
+        if (cid) cid[q] = bcid[k];
+        if (sce) sce[q] = bsc[k];
+    }
+}
+
+// Chain positions of node n whose entry opens a new OpenMP chunk of the
+// nodal-force loop (the chunk of its bond differs from that of the node's
+// previous entry), packed 8 bits each; *overflow when a node has more than 8.
+__global__ void k_lattice_chunks(int64_t nN, int nsig, const int4 *__restrict__ tab,
+                                 const uint32_t *__restrict__ slot_bond, int64_t nB, int T, uint64_t *cpos,
+                                 int *overflow)
+{
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nN; n += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t packed = ~0ull;
+        int cnt = 0, prev = -1;
+        for (int sig = 0; sig < nsig; sig++) {
+            const int4 t = tab[sig];
+            const int64_t lo = n + t.z;
+            if ((uint64_t)lo >= (uint64_t)nN) continue;
+            const uint32_t k = slot_bond[(int64_t)t.y + lo];
+            if (k == 0xFFFFFFFFu) continue;
+            const int c = omp_chunk_of((int64_t)k, nB, T);
+            if (prev >= 0 && c != prev) {
+                if (cnt == 8) {
+                    atomicOr(overflow, 1);
+                } else {
+                    packed = (packed & ~(0xFFull << (8 * cnt))) | ((uint64_t)sig << (8 * cnt));
+                    cnt++;
+                }
+            }
+            prev = c;
+        }
+        cpos[n] = packed;
+    }
+}
+
+// Lattice form (BBPD_ORDER_LATTICE). Builds the bond slots when the input is a
+// regular lattice in x-fastest order (coordinates bit-equal along every lattice
+// row, column and plane) whose bond list is ordered by its first node, with
+// the second node after the first and every node's family in one common order
+// of stencil offsets; S->lattice stays false otherwise, and nothing is built.
+template <class FwdIds>
+static int lattice_layout(bbpd_solver *S, const bbpd_problem *pb, FwdIds fwd_ids, std::vector<DictEntry> &dict,
+                          PhaseTimer &phase)
+{
+    S->lattice = false;
+    const bbpd_params *prm = &S->prm;
+    const int64_t nN = S->nN, nB = S->nB;
+    if (S->prec != kP64 || S->wide || pb->s0 || pb->s1 || nB == 0 || dict.size() > 65535) return BBPD_OK;
+    const double *X = pb->undeformed_coordinates, *Y = X + nN, *Z = X + 2 * nN;
+    int64_t nx = 1;
+    while (nx < nN && X[nx] > X[nx - 1]) nx++;
+    int64_t ny = 1;
+    while (ny * nx < nN && Y[ny * nx] > Y[(ny - 1) * nx]) ny++;
+    if (nN % (nx * ny)) return BBPD_OK;
+    const int64_t nz = nN / (nx * ny), pl = nx * ny;
+    if (nx > 32767 || ny > 32767 || nz > 32767) return BBPD_OK;
+    for (int64_t c = 1; c < nz; c++)
+        if (!(Z[c * pl] > Z[(c - 1) * pl])) return BBPD_OK;
+    const int HT = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nB / 65536));
+    {
+        std::atomic<bool> ok(true);
+        host_ranges(nN, HT, [&](int, int64_t lo, int64_t hi) {
+            for (int64_t n = lo; n < hi && ok.load(std::memory_order_relaxed); n++) {
+                const int64_t a = n % nx, b = (n / nx) % ny, c = n / pl;
+                if (bits_of(X[n]) != bits_of(X[a]) || bits_of(Y[n]) != bits_of(Y[b * nx]) ||
+                    bits_of(Z[n]) != bits_of(Z[c * pl]))
+                    ok = false;
+            }
+        });
+        if (!ok) return BBPD_OK;
+    }
+    // pass 1 over the bonds: rows, order, stencil offsets (|component| <= 4)
+    const double *bl = pb->bondlist;
+    constexpr int KR = 4, KW = 2 * KR + 1, NKEY = KW * KW * KW;
+    auto grid_off = [&](int64_t i, int64_t j, int &ox, int &oy, int &oz) {
+        ox = (int)(j % nx - i % nx);
+        oy = (int)((j / nx) % ny - (i / nx) % ny);
+        oz = (int)(j / pl - i / pl);
+    };
+    std::vector<std::vector<char>> seen(HT, std::vector<char>(NKEY, 0));
+    std::atomic<int64_t> bad_row(nB);
+    std::atomic<bool> lat(true);
+    host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
+        for (int64_t k = lo; k < hi; k++) {
+            if (!bond_row_ok(bl, nB, nN, k)) {
+                int64_t cur = bad_row.load();
+                while (k < cur && !bad_row.compare_exchange_weak(cur, k)) {
+                }
+                return;
+            }
+            const int64_t i = (int64_t)bl[k] - 1, j = (int64_t)bl[nB + k] - 1;
+            if (j <= i || (k > 0 && bl[k] < bl[k - 1])) { lat = false; return; }
+            int ox, oy, oz;
+            grid_off(i, j, ox, oy, oz);
+            if (std::abs(ox) > KR || std::abs(oy) > KR || std::abs(oz) > KR) { lat = false; return; }
+            seen[t][(ox + KR) + KW * ((oy + KR) + KW * (oz + KR))] = 1;
+        }
+    });
+    if (bad_row.load() < nB) return bad_bond_row(bl, nB, bad_row.load());
+    if (!lat) return BBPD_OK;
+    std::vector<int> fidx_of(NKEY, -1);
+    std::vector<int3> foff;
+    for (int key = 0; key < NKEY; key++) {
+        bool any = false;
+        for (int t = 0; t < HT; t++) any |= seen[t][key] != 0;
+        if (!any) continue;
+        fidx_of[key] = (int)foff.size();
+        foff.push_back(make_int3(key % KW - KR, (key / KW) % KW - KR, key / (KW * KW) - KR));
+    }
+    const int NF = (int)foff.size();
+    if (NF > 64 || (int64_t)NF * nN >= ((int64_t)1 << 31)) return BBPD_OK;
+    // pass 2: forward offset index per bond, order of offsets within families
+    // (an edge a -> b when b follows a in some family), dictionary id use
+    std::unique_ptr<uint8_t[]> bf(new uint8_t[nB]);
+    std::vector<std::vector<uint64_t>> edge(HT, std::vector<uint64_t>(NF, 0));
+    std::vector<std::vector<uint32_t>> use(HT, std::vector<uint32_t>(dict.size(), 0));
+    std::unique_ptr<uint16_t[]> bcid(new uint16_t[nB]);
+    host_ranges(nB, HT, [&](int t, int64_t lo, int64_t hi) {
+        fwd_ids(lo, hi - lo, bcid.get() + lo);
+        for (int64_t k = lo; k < hi; k++) {
+            const int64_t i = (int64_t)bl[k] - 1, j = (int64_t)bl[nB + k] - 1;
+            int ox, oy, oz;
+            grid_off(i, j, ox, oy, oz);
+            bf[k] = (uint8_t)fidx_of[(ox + KR) + KW * ((oy + KR) + KW * (oz + KR))];
+            use[t][bcid[k]]++;
+        }
+        for (int64_t k = std::max<int64_t>(lo, 1); k < hi; k++) {
+            if (bl[k] != bl[k - 1]) continue;
+            const int64_t i = (int64_t)bl[k] - 1;
+            int ox, oy, oz;
+            grid_off(i, (int64_t)bl[nB + k - 1] - 1, ox, oy, oz);
+            const int a = fidx_of[(ox + KR) + KW * ((oy + KR) + KW * (oz + KR))];
+            grid_off(i, (int64_t)bl[nB + k] - 1, ox, oy, oz);
+            const int b = fidx_of[(ox + KR) + KW * ((oy + KR) + KW * (oz + KR))];
+            edge[t][a] |= 1ull << b;
+        }
+    });
+    // family order: a topological order of the offsets (smallest index first
+    // among the free ones); a cycle, or an offset twice in one family (a
+    // self-edge), means no common order
+    std::vector<uint64_t> E(NF, 0);
+    for (int t = 0; t < HT; t++)
+        for (int a = 0; a < NF; a++) E[a] |= edge[t][a];
+    std::vector<int> indeg(NF, 0), pi;
+    for (int a = 0; a < NF; a++) {
+        if (E[a] >> a & 1) return BBPD_OK;
+        for (int b = 0; b < NF; b++)
+            if (E[a] >> b & 1) indeg[b]++;
+    }
+    std::vector<char> done(NF, 0);
+    for (int r = 0; r < NF; r++) {
+        int pick = -1;
+        for (int a = 0; a < NF && pick < 0; a++)
+            if (!done[a] && indeg[a] == 0) pick = a;
+        if (pick < 0) return BBPD_OK;
+        done[pick] = 1;
+        pi.push_back(pick);
+        for (int b = 0; b < NF; b++)
+            if (E[pick] >> b & 1) indeg[b]--;
+    }
+    // chain order: the bonds to lower nodes by ascending partner (the list is
+    // ordered by first node), then the node's own family in family order
+    int H = 0;
+    for (const int3 &f : foff) H = std::max({H, std::abs(f.x), std::abs(f.y), std::abs(f.z)});
+    // tile shape: 32 x ty x tz with ty * tz = 8 rows, least padding
+    int bty = 4, btz = 2;
+    {
+        int64_t best = -1;
+        const int cand[4][2] = {{4, 2}, {8, 1}, {2, 4}, {1, 8}};
+        for (auto &c : cand) {
+            const int64_t pad = ((ny + c[0] - 1) / c[0]) * c[0] * ((nz + c[1] - 1) / c[1]) * c[1];
+            if (best < 0 || pad < best) { best = pad; bty = c[0]; btz = c[1]; }
+        }
+    }
+    const int lsx = 32 + 2 * H, lsy = bty + 2 * H, lsz = btz + 2 * H;
+    auto lin = [&](const int3 &f) { return (int64_t)f.x + nx * ((int64_t)f.y + ny * (int64_t)f.z); };
+    std::vector<int> back(NF);
+    std::iota(back.begin(), back.end(), 0);
+    std::sort(back.begin(), back.end(), [&](int a, int b) { return lin(foff[a]) > lin(foff[b]); });
+    std::vector<int4> tab;
+    for (int a : back) {
+        const int3 &f = foff[a];
+        tab.push_back(make_int4(-(f.x + lsx * (f.y + lsy * f.z)), a * (int)nN, (int)-lin(f), 0));
+    }
+    for (int a : pi) {
+        const int3 &f = foff[a];
+        tab.push_back(make_int4(f.x + lsx * (f.y + lsy * f.z), a * (int)nN, 0, 0));
+    }
+    while (tab.size() % 4) tab.push_back(make_int4(0, 0, -(1 << 30), 0));   // padding: never present
+    const int nsig = (int)tab.size();
+    if (nsig > 255) return BBPD_OK;
+    // shared memory: positions of the staged box, the chain table, and as many
+    // of the most used dictionary entries as fit two blocks per SM
+    const size_t box = (size_t)lsx * lsy * lsz;
+    const size_t fixed = 24 * box + 16 * (size_t)nsig;
+    const size_t budget = 110 * 1024;
+    if (fixed > budget) return BBPD_OK;
+    const int ncache = (int)std::min<size_t>({(size_t)kDictCache, dict.size(), (budget - fixed) / 32});
+    // dictionary renumbered by use, most used first (those are cached)
+    std::vector<uint32_t> cnt(dict.size(), 0);
+    for (int t = 0; t < HT; t++)
+        for (size_t c = 0; c < dict.size(); c++) cnt[c] += use[t][c];
+    std::vector<uint32_t> order(dict.size());
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
+    std::vector<uint16_t> remap(dict.size());
+    {
+        std::vector<DictEntry> nd(dict.size());
+        for (size_t q = 0; q < order.size(); q++) {
+            remap[order[q]] = (uint16_t)q;
+            nd[q] = dict[order[q]];
+        }
+        dict.swap(nd);
+    }
+    phase.mark("lattice check");
+
+    // staged per-bond data, chunk positions, then the slots
+    cudaStream_t st = S->stream;
+    Dev &d = S->d;
+    keep_layout_pool(S->device);
+    TempBufs tmp(st);
+    const int64_t NS = (int64_t)NF * nN;
+    uint32_t *slot = nullptr, *slot_bond = nullptr;
+    TRY(tmp.get(&slot, (size_t)nB));
+    TRY(staging::upload(slot, nB, st, [&](int64_t k0, int64_t c, uint32_t *out) {
+        for (int64_t q = 0; q < c; q++) {
+            const int64_t k = k0 + q;
+            out[q] = (uint32_t)((int64_t)bf[k] * nN + (int64_t)bl[k] - 1);
+        }
+    }));
+    TRY(tmp.get(&slot_bond, (size_t)NS));
+    BBPD_CUDA_TRY(cudaMemsetAsync(slot_bond, 0xFF, sizeof(uint32_t) * NS, st));
+    k_lattice_scatter<<<grid_for(nB), 256, 0, st>>>(nB, slot, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                    slot_bond);
+    BBPD_CUDA_TRY(cudaGetLastError());
+    int4 *dtab = nullptr;
+    TRY(tmp.get(&dtab, tab.size()));
+    BBPD_CUDA_TRY(cudaMemcpyAsync(dtab, tab.data(), sizeof(int4) * tab.size(), cudaMemcpyHostToDevice, st));
+    uint64_t *cpos = nullptr;
+    TRY(tmp.get(&cpos, (size_t)nN));
+    int *over = nullptr;
+    TRY(tmp.get(&over, 1));
+    BBPD_CUDA_TRY(cudaMemsetAsync(over, 0, sizeof(int), st));
+    k_lattice_chunks<<<grid_for(nN), 256, 0, st>>>(nN, nsig, dtab, slot_bond, nB, prm->n_chunks, cpos, over);
+    BBPD_CUDA_TRY(cudaGetLastError());
+    int hover = 0;
+    BBPD_CUDA_TRY(cudaMemcpyAsync(&hover, over, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(st));
+    if (hover) return BBPD_OK;   // more than 8 chunk starts in some list (many OpenMP chunks)
+
+    uint8_t *bflag = nullptr;
+    if (pb->fail || pb->bond_type) {
+        TRY(tmp.get(&bflag, (size_t)nB));
+        const double *fl = pb->fail, *btp = pb->bond_type;
+        TRY(staging::upload(bflag, nB, st, [&](int64_t k0, int64_t c, uint8_t *out) {
+            for (int64_t q = 0; q < c; q++) {
+                const int64_t k = k0 + q;
+                out[q] = (uint8_t)((fl && fl[k] == 0 ? ST_BROKEN : 0) | (btp ? (int)btp[k] << LST_BT_SHIFT : 0));
+            }
+        }));
+    }
+    uint16_t *dcid = nullptr;
+    TRY(tmp.get(&dcid, (size_t)nB));
+    TRY(staging::upload(dcid, nB, st, [&](int64_t k0, int64_t c, uint16_t *out) {
+        for (int64_t q = 0; q < c; q++) out[q] = remap[bcid[k0 + q]];
+    }));
+    double *dsc = nullptr;
+    if (pb->sc) {
+        TRY(tmp.get(&dsc, (size_t)nB));
+        TRY(staging::upload_copy(dsc, pb->sc, nB, st));
+    }
+    // from here on the lattice form is committed: its arrays belong to the solver
+    int4 *ltab = nullptr;
+    TRY(S->put(&ltab, tab));
+    d.ltab = ltab;
+    uint64_t *lcpos = nullptr;
+    TRY(S->alloc(&lcpos, (size_t)nN));
+    BBPD_CUDA_TRY(cudaMemcpyAsync(lcpos, cpos, sizeof(uint64_t) * nN, cudaMemcpyDeviceToDevice, st));
+    d.lcpos = lcpos;
+    TRY(S->alloc(&d.st, (size_t)NS));
+    BBPD_CUDA_TRY(cudaMemsetAsync(d.st, LST_ABSENT, (size_t)NS, st));
+    uint16_t *lcid = nullptr;
+    TRY(S->alloc(&lcid, (size_t)NS));
+    BBPD_CUDA_TRY(cudaMemsetAsync(lcid, 0, 2 * (size_t)NS, st));
+    d.cid = lcid;
+    TRY(S->alloc(&d.bsf, (size_t)NS));
+    BBPD_CUDA_TRY(cudaMemsetAsync(d.bsf, 0, 8 * (size_t)NS, st));
+    if (pb->sc) {
+        TRY(S->alloc((double **)&d.sce, (size_t)NS));
+        k_fill<<<grid_for(NS), 256, 0, st>>>((double *)d.sce, NS, prm->sc);
+        BBPD_CUDA_TRY(cudaGetLastError());
+    }
+    k_lattice_scatter<<<grid_for(nB), 256, 0, st>>>(nB, slot, bflag, dcid, dsc, d.st, lcid, (double *)d.sce,
+                                                    nullptr);
+    BBPD_CUDA_TRY(cudaGetLastError());
+    // bond -> slot map for per-bond gets and sets (both "copies" are the slot)
+    S->ent32 = true;
+    TRY(S->alloc((uint32_t **)&S->d_ent, (size_t)(2 * nB)));
+    BBPD_CUDA_TRY(cudaMemcpyAsync(S->d_ent, slot, sizeof(uint32_t) * nB, cudaMemcpyDeviceToDevice, st));
+    BBPD_CUDA_TRY(cudaMemcpyAsync((uint32_t *)S->d_ent + nB, slot, sizeof(uint32_t) * nB, cudaMemcpyDeviceToDevice, st));
+    BBPD_CUDA_TRY(cudaStreamSynchronize(st));
+
+    S->ne = NS;
+    S->lattice = true;
+    d.n_sigma = nsig;
+    d.lnx = (int)nx; d.lny = (int)ny; d.lnz = (int)nz;
+    d.lty = bty; d.ltz = btz; d.lhalo = H;
+    d.lsx = lsx; d.lsy = lsy; d.lsz = lsz;
+    d.ltiles[0] = (nx + 31) / 32;
+    d.ltiles[1] = (ny + bty - 1) / bty;
+    d.ltiles[2] = (nz + btz - 1) / btz;
+    d.ncache = ncache;
+    S->smem = 32 * (size_t)ncache + fixed;
+    phase.mark("lattice slots");
+    return BBPD_OK;
+}
+
 extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int device,
                            bbpd_solver **out)
 {
@@ -2810,8 +3403,13 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     d.s0e = d.s1e = d.sce = nullptr;
     d.smax = nullptr;
     BBPD_CUDA_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
-    if (prm->node_order == BBPD_ORDER_TILED) TRY(host_layout(S, pb, inv, fwd_ids, negid, dict, dictx, phase));
-    else TRY(device_layout(S, pb, inv, fwd_ids, negid, phase));
+    if (prm->node_order == BBPD_ORDER_LATTICE) TRY(lattice_layout(S, pb, fwd_ids, dict, phase));
+    if (S->lattice) {
+    } else if (prm->node_order == BBPD_ORDER_TILED) {
+        TRY(host_layout(S, pb, inv, fwd_ids, negid, dict, dictx, phase));
+    } else {
+        TRY(device_layout(S, pb, inv, fwd_ids, negid, phase));
+    }
     lid.reset();
 
     // node arrays in device order, staged; the initial displacement and
@@ -2961,7 +3559,11 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     d.timeout_ns = (unsigned long long)(to * 1e9);
 
     // kernel and grid
-    if (S->tiled) {
+    if (S->lattice) {
+        S->kernel = pick_lkernel(prm->law, prm->scheme, pb->sc != nullptr);
+        BBPD_CUDA_TRY(cudaFuncSetAttribute((const void *)S->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)S->smem));
+    } else if (S->tiled) {
         S->kernel = pick_tkernel(prm->law, prm->scheme, S->prec, pb->sc != nullptr);
         BBPD_CUDA_TRY(cudaFuncSetAttribute((const void *)S->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)S->smem));
@@ -2983,6 +3585,8 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     // node arrays; dictionary and damaged-bond BSF reads excluded)
     {
         double per_entry = (S->tiled ? 2 : 4) + (S->wide ? 4 : 2) + 1 + (pb->s0 ? 8 : 0) + (pb->s1 ? 8 : 0) + (pb->sc ? 8 : 0);
+        // lattice form: each bond slot (state byte, dictionary id, sc) read once from DRAM
+        if (S->lattice) per_entry = 0.5 * (double)S->ne / (double)std::max<int64_t>(nB, 1) * (2 + 1 + (pb->sc ? 8 : 0));
         double node = prm->scheme == BBPD_SCHEME_ADR
                           ? (24 /*x*/ + 4 /*deg*/ + 24 * 3 + 8 /*u v Fp m*/ + 24 /*F w*/ +
                              24 * 4 + 8 + 1 /*F u v X m flag*/ + 72 /*v u x w*/)
@@ -3350,7 +3954,7 @@ extern "C" int bbpd_get_info(bbpd_solver *S, bbpd_info *info)
     info->block_threads = kBlock;
     info->device_bytes = S->device_bytes;
     info->bytes_per_step = S->bytes_per_step;
-    info->layout = (S->wide ? 2 : (S->prec == kP32X ? 3 : 1)) + (S->tiled ? 16 : 0);
+    info->layout = (S->wide ? 2 : (S->prec == kP32X ? 3 : 1)) + (S->tiled ? 16 : 0) + (S->lattice ? 32 : 0);
     info->reserved = (int32_t)std::min<int64_t>(S->ndict, INT32_MAX);
     return BBPD_OK;
 }
@@ -3490,7 +4094,7 @@ extern "C" int bbpd_batch_add(bbpd_batch *B, bbpd_solver *S)
     if (S->prm.scheme != BBPD_SCHEME_ADR) return fail(BBPD_ERR_UNSUPPORTED, "batches run the ADR scheme");
     if (S->prm.precision != (B->prec == kP64 ? BBPD_PREC_FP64 : BBPD_PREC_FP32))
         return fail(BBPD_ERR_UNSUPPORTED, "solver precision form differs from the batch's");
-    if (S->wide || S->tiled)
+    if (S->wide || S->tiled || S->lattice)
         return fail(BBPD_ERR_UNSUPPORTED, "batch members need 16-bit dictionary ids and input or Morton node order");
     BBPD_CUDA_TRY(cudaSetDevice(S->device));
     BBPD_CUDA_TRY(cudaStreamSynchronize(S->stream));

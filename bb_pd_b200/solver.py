@@ -38,7 +38,8 @@ def make_params(inp: dict | None = None, *, law: str | int = "exponential",
     p.precision = {"fp64": N.PREC_FP64, "fp32": N.PREC_FP32}[precision] if isinstance(precision, str) else int(precision)
     p.n_chunks = n_chunks
     p.amplitude = {"linear": N.AMP_LINEAR, "smoothstep": N.AMP_SMOOTHSTEP}[amplitude] if isinstance(amplitude, str) else int(amplitude)
-    p.node_order = {"input": N.ORDER_INPUT, "morton": N.ORDER_MORTON, "tiled": N.ORDER_TILED}[node_order]
+    p.node_order = {"input": N.ORDER_INPUT, "morton": N.ORDER_MORTON, "tiled": N.ORDER_TILED,
+                    "lattice": N.ORDER_LATTICE}[node_order]
     p.rate, p.applied_final, p.n_time_steps = rate, applied_final, n_time_steps
     p.s0, p.s1, p.sc, p.sc_steel = s0, s1, sc, sc_steel
     p.k_exp, p.alpha_exp, p.beta_tri = k_exp, alpha_exp, beta_tri

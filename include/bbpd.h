@@ -55,9 +55,16 @@ enum { BBPD_AMP_LINEAR = 0,       /* U(n) = rate * n */
 enum { BBPD_ORDER_INPUT = 0,      /* input node order, neighbours gathered from HBM/L2
                                      with L2 prefetch of the bond streams; the default */
        BBPD_ORDER_MORTON = 1,     /* Morton node order, neighbours gathered from HBM/L2 */
-       BBPD_ORDER_TILED = 2       /* Morton order in 512-node tiles whose neighbours are
+       BBPD_ORDER_TILED = 2,      /* Morton order in 512-node tiles whose neighbours are
                                      staged in shared memory (falls back to MORTON when a
-                                     tile's neighbourhood does not fit) */ };
+                                     tile's neighbourhood does not fit) */
+       BBPD_ORDER_LATTICE = 3     /* lattice form: nodes on a regular lattice in x-fastest
+                                     order (buildmaterialpointcoordinates.m) with a bond
+                                     list ordered by first node and one common family
+                                     order (buildbonddata.m): neighbours addressed by the
+                                     stencil, one state slot per bond, tiles of positions
+                                     staged in shared memory. FP64 form; other inputs and
+                                     the FP32 form fall back to INPUT */ };
 
 /* Message of the last failing call on this thread ("" if none). */
 const char *bbpd_last_error(void);
@@ -485,7 +492,8 @@ typedef struct bbpd_info {
     double bytes_per_step;                /* algorithmic DRAM bytes of one step */
     int32_t layout;                       /* 1 = 16-bit dictionary ids, 2 = 32-bit ids
                                              (irregular input), 3 = FP32 dictionary of bond
-                                             vectors; +16 when the tiled kernel runs */
+                                             vectors; +16 when the tiled kernel runs,
+                                             +32 when the lattice form runs */
     int32_t reserved;                     /* dictionary entries */
 } bbpd_info;
 int bbpd_get_info(bbpd_solver *s, bbpd_info *info);

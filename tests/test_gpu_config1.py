@@ -1,0 +1,104 @@
+"""GPU parity at a benchmark size: the 20 000-node beam of the first
+configuration (500 x 100 x 50 mm, dx 5 mm, 1 005 544 bonds), run for 5 000
+steps against the oracle driving the reference's own compiled MEX routines
+(oracle/_ref: deformed length, bond force, nodal force in the OpenMP order,
+Euler-Cromer, exponential law), with the MATLAB-only pieces (trilinear law,
+ADR, prescribed displacement) restated from their .m files.
+
+ADR (dynamicsolverdisplacementcontrolledADR.m:91-155 with
+calculatedampingcoefficient.m:59-112 and timeintegrationADR.m:53-80):
+  * the fused kernel forms the Rayleigh-quotient sums in a fixed 32-ary tree;
+    against the oracle in that order every field is bit-identical;
+  * against the oracle in MATLAB's sequential node order, displacement and
+    nodal force must agree within 1e-12 of their largest magnitude, with
+    identical softening and broken-bond sets.
+Two loading rates: the benchmark's 1e-7 mm per step, and 1e-4 mm per step, at
+which the beam softens, peaks and cracks within the 5 000 steps. Both device
+forms run against the same oracle runs: the input-order kernel and the
+lattice form (stencil-addressed neighbours, one state slot per bond).
+
+Euler-Cromer with the exponential law (dynamicsolverdisplacementcontrolled.m:
+71-143) against the same loop with every MEX routine compiled from the
+reference: bit-identical when the device exp and glibc's agree on every call,
+else within the exponential-law bar of test_gpu_solver.compare."""
+import numpy as np
+import pytest
+
+import bb_pd_b200 as bb
+from oracle import pyoracle as po
+
+from test_gpu_solver import LAWKW, compare, same
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not po.ref_available(), reason="oracle/_ref (reference MEX routines) not built")]
+
+NODAL = ("displacement", "velocity", "force", "deformed")
+BOND = ("bsf", "flag", "fail")
+STEPS = 5000
+SEQ_RTOL = 1e-12     # MATLAB's sequential damping sums vs the kernel's tree
+
+
+@pytest.fixture(scope="module")
+def beam1():
+    inp = bb.beam.build(bb.beam.config1())
+    assert inp["nNodes"] == 20000 and inp["nBonds"] == 1005544
+    return inp
+
+
+def _identical(s, r, where):
+    for f in NODAL + BOND:
+        a, b = s.get(f), r.get(f)
+        assert same(a, b), f"{where}: {f}: {int(np.sum(a != b))} of {a.size} differ"
+
+
+def _march(solvers, runs, marks, check):
+    done = 0
+    for m in marks:
+        for s in solvers:
+            s.step(m - done)
+        for r in runs:
+            r.step(m - done)
+        done = m
+        check(m)
+
+
+@pytest.mark.parametrize("rate", [-1e-10, -1e-7], ids=["1e-7mm_per_step", "1e-4mm_per_step"])
+def test_config1_adr_vs_reference_mex(beam1, rate):
+    kw = dict(LAWKW["trilinear"], scheme="adr", rate=rate)
+    forms = {"input": bb.Solver(beam1, **kw), "lattice": bb.Solver(beam1, node_order="lattice", **kw)}
+    assert forms["lattice"].info()["layout"] & 32
+    tree = po.Run(beam1, kernels="reference", cn_order="tree", **kw)
+    seq = po.Run(beam1, kernels="reference", cn_order="seq", **kw)
+
+    def check(m):
+        for name, s in forms.items():
+            _identical(s, tree, f"{name} form, step {m}, tree order")
+            assert s.cn == tree.cn
+            for f in ("displacement", "force"):
+                a, b = s.get(f), seq.get(f)
+                np.testing.assert_allclose(a, b, rtol=0, atol=SEQ_RTOL * max(np.abs(b).max(), 1e-300),
+                                           err_msg=f"{name} form, step {m}, sequential order: {f}")
+            assert np.array_equal(s.get("flag"), seq.get("flag")), f"{name}, step {m}: softening set"
+            assert np.array_equal(s.get("bsf") == 1, seq.get("bsf") == 1), f"{name}, step {m}: broken set"
+            assert np.array_equal(s.get("fail"), seq.get("fail")), f"{name}, step {m}: fail"
+
+    _march(list(forms.values()), (tree, seq), (1, 2, 100, 1200, 2500, STEPS), check)
+    if rate == -1e-7:   # the run reaches softening and cracking
+        assert (tree.get("bsf") == 1).sum() > 1000
+    for s in forms.values():
+        s.close()
+
+
+def test_config1_eulercromer_exponential_vs_reference_mex(beam1):
+    kw = dict(LAWKW["exponential"], scheme="eulercromer", rate=-1e-7)
+    forms = [bb.Solver(beam1, **kw), bb.Solver(beam1, node_order="lattice", **kw)]
+    r = po.Run(beam1, kernels="reference", **kw)
+
+    def check(m):
+        for s in forms:
+            compare(s, r, "exponential")
+
+    _march(forms, (r,), (1, 300, 700, 1000), check)
+    assert (r.get("flag") > 0).any()
+    for s in forms:
+        s.close()

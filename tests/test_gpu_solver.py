@@ -454,3 +454,147 @@ def test_savedata_mat(small, tmp_path):
     m = scipy.io.loadmat(path)
     assert same(m["deformedCoordinates"], s.get("deformed"))
     assert m["fail"].shape == (small["nBonds"], 1) and m["flagBondSoftening"].shape == (small["nBonds"], 1)
+
+
+# ---------------------------------------------------------------- lattice form
+
+def _lattice(inp, **kw):
+    s = bb.Solver(inp, node_order="lattice", **kw)
+    assert s.info()["layout"] & 32, "lattice form expected"
+    return s
+
+
+@pytest.mark.parametrize("law", list(LAWKW))
+@pytest.mark.parametrize("scheme", ["eulercromer", "adr"])
+def test_lattice_vs_oracle(small, law, scheme):
+    """Stencil-addressed neighbours and one state slot per bond: the same
+    arithmetic in the same order as the reference loop, bit for bit."""
+    kw = dict(LAWKW[law], scheme=scheme, rate=-4e-6 if scheme == "eulercromer" else -2e-6)
+    s = _lattice(small, **kw)
+    r = po.Run(small, **kw)
+    for n in (1, 40, 119):
+        s.step(n)
+        r.step(n)
+        compare(s, r, law)
+    if scheme == "adr":
+        assert s.cn == r.cn or law == "exponential"
+    if law == "linear":
+        assert (r.get("fail") == 0).any()
+    else:
+        assert (r.get("bsf") > 0).any()
+    s.close()
+
+
+@pytest.fixture(scope="module")
+def ragged():
+    """70 x 9 x 11 nodes: partial tiles along every axis (x rows of 32, rows of
+    the tile's y and z extents), supports and load away from tile edges."""
+    return bb.beam.build(bb.beam.small(nx=70, ny=9, nz=11))
+
+
+@pytest.mark.parametrize("law", ["trilinear", "linear"])
+def test_lattice_ragged_tiles_vs_input_order(ragged, law):
+    nB = ragged["nBonds"]
+    rng = np.random.default_rng(5)
+    inp = dict(ragged)
+    inp["fail"] = (rng.random(nB) > 0.03).astype(np.float64)
+    inp["BONDTYPE"] = rng.integers(0, 3, nB).astype(np.float64)
+    kw = dict(LAWKW[law], scheme="adr", rate=-4e-6)
+    a = bb.Solver(inp, node_order="input", **kw)
+    b = _lattice(inp, **kw)
+    for n in (1, 30, 90):
+        a.step(n)
+        b.step(n)
+        for f in NODAL + BOND:
+            assert same(a.get(f), b.get(f)), (n, f)
+    assert a.cn == b.cn
+    a.close()
+    b.close()
+
+
+def test_lattice_notched_per_bond_sc_vs_oracle():
+    """Bonds across the notch are missing from the list (absent slots) and the
+    critical stretch is per bond (lognormal): exponential law, ADR."""
+    sp = bb.beam.spec(40, 4, 12, 2.5e-3, supports=(7.5e-3, 0.0925), notch_x=0.05 + 1.25e-3 + 0.01,
+                      notch_depth=0.01, sc_lognormal=(2e-3, 0.1))
+    inp = bb.beam.build(sp)
+    kw = dict(law="exponential", scheme="adr", s0=1e-4, rate=-1e-6)
+    s = _lattice(inp, **kw)
+    r = po.Run(inp, **kw)
+    s.step(150)
+    r.step(150)
+    compare(s, r, "exponential")
+
+
+@pytest.mark.parametrize("T", [1, 3])
+def test_lattice_chunk_counts(small, T):
+    kw = dict(LAWKW["trilinear"], scheme="adr", rate=-2e-6, n_chunks=T)
+    s = _lattice(small, **kw)
+    r = po.Run(small, **kw)
+    s.step(30)
+    r.step(30)
+    compare(s, r, "trilinear")
+
+
+def test_lattice_falls_back_when_not_a_lattice(small):
+    """Inputs the lattice form does not cover run the input-order kernel:
+    jittered coordinates, a bond list not ordered by first node, and more
+    OpenMP chunk starts in a list than the form records."""
+    kw = dict(LAWKW["trilinear"], scheme="adr", rate=-2e-6)
+    X = small["undeformedCoordinates"].copy(order="F")
+    X[7, 1] += 1e-9
+    nB = small["nBonds"]
+    shuffled = dict(small)
+    perm = np.random.default_rng(3).permutation(nB)
+    for k, v in small.items():
+        if isinstance(v, np.ndarray) and v.ndim >= 1 and v.shape[0] == nB:
+            shuffled[k] = np.asfortranarray(v[perm])
+    for inp, extra in ((dict(small, undeformedCoordinates=X), {}), (shuffled, {}), (small, {"n_chunks": 64})):
+        s = bb.Solver(inp, node_order="lattice", **kw, **extra)
+        assert not s.info()["layout"] & 32
+        r = po.Run(inp, **kw, **extra)
+        s.step(20)
+        r.step(20)
+        compare(s, r, "trilinear")
+        s.close()
+
+
+def test_lattice_state_roundtrip_and_restore(ragged):
+    """Per-bond fields cross the C ABI through the bond -> slot map; a
+    checkpoint restored into a fresh lattice solver continues bit for bit."""
+    nB = ragged["nBonds"]
+    rng = np.random.default_rng(9)
+    kw = dict(LAWKW["bilinear"], scheme="adr", rate=-4e-6)
+    a = _lattice(ragged, **kw)
+    v = rng.random(nB)
+    v[rng.random(nB) < 0.7] = 0.0
+    a.set("bsf", v)
+    assert same(a.get("bsf"), v)
+    fl = (rng.random(nB) < 0.2).astype(np.float64)
+    a.set("flag", fl)
+    assert same(a.get("flag"), fl)
+    fa = (rng.random(nB) > 0.1).astype(np.float64)
+    a.set("fail", fa)
+    assert same(a.get("fail"), fa)
+    a.step(25)
+    ck = a.checkpoint()
+    b = _lattice(ragged, **kw)
+    b.restore(ck)
+    a.step(40)
+    b.step(40)
+    for f in NODAL + BOND:
+        assert same(a.get(f), b.get(f)), f
+    a.close()
+    b.close()
+
+
+def test_lattice_damage_energy_tracking(small):
+    kw = dict(LAWKW["trilinear"], scheme="adr", rate=-4e-6)
+    a = bb.Solver(small, **kw)
+    b = _lattice(small, **kw)
+    a.track_damage_energy()
+    b.track_damage_energy()
+    a.step(90)
+    b.step(90)
+    ea, eb = a.get("damage_energy"), b.get("damage_energy")
+    assert (ea > 0).any() and same(ea, eb)
