@@ -8,6 +8,8 @@
 
 #include <cstdint>
 
+#include "crexp.cuh"
+
 namespace bbpd {
 
 // Law parameters that are scalars in the reference calls.
@@ -93,7 +95,9 @@ __device__ __forceinline__ void law_exponential(double s, double s0, double sc,
     double bsf = 0.0;
     if (s0 < s && s <= sc) {
         flag = true;
-        double numerator = 1 - exp(-P.k * (s - s0) / (sc - s0));
+        // exp correctly rounded (crexp.cuh); glibc's exp agrees on all but
+        // about 8 in 10^4 arguments of the law's range
+        double numerator = 1 - cr_exp(-P.k * (s - s0) / (sc - s0));
         double residual = P.alpha * (1 - (s - s0) / (sc - s0));
         bsf = 1 - (s0 / s) * ((1 - (numerator / P.exp_den)) + residual) / (1 + P.alpha);
     } else if (s > sc) {

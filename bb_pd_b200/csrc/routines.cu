@@ -65,7 +65,7 @@ __global__ void k_bsfexponential(const double *__restrict__ s, const double *__r
         double s0k = s0[k], sck = sc[k], sk = s[k];
         if (s0k < sk && sk <= sck) {
             f = true;
-            double numerator = 1 - exp(-P.k * (sk - s0k) / (sck - s0k));
+            double numerator = 1 - cr_exp(-P.k * (sk - s0k) / (sck - s0k));   // correctly rounded (crexp.cuh)
             double residual = P.alpha * (1 - (sk - s0k) / (sck - s0k));
             bs = 1 - (s0k / sk) * ((1 - (numerator / P.exp_den)) + residual) / (1 + P.alpha);
             bsf[k] = bs;

@@ -1,5 +1,6 @@
 // Device self-tests of the arithmetic the kernels rely on.
 #include "bbpd_internal.h"
+#include "crexp.cuh"
 #include "divide.cuh"
 
 #include <cstring>
@@ -72,7 +73,56 @@ __global__ void division_selftest_kernel(int64_t n, uint64_t seed, Counts *c)
     atomicMax(&c->rcp_err_bits, (unsigned long long)__double_as_longlong(maxerr));
 }
 
+// Uniform doubles in [lo, hi) from a counter (splitmix64), the sampler of the
+// host-side check of the same exp code.
+__device__ __forceinline__ double exp_sample(uint64_t seed, uint64_t i, double lo, double hi)
+{
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * (i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return __dadd_rn(lo, __dmul_rn(__dsub_rn(hi, lo), __dmul_rn((double)(z >> 11), 0x1p-53)));
+}
+
+// cr_exp on n samples: results whose fast step differs from the accurate
+// step, and the sum (mod 2^64) of the results' bit patterns.
+__global__ void exp_selftest_kernel(double lo, double hi, int64_t n, uint64_t seed, unsigned long long *out)
+{
+    unsigned long long bad = 0, sum = 0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const double x = exp_sample(seed, (uint64_t)t, lo, hi);
+        const double c = cr_exp(x);
+        sum += (unsigned long long)__double_as_longlong(c);
+        if (fabs(x) >= 0x1p-60 && x >= -745.2 && x <= 709.8) {
+            const double a = crexp_detail::accurate(x, (int)rint(x * crexp_tab::INV_LN2_N));
+            if (__double_as_longlong(a) != __double_as_longlong(c)) bad++;
+        }
+    }
+    atomicAdd(&out[0], bad);
+    atomicAdd(&out[1], sum);
+}
+
 }  // namespace
+
+extern "C" int bbpd_selftest_exp(double lo, double hi, int64_t n, uint64_t seed, int64_t *fast_vs_accurate,
+                                 uint64_t *bits_sum)
+{
+    int rc = require_device();
+    if (rc) return rc;
+    if (n < 0 || !fast_vs_accurate || !bits_sum || !(lo <= hi)) return fail(BBPD_ERR_ARG, "bad argument");
+    unsigned long long *dc = nullptr;
+    BBPD_CUDA_TRY(cudaMalloc(&dc, 2 * sizeof(unsigned long long)));
+    BBPD_CUDA_TRY(cudaMemset(dc, 0, 2 * sizeof(unsigned long long)));
+    exp_selftest_kernel<<<148 * 8, 256>>>(lo, hi, n, seed, dc);
+    unsigned long long h[2] = {0, 0};
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(h, dc, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(dc);
+    if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "exp selftest: %s", cudaGetErrorString(e));
+    *fast_vs_accurate = (int64_t)h[0];
+    *bits_sum = (uint64_t)h[1];
+    return BBPD_OK;
+}
 
 extern "C" int bbpd_selftest_division(int64_t n, uint64_t seed, int64_t *recip_mismatches,
                                       int64_t *quot_mismatches, int64_t *samples,

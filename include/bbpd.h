@@ -588,6 +588,16 @@ int bbpd_selftest_division(int64_t n, uint64_t seed, int64_t *recip_mismatches,
                            int64_t *quot_mismatches, int64_t *samples,
                            double *rcp_approx_max_relerr);
 
+/* Diagnostic: the device's correctly rounded exp (the exponential law's exp,
+ * in place of CUDA's, so that the law rounds like the reference's libm call,
+ * calculatebsfexponentialMex.c:43) on n samples uniform in [lo, hi) drawn
+ * from `seed` (splitmix64 of the sample index): reports how many results of
+ * the fast double-double step differ from the 128-bit accurate step, and the
+ * sum modulo 2^64 of the results' bit patterns, which the host build of the
+ * same code reproduces for the same samples. */
+int bbpd_selftest_exp(double lo, double hi, int64_t n, uint64_t seed, int64_t *fast_vs_accurate,
+                      uint64_t *bits_sum);
+
 /* ===================================================================== *
  *  Synthetic beam builder (the inputs of input/scripts/Gregoire_beam_    *
  *  tests.m and the functions it calls, for a regular lattice).          *
