@@ -146,6 +146,7 @@ def lib() -> C.CDLL:
         L.bbpd_batch_step.argtypes = [C.c_void_p, C.c_int64]
         L.bbpd_batch_tune.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.bbpd_batch_set_schedule.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.bbpd_batch_set_mixing.argtypes = [C.c_void_p, C.c_int]
         L.bbpd_batch_get_info.argtypes = [C.c_void_p, C.POINTER(BatchInfo)]
         L.bbpd_batch_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
         L.bbpd_beam_count.argtypes = [C.POINTER(BeamSpec), C.POINTER(BeamScalars)]

@@ -45,6 +45,11 @@ class Batch:
     def set_schedule(self, blocks_per_sm: int, grab: int = 1, use_graph: bool = True) -> None:
         N.check(N.lib().bbpd_batch_set_schedule(self._h, blocks_per_sm, grab, int(use_graph)))
 
+    def set_mixing(self, mixed: bool) -> None:
+        """True (default): all laws in one launch per kernel variant; False: one
+        specialised launch per law and critical-stretch form."""
+        N.check(N.lib().bbpd_batch_set_mixing(self._h, int(mixed)))
+
     def info(self) -> dict:
         i = N.BatchInfo()
         N.check(N.lib().bbpd_batch_get_info(self._h, C.byref(i)))

@@ -1720,7 +1720,89 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
         for (int m = threadIdx.x; m < B.S; m += blockDim.x) B.mstep[m] += nsteps;
 }
 
+// Forces and integration terms of slice sl of member d under law LAW, out of
+// line: each law keeps a register allocation of its own instead of sharing one
+// sized for all four.
+template <int LAW, int PREC>
+__device__ __noinline__ void mixed_law_slice(const Dev &d, const StepBufs &b, int64_t sl, int lane, int64_t it)
+{
+    const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
+    double tx, ty, tz;
+    if (PREC == kP32X) slice_forces_x<LAW, uint16_t, 2>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
+    else slice_forces<LAW, PREC, uint16_t, 2>(d, sl, lane, safe, b.xs, b.xas, tx, ty, tz);
+    finish_slice<BBPD_SCHEME_ADR, PREC>(d, b, sl, lane, tx, ty, tz, it);
+}
+
+// Slice sl of member d with its own law (a warp-uniform switch: a slice
+// belongs to one member), reading a per-entry critical stretch when the
+// member has one.
+template <int PREC>
+__device__ __forceinline__ void mixed_slice(const Dev &d, const StepBufs &b, int64_t sl, int lane, int64_t it)
+{
+    switch (d.law) {
+    case BBPD_LAW_LINEAR: mixed_law_slice<BBPD_LAW_LINEAR, PREC>(d, b, sl, lane, it); break;
+    case BBPD_LAW_BILINEAR: mixed_law_slice<BBPD_LAW_BILINEAR, PREC>(d, b, sl, lane, it); break;
+    case BBPD_LAW_TRILINEAR: mixed_law_slice<BBPD_LAW_TRILINEAR, PREC>(d, b, sl, lane, it); break;
+    default: mixed_law_slice<BBPD_LAW_EXPONENTIAL, PREC>(d, b, sl, lane, it); break;
+    }
+}
+
+// Every member of a batch of one kernel precision variant, whatever its law
+// and whether it reads a per-entry critical stretch, in one persistent launch
+// (the schedule of batch_kernel; each member's arithmetic is that of its own
+// solver's kernel).
+template <int PREC>
+__global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel_mixed(BatchCtl B, int64_t nsteps)
+{
+    __shared__ Dev s_dev[kBlock / 32];
+    __shared__ int s_held[kBlock / 32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t G = B.grab;
+    const int64_t ngrabs = (B.total + G - 1) / G;
+    if (lane == 0) s_held[wib] = -1;
+    __syncwarp();
+
+    for (int64_t it = 0; it < nsteps; it++) {
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            for (int m = 0; m < B.S; m++)
+                if (B.members[m].n_pen) contact_advance(B.members[m], __ldg(&B.mstep[m]) + it);
+        const int64_t base = it * (ngrabs + nwarps);
+        int64_t gi = grab_counter(B.work, lane) - base;
+        while (gi < ngrabs) {
+            const int64_t gnext = grab_counter(B.work, lane) - base;
+            const int64_t w1 = min(B.total, (gi + 1) * G);
+            for (int64_t w = gi * G; w < w1; w++) {
+                const int m = member_of(B, w);
+                const Dev &d = warp_member(B, m, &s_dev[wib], &s_held[wib], lane);
+                const StepBufs b = step_bufs(d, __ldg(&B.mstep[m]) + it);
+                mixed_slice<PREC>(d, b, w - __ldg(&B.prefix[m]), lane, it);
+            }
+            gi = gnext;
+        }
+        if (!grid_barrier_raw(B.bar, B.err, B.timeout_ns)) return;
+        for (int64_t w = gwarp; w < B.total; w += nwarps) {
+            const int m = member_of(B, w);
+            const Dev &d = warp_member(B, m, &s_dev[wib], &s_held[wib], lane);
+            const StepBufs b = step_bufs(d, __ldg(&B.mstep[m]) + it);
+            adr_update_slice<PREC>(d, b, w - __ldg(&B.prefix[m]), lane, it);
+        }
+        if (!grid_barrier_raw(B.bar, B.err, B.timeout_ns)) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            for (int m = 0; m < B.S; m++)
+                if (B.members[m].n_pen) contact_reaction(B.members[m], __ldg(&B.mstep[m]) + it, it);
+    }
+    if (blockIdx.x == 0)
+        for (int m = threadIdx.x; m < B.S; m += blockDim.x) B.mstep[m] += nsteps;
+}
+
 typedef void (*batch_kernel_t)(BatchCtl, int64_t);
+
+batch_kernel_t pick_batch_mixed(int prec)
+{
+    return prec == kP32X ? batch_kernel_mixed<kP32X> : batch_kernel_mixed<kP64>;
+}
 
 template <int PREC, bool SCE>
 batch_kernel_t pick_batch_law(int law)
@@ -3029,14 +3111,7 @@ static int lattice_layout(bbpd_solver *S, const bbpd_problem *pb, FwdIds fwd_ids
     std::iota(order.begin(), order.end(), 0u);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
     std::vector<uint16_t> remap(dict.size());
-    {
-        std::vector<DictEntry> nd(dict.size());
-        for (size_t q = 0; q < order.size(); q++) {
-            remap[order[q]] = (uint16_t)q;
-            nd[q] = dict[order[q]];
-        }
-        dict.swap(nd);
-    }
+    for (size_t q = 0; q < order.size(); q++) remap[order[q]] = (uint16_t)q;
     phase.mark("lattice check");
 
     // staged per-bond data, chunk positions, then the slots
@@ -3094,7 +3169,14 @@ static int lattice_layout(bbpd_solver *S, const bbpd_problem *pb, FwdIds fwd_ids
         TRY(tmp.get(&dsc, (size_t)nB));
         TRY(staging::upload_copy(dsc, pb->sc, nB, st));
     }
-    // from here on the lattice form is committed: its arrays belong to the solver
+    // from here on the lattice form is committed: its arrays belong to the
+    // solver, and the dictionary takes the new numbering (until here the
+    // input-order layout may still be built with the old one)
+    {
+        std::vector<DictEntry> nd(dict.size());
+        for (size_t q = 0; q < order.size(); q++) nd[q] = dict[order[q]];
+        dict.swap(nd);
+    }
     int4 *ltab = nullptr;
     TRY(S->put(&ltab, tab));
     d.ltab = ltab;
@@ -4003,6 +4085,7 @@ struct bbpd_batch {
     int64_t total = 0;
     double timeout_s = 2.0;
     bool use_graph = true;                 // replay the launches from a captured CUDA graph
+    bool mixed = true;                     // all laws of a precision variant in one launch
     cudaGraphExec_t gexec = nullptr;
     int64_t g_nsteps = -1;
     int g_bps = 0, g_grab = 0;
@@ -4073,6 +4156,12 @@ extern "C" int bbpd_batch_create(int device, int precision, bbpd_batch **out)
                 occ = std::min(occ, o);
             }
         }
+    for (int pv : {kP64, kP32X}) {
+        if (pv == kP32X && B->prec == kP64) continue;
+        int o = 0;
+        BBPD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void *)pick_batch_mixed(pv), kBlock, 0));
+        occ = std::min(occ, o);
+    }
     if (occ < 1) return fail(BBPD_ERR_CUDA, "batch kernel cannot be resident");
     B->occ = occ;
     B->blocks_per_sm = occ;
@@ -4127,16 +4216,19 @@ static int batch_rebuild(bbpd_batch *B)
     old.swap(B->classes);
     for (bbpd_solver *S : B->members) {
         BatchClass *c = nullptr;
-        const bool sce = S->d.sce != nullptr;
+        // one class per kernel precision variant (every law in one launch),
+        // or, with mixing off, per law and critical-stretch form as well
+        const bool sce = B->mixed ? false : S->d.sce != nullptr;
+        const int law = B->mixed ? -1 : S->prm.law;
         for (BatchClass &k : B->classes)
-            if (k.law == S->prm.law && k.prec == S->prec && k.sce == sce) c = &k;
+            if (k.law == law && k.prec == S->prec && k.sce == sce) c = &k;
         if (!c) {
             B->classes.emplace_back();
             c = &B->classes.back();
-            c->law = S->prm.law;
+            c->law = law;
             c->prec = S->prec;
             c->sce = sce;
-            c->kernel = pick_batch_kernel(c->law, c->prec, sce);
+            c->kernel = B->mixed ? pick_batch_mixed(c->prec) : pick_batch_kernel(c->law, c->prec, sce);
             // reuse the device tables of the same class from before
             for (BatchClass &o : old)
                 if (o.law == c->law && o.prec == c->prec && o.sce == c->sce && o.cap) {
@@ -4332,6 +4424,14 @@ extern "C" int bbpd_batch_set_schedule(bbpd_batch *B, int blocks_per_sm, int gra
     B->grab = grab;
     B->use_graph = use_graph != 0;
     B->drop_graph();
+    return BBPD_OK;
+}
+
+extern "C" int bbpd_batch_set_mixing(bbpd_batch *B, int mixed)
+{
+    if (!B) return fail(BBPD_ERR_ARG, "null batch");
+    TRY(batch_member_changed(B));
+    B->mixed = mixed != 0;
     return BBPD_OK;
 }
 

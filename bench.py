@@ -182,12 +182,19 @@ def run_batch(args):
     import bb_pd_b200 as bb
     from bb_pd_b200 import serving
     series = bb.beam.size_effect_series(args.members, dx=args.dx)
-    inps = [(bb.beam.build(sp), law) for sp, law in series]
-    nodes = [i["nNodes"] for i, _ in inps]
-    bonds = [i["nBonds"] for i, _ in inps]
-    tot_b = float(sum(bonds))
     mk = lambda i, law, prec: bb.Solver(i, scheme="adr", rate=RATE, precision=prec, **serving.LAWKW[law])
-    sol = [mk(i, law, args.form) for i, law in inps]
+    # one beam's host arrays at a time: the full series (dx 2.5 mm) holds
+    # billions of bonds, resident on the device but not at once on the host
+    sol, nodes, bonds = [], [], []
+    t_create = time.perf_counter()
+    for sp, law in series:
+        i = bb.beam.build(sp)
+        nodes.append(i["nNodes"])
+        bonds.append(i["nBonds"])
+        sol.append(mk(i, law, args.form))
+        del i
+    t_create = time.perf_counter() - t_create
+    tot_b = float(sum(bonds))
     batch = bb.Batch(args.form)
     for s in sol:
         batch.add(s)
@@ -211,8 +218,8 @@ def run_batch(args):
     seq_ms = 0.0
     for s in sol:
         s.close()
-    for i, law in inps:
-        s = mk(i, law, "fp64")
+    for sp, law in series:
+        s = mk(bb.beam.build(sp), law, "fp64")
         s.step(args.warmup)
         s.step(args.steps)
         seq_ms += s.last_kernel_ms()
@@ -225,14 +232,16 @@ def run_batch(args):
                           f"width 50 mm, dx {args.dx * 1e3:g} mm, linear/trilinear, lognormal sc, ADR, "
                           f"1e-7 mm/step", "nodes": int(sum(nodes)), "bonds": int(tot_b),
               "min_nodes": int(min(nodes)), "max_nodes": int(max(nodes)), "form": args.form,
-              "l2": "inputs larger than L2", "parallelism": "1 GPU, one persistent batch launch"}
+              "l2": "inputs larger than L2", "parallelism": "1 GPU, one persistent batch launch",
+              "steps_note": f"{args.steps} timed steps of the 10 000 the series names (time budget)",
+              "create_s": round(t_create, 1), "classes": info["n_classes"]}
     _batch_line(args, "bond-updates/s", "bond-updates/s", value, ms / args.steps, config, {
         "sequential_plain_fp64": {"value": seq, "unit": "bond-updates/s", "ms_per_step": seq_ms / args.steps},
         "speedup_vs_sequential_fp64": value / seq,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                      "peak_kind": peak_kind_str(kind), "traffic": None},
         "schedule": {"blocks_per_sm": bps, "grab": grab, "graph": bool(info["graph"])},
-        "gpu_launches": 1, "clocks": clk, "cpu_baseline": None, "e2e": None})
+        "gpu_launches": info["n_classes"], "clocks": clk, "cpu_baseline": None, "e2e": None})
 
 
 def peak_kind_str(kind):
@@ -331,6 +340,36 @@ def run_precision(args):
     print(json.dumps(line), flush=True)
 
 
+def serving_sample(requests=12, max_nodes=6e4, arrival_hz=6.0, rate=-1e-7, max_steps=4000, seed=20261203):
+    """A short serving run (continuous batching vs one plain FP64 solve at a
+    time) for the default bench line: a Poisson stream of `requests` beams of
+    1e4 .. max_nodes nodes, the four laws, each to 80 % post-peak load or
+    max_steps, at `rate` metres per step."""
+    import bb_pd_b200 as bb
+    from bb_pd_b200 import serving
+    stream = bb.beam.serving_stream(requests, seed=seed, nodes_range=(1e4, max_nodes), rate_hz=arrival_hz,
+                                    dx_choices=(2.5e-3, 5e-3))
+    reqs = [serving.Request(k, r["arrival"], bb.beam.build(r["spec"]), r["law"], rate, max_steps)
+            for k, r in enumerate(stream)]
+    res, st = serving.run_batched(reqs, precision="fp64", chunk=100)
+    seq, sst = serving.run_sequential(reqs, precision="fp64", chunk=100)
+    a, b = serving.summary(res, st), serving.summary(seq, sst)
+    peaks = {r.id: r for r in res}
+    peak_err = max((abs(peaks[r.id].peak - r.peak) / r.peak for r in seq if r.peak > 0), default=0.0)
+    return {"metric": "solves/h", "value": a["solves_per_hour"], "unit": "solves/h",
+            "p50_latency_s": a["p50_latency_s"], "p99_latency_s": a["p99_latency_s"],
+            "sequential_plain_fp64": {"solves_per_hour": b["solves_per_hour"], "p50_latency_s": b["p50_latency_s"],
+                                      "p99_latency_s": b["p99_latency_s"]},
+            "speedup_solves_per_hour": a["solves_per_hour"] / b["solves_per_hour"],
+            "peak_load_rel_diff_vs_sequential_max": peak_err,
+            "solves_past_peak": sum(1 for r in res if r.steps < max_steps),
+            "config": {"workload": f"serving sample: {requests} Poisson arrivals at {arrival_hz:g}/s, nodes "
+                                   f"log-uniform 1e4-{max_nodes:.0e}, dx 2.5/5 mm, four laws, to 80 % post-peak "
+                                   f"load or {max_steps} steps, {abs(rate) * 1e3:g} mm/step, plain FP64, "
+                                   "continuous batching vs one solve at a time"},
+            "gpu_launches": st["launches"], "peak_members": st.get("peak_members")}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -339,9 +378,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=list(CONFIGS))
     ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--node-order", default="input", choices=["input", "morton", "tiled"])
+    ap.add_argument("--node-order", default="lattice", choices=["input", "morton", "tiled", "lattice"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving sample of the default line")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "precision"],
                     help="single: one beam (--config); batch: the size-effect series in one "
                          "persistent batch launch; serve: a Poisson stream of solves, continuous batching")
@@ -483,12 +523,19 @@ def main():
         cpu = {"value": rate, "unit": unit, "cores": threads, "kind": kind,
                "sample": f"{n} time steps of the same beam ({dt:.1f} s)"}
 
+    serve = None
+    if not args.no_serving and world == 1:
+        t0 = time.perf_counter()
+        serve = serving_sample()
+        serve["seconds"] = round(time.perf_counter() - t0, 1)
+
     line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+f64", "data": "synthetic",
             "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 1,
             "clocks": clk, "solver": {"grid_blocks": info["grid_blocks"], "entries": info["n_entries"],
-                                      "device_bytes": info["device_bytes"]}}
+                                      "device_bytes": info["device_bytes"], "layout": info["layout"]},
+            "serving": serve}
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

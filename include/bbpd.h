@@ -552,7 +552,9 @@ typedef struct bbpd_batch_info {
     int32_t blocks_per_sm;     /* schedule in use */
     int32_t grab;              /* slices taken per work-counter grab */
     int32_t graph;             /* 1 if the last launch replayed a CUDA graph */
-    int32_t n_classes;         /* member classes (law x kernel variant): one launch each */
+    int32_t n_classes;         /* member classes: one launch each (one per kernel precision
+                                  variant; with mixing off, per law and critical-stretch
+                                  form too) */
     int32_t reserved;
     int64_t total_slices;
     int64_t device_bytes;      /* device memory held by the members */
@@ -569,6 +571,13 @@ int bbpd_batch_step(bbpd_batch *b, int64_t nsteps);
 int bbpd_batch_tune(bbpd_batch *b, int64_t nsteps_per_trial, int *blocks_per_sm, int *grab);
 int bbpd_batch_set_schedule(bbpd_batch *b, int blocks_per_sm, int grab, int use_graph);
 int bbpd_batch_get_info(bbpd_batch *b, bbpd_batch_info *info);
+/* Mixing (the default, 1): members of every law, with or without a per-entry
+ * critical stretch, step in one persistent launch per kernel precision
+ * variant, each slice taking its member's law. 0: one launch per law and
+ * critical-stretch form, each specialised to it. The reference's batch is
+ * the sequential loop over random-field realisations
+ * (randomfield/dynamicsolverdisplacementcontrolledRF.m:20). */
+int bbpd_batch_set_mixing(bbpd_batch *b, int mixed);
 int bbpd_batch_last_kernel_ms(bbpd_batch *b, float *ms);
 
 /* Elapsed device time of the last bbpd_step / bbpd_step_async launch (ms). */

@@ -35,10 +35,13 @@ def _solver(inp, law, precision="fp64", rate=-3e-6):
     return bb.Solver(inp, scheme="adr", rate=rate, precision=precision, **LAWKW[law])
 
 
+@pytest.mark.parametrize("mixed", [True, False], ids=["one_launch", "launch_per_law"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_alone_and_in_mix_identical(beams, precision):
+def test_alone_and_in_mix_identical(beams, precision, mixed):
     """Members of uneven size and law join and leave a batch at different
-    steps; each ends bit-identical to its solo run of the same length."""
+    steps; each ends bit-identical to its solo run of the same length. With
+    mixing (the default) the three laws, one member with a per-bond critical
+    stretch, run in a single persistent launch per kernel variant."""
     laws = ["trilinear", "linear", "exponential"]
     solo = []
     for inp, law, n in zip(beams, laws, (90, 70, 50)):
@@ -46,6 +49,7 @@ def test_alone_and_in_mix_identical(beams, precision):
         s.step(n)
         solo.append(s)
     batch = bb.Batch(precision)
+    batch.set_mixing(mixed)
     m = [_solver(inp, law, precision) for inp, law in zip(beams, laws)]
     batch.add(m[0])
     batch.step(20)                      # member 0 alone in the batch
@@ -53,6 +57,8 @@ def test_alone_and_in_mix_identical(beams, precision):
     batch.step(30)                      # 0 at 50, 1 at 30
     batch.add(m[2])
     batch.step(40)                      # 0 at 90, 1 at 70, 2 at 40
+    variants = len({mm.info()["layout"] & 15 for mm in m})
+    assert batch.info()["n_classes"] == (variants if mixed else 3)
     batch.remove(m[0])
     batch.remove(m[1])
     batch.step(10)                      # 2 at 50
