@@ -29,6 +29,14 @@ void orc_deformedlength(const double *x, const double *bl, const double *L0,
     }
 }
 
+/* The exp of the exponential law's numerator: libm's (the reference's
+ * call), or, after orc_use_cr_exp(1), a correctly rounded one (the host build
+ * of the device's, oracle/crexp_shim.cpp) to tell the device's arithmetic
+ * apart from libm's occasional misrounding. */
+double orc_cr_exp(double x);
+static double (*law_exp)(double) = exp;
+void orc_use_cr_exp(int on) { law_exp = on ? orc_cr_exp : exp; }
+
 /* calculatebsfexponentialMex.c:26-66 */
 void orc_bsf_exponential(const double *s, const double *s0, int s0_stride,
                          const double *sc, int sc_stride, double k, double alpha,
@@ -40,7 +48,7 @@ void orc_bsf_exponential(const double *s, const double *s0, int s0_stride,
             double s0b = s0[b * s0_stride], scb = sc[b * sc_stride];
             if (s0b < s[b] && s[b] <= scb) {
                 flag[b] = 1;
-                double numerator = 1 - exp(-k * (s[b] - s0b) / (scb - s0b));
+                double numerator = 1 - law_exp(-k * (s[b] - s0b) / (scb - s0b));
                 double denominator = 1 - exp(-k);
                 double residual = alpha * (1 - (s[b] - s0b) / (scb - s0b));
                 bsf[b] = 1 - (s0b / s[b]) * ((1 - (numerator / denominator)) + residual) / (1 + alpha);

@@ -41,6 +41,9 @@ void orc_deformedlength(const double *x, const double *bl, const double *L0,
                         int64_t nBonds, int64_t nNodes, double *L,
                         double *dX, double *dY, double *dZ, double *s);
 
+/* Numerator exp of the restated exponential law: libm's (0, the default) or a
+ * correctly rounded one (1). The compiled reference routines always use libm. */
+void orc_use_cr_exp(int on);
 /* calculatebsfexponentialMex.c:26-66. bsf is the caller-zeroed scratch
  * (dynamicsolverdisplacementcontrolled.m:86). s0/sc strides: 1 = per bond, 0 = scalar. */
 void orc_bsf_exponential(const double *s, const double *s0, int s0_stride,

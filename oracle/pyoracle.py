@@ -81,6 +81,7 @@ def lib() -> C.CDLL:
         L.orc_smoothstep.restype = C.c_double
         L.orc_smoothstep.argtypes = [C.c_double] * 5
         L.orc_restated_kernels.restype = C.c_void_p
+        L.orc_use_cr_exp.argtypes = [C.c_int]
         L.orc_load_reference.restype = C.c_void_p
         L.orc_load_reference.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
         L.orc_run.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.c_void_p, C.c_int64]
@@ -157,10 +158,13 @@ class Run:
                  s0=1e-4, s1=3e-4, sc=2e-3, sc_steel=1.0, k_exp=25.0, alpha_exp=0.25,
                  beta_tri=0.25, failure_functionality=0.0, damping=0.0, dt=None,
                  cell_volume=None, per_bond_sc=None, cn_order="tree", kernels="restated",
-                 penetrators=()):
+                 penetrators=(), law_exp="libm"):
         L = lib()
         nN, nB = int(inp["nNodes"]), int(inp["nBonds"])
         self.nN, self.nB = nN, nB
+        if law_exp not in ("libm", "cr") or (law_exp == "cr" and kernels != "restated"):
+            raise ValueError("law_exp is 'libm', or 'cr' with the restated kernels")
+        self.law_exp = law_exp
         self.keep = {k: f64(inp.get(k)) for k in (
             "undeformedCoordinates", "BONDLIST", "UNDEFORMEDLENGTH", "BONDSTIFFNESS",
             "VOLUMECORRECTIONFACTORS", "BONDTYPE", "stretchPlastic", "DENSITY", "massVector",
@@ -216,6 +220,9 @@ class Run:
             self.kern = L.orc_restated_kernels()
 
     def step(self, n: int = 1) -> None:
+        # the restated exponential law's exp: libm's (the reference's call) or
+        # a correctly rounded one ("cr"); the compiled reference always uses libm
+        lib().orc_use_cr_exp(1 if self.law_exp == "cr" else 0)
         lib().orc_run(C.byref(self.p), C.byref(self.st), self.kern, n)
 
     @property

@@ -3,10 +3,12 @@ reference loop (dynamicsolverdisplacementcontrolled.m:71-105 and its ADR form)
 run on the CPU by the restatement or by the reference's compiled MEX routines.
 
 Bar: plain FP64 form bit-identical in displacement, velocity, force, damage,
-softening flags and fail flags (up to the sign of zero); the exponential law
-within 1e-10 relative with an identical broken-bond set (CUDA's exp may differ
-from glibc's in the last bit); the FP32 form within the stated tolerances of the
-FP64 form with an identical broken-bond set."""
+softening flags and fail flags (up to the sign of zero), every law included
+when the oracle's exponential law rounds exp correctly as the device does;
+against libm's exp (the compiled reference) the exponential law within 1e-9
+of the largest magnitude with identical softening and broken-bond sets; the
+FP32 form within the stated tolerances of the FP64 form with an identical
+broken-bond set."""
 import os
 
 import numpy as np
@@ -28,19 +30,29 @@ NODAL = ("displacement", "velocity", "force", "deformed")
 BOND = ("bsf", "flag", "fail")
 
 
+def orun(inp, **kw):
+    """The oracle with the restated routines and a correctly rounded exp in the
+    exponential law (the device's exp rounds correctly; libm's misrounds about
+    8 in 10^4 of the law's arguments, which the libm runs below measure)."""
+    return po.Run(inp, law_exp="cr", **kw)
+
+
 def same(a, b):
     a, b = np.asarray(a), np.asarray(b)
     return a.shape == b.shape and bool(np.all((a == b) | (np.isnan(a) & np.isnan(b))))
 
 
 def compare(s, r, law, fields=NODAL + BOND, rtol=1e-9):
-    """Bit-identical, except the exponential law: CUDA's exp() and glibc's may
-    differ in the last bit, and undamped dynamics carry that along; there nodal
-    fields must agree within 1e-9 of their largest magnitude, damage within
-    1e-8, and softening flags and the broken-bond set exactly."""
+    """Bit-identical, except the exponential law against an oracle whose exp
+    is libm's (the compiled reference routines): libm's exp misrounds about 8
+    in 10^4 arguments where the device's is correctly rounded, and undamped
+    dynamics carry a last-bit difference along; there nodal fields must agree
+    within 1e-9 of their largest magnitude, damage within 1e-8, and softening
+    flags and the broken-bond set exactly."""
+    libm = law == "exponential" and getattr(r, "law_exp", "libm") == "libm"
     for f in fields:
         a, b = s.get(f), r.get(f)
-        if law == "exponential" and f not in ("flag", "fail"):
+        if libm and f not in ("flag", "fail"):
             atol = 1e-8 if f == "bsf" else rtol * max(np.abs(b).max(), 1e-300)
             np.testing.assert_allclose(a, b, rtol=0, atol=atol, err_msg=f)
         else:
@@ -58,13 +70,13 @@ def small():
 def test_fused_vs_oracle(small, law, scheme):
     kw = dict(LAWKW[law], scheme=scheme, rate=-4e-6 if scheme == "eulercromer" else -2e-6)
     s = bb.Solver(small, **kw)
-    r = po.Run(small, **kw)
+    r = orun(small, **kw)
     for n in (1, 40, 119):
         s.step(n)
         r.step(n)
         compare(s, r, law)
     if scheme == "adr":
-        assert s.cn == r.cn or law == "exponential"
+        assert s.cn == r.cn
     # the run exercises the law: some bonds soften or break
     if law == "linear":
         assert (r.get("fail") == 0).any()
@@ -108,7 +120,7 @@ def test_per_bond_sc_notched_adr():
     inp = bb.beam.build(sp)
     kw = dict(law="exponential", scheme="adr", s0=1e-4, rate=-1e-6)
     s = bb.Solver(inp, **kw)
-    r = po.Run(inp, **kw)
+    r = orun(inp, **kw)
     s.step(150)
     r.step(150)
     compare(s, r, "exponential")
@@ -118,7 +130,7 @@ def test_per_bond_sc_notched_adr():
 def test_chunk_counts(small, T):
     kw = dict(LAWKW["trilinear"], scheme="adr", rate=-2e-6, n_chunks=T)
     s = bb.Solver(small, **kw)
-    r = po.Run(small, **kw)
+    r = orun(small, **kw)
     s.step(30)
     r.step(30)
     compare(s, r, "trilinear")
@@ -136,7 +148,7 @@ def test_tiled_vs_oracle(tiled_beam, law, scheme):
     kw = dict(LAWKW[law], scheme=scheme, rate=-4e-6 if scheme == "eulercromer" else -2e-6)
     s = bb.Solver(tiled_beam, node_order="tiled", **kw)
     assert s.info()["layout"] & 16, "tiled kernel expected"
-    r = po.Run(tiled_beam, **kw)
+    r = orun(tiled_beam, **kw)
     for n in (1, 60):
         s.step(n)
         r.step(n)
@@ -225,12 +237,12 @@ def test_bad_bondlist_first_row_reported(medium, precision):
 def test_damage_energy_tracking_vs_oracle(small, law):
     """The fused solver's damage energy against the oracle's loop with
     calculatedamageenergy.m applied to every step's stretch (the drivers'
-    order): bit-identical for the FP64 laws without exp, within 1e-9 relative
-    for the exponential law (CUDA's and glibc's exp may differ in the last bit)."""
+    order): bit-identical for every law (the oracle's exponential law with a
+    correctly rounded exp, as the device's)."""
     kw = dict(LAWKW[law], scheme="adr", rate=-4e-6)
     s = bb.Solver(small, **kw)
     s.track_damage_energy()
-    r = po.Run(small, **kw)
+    r = orun(small, **kw)
     nB = small["nBonds"]
     s0 = np.full(nB, kw.get("s0", 1e-4))
     sc = np.full(nB, kw["sc"])
@@ -245,10 +257,7 @@ def test_damage_energy_tracking_vs_oracle(small, law):
     s.step(50)
     got = s.get("damage_energy")
     assert (E > 0).any()
-    if law == "exponential":
-        np.testing.assert_allclose(got, E, rtol=1e-9, atol=1e-9 * np.abs(E).max())
-    else:
-        assert same(got, E)
+    assert same(got, E)
     s.track_damage_energy()                    # restart: nothing recorded yet
     assert not s.get("damage_energy").any()
     s.close()
@@ -300,7 +309,7 @@ def test_checkpoint_resume_bit_identical(small, scheme):
 
 def test_smoothstep_amplitude(small):
     kw = dict(LAWKW["trilinear"], scheme="adr", amplitude="smoothstep", applied_final=-2e-4, n_time_steps=120)
-    s, r = bb.Solver(small, **kw), po.Run(small, **kw)
+    s, r = bb.Solver(small, **kw), orun(small, **kw)
     s.step(120)
     r.step(120)
     compare(s, r, "trilinear")
@@ -384,7 +393,7 @@ def test_contact_vs_oracle(small, scheme):
     kw = dict(LAWKW["trilinear"], scheme=scheme)
     s = bb.Solver(inp, **kw)
     s.set_contact(pens)
-    r = po.Run(inp, penetrators=pens, **kw)
+    r = orun(inp, penetrators=pens, **kw)
     for n in (1, 60, 79):
         s.step(n)
         r.step(n)
@@ -471,13 +480,13 @@ def test_lattice_vs_oracle(small, law, scheme):
     arithmetic in the same order as the reference loop, bit for bit."""
     kw = dict(LAWKW[law], scheme=scheme, rate=-4e-6 if scheme == "eulercromer" else -2e-6)
     s = _lattice(small, **kw)
-    r = po.Run(small, **kw)
+    r = orun(small, **kw)
     for n in (1, 40, 119):
         s.step(n)
         r.step(n)
         compare(s, r, law)
     if scheme == "adr":
-        assert s.cn == r.cn or law == "exponential"
+        assert s.cn == r.cn
     if law == "linear":
         assert (r.get("fail") == 0).any()
     else:
@@ -520,7 +529,7 @@ def test_lattice_notched_per_bond_sc_vs_oracle():
     inp = bb.beam.build(sp)
     kw = dict(law="exponential", scheme="adr", s0=1e-4, rate=-1e-6)
     s = _lattice(inp, **kw)
-    r = po.Run(inp, **kw)
+    r = orun(inp, **kw)
     s.step(150)
     r.step(150)
     compare(s, r, "exponential")
@@ -530,7 +539,7 @@ def test_lattice_notched_per_bond_sc_vs_oracle():
 def test_lattice_chunk_counts(small, T):
     kw = dict(LAWKW["trilinear"], scheme="adr", rate=-2e-6, n_chunks=T)
     s = _lattice(small, **kw)
-    r = po.Run(small, **kw)
+    r = orun(small, **kw)
     s.step(30)
     r.step(30)
     compare(s, r, "trilinear")
@@ -552,7 +561,7 @@ def test_lattice_falls_back_when_not_a_lattice(small):
     for inp, extra in ((dict(small, undeformedCoordinates=X), {}), (shuffled, {}), (small, {"n_chunks": 64})):
         s = bb.Solver(inp, node_order="lattice", **kw, **extra)
         assert not s.info()["layout"] & 32
-        r = po.Run(inp, **kw, **extra)
+        r = orun(inp, **kw, **extra)
         s.step(20)
         r.step(20)
         compare(s, r, "trilinear")
