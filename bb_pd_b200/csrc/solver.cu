@@ -164,9 +164,7 @@ struct Dev {
     const int32_t *cidx;             // per node: its contact entry, or -1
     // lattice form (lstep_kernel): bond slot f * n_nodes + lo holds the bond
     // between node lo and node lo + offset f of the forward stencil
-    const int4 *ltab;                // per chain position: (partner offset in the staged box, f * n_nodes,
-                                     // offset of the slot's lower node from this node, 0)
-    int n_sigma;                     // chain positions, a multiple of 4
+    int n_sigma;                     // chain positions, a multiple of 4 (the table travels as an LTab)
     const uint64_t *lcpos;           // per node: chain positions opening an OpenMP chunk, 8 bits each, 0xFF none
     int lnx, lny, lnz;               // lattice nodes per axis
     int lty, ltz, lhalo;             // tile rows per y and z (a tile is 32 nodes long in x), stencil reach
@@ -194,6 +192,13 @@ struct Dev {
     int64_t n_time_steps;
     double guard;
     unsigned long long timeout_ns;
+};
+
+// Lattice form: the chain table, passed by value with the launch so that its
+// entries are warp-uniform constant-bank reads.
+constexpr int kMaxSigma = 128;
+struct LTab {
+    int4 e[kMaxSigma];   // (partner offset in the staged box, slot row base, lower-node offset, 0)
 };
 
 __device__ __forceinline__ unsigned long long globaltimer()
@@ -1431,7 +1436,7 @@ __global__ void __launch_bounds__(kBlock, 2) tstep_kernel(Dev d, int64_t step0, 
 template <int LAW, bool SCE>
 __device__ __forceinline__ void lattice_forces(const Dev &d, int64_t n, bool valid, int own, bool safe,
                                                const double *sx, const double *sy, const double *sz,
-                                               const int4 *stab, const DictEntry *sdict, int ncache,
+                                               const LTab &tab, const DictEntry *sdict, int ncache,
                                                double &tx, double &ty, double &tz)
 {
     const int64_t nN = d.n_nodes;
@@ -1444,15 +1449,15 @@ __device__ __forceinline__ void lattice_forces(const Dev &d, int64_t n, bool val
     const int nsig = d.n_sigma;
     // state bytes and dictionary ids of one group of 4 chain positions
     uint32_t Sc[4], Cc[4], Sn[4], Cn[4];
+    // slot rows are padded by the stencil's reach on both sides, so every
+    // n + lower-node offset addresses a slot of the row (padding is absent)
     auto fetch = [&](int g, uint32_t *S, uint32_t *Cd) {
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const int4 t = stab[4 * g + q];
-            const int64_t lo = n + t.z;
-            const bool in = valid && (uint64_t)lo < (uint64_t)nN;
-            const int64_t slot = (int64_t)t.y + (in ? lo : 0);
-            S[q] = in ? (uint32_t)__ldcs(d.st + slot) : (uint32_t)LST_ABSENT;
-            Cd[q] = in ? (uint32_t)__ldcs(cids + slot) : 0u;
+            const int4 t = tab.e[4 * g + q];
+            const int64_t slot = (int64_t)t.y + n + t.z;
+            S[q] = (uint32_t)__ldcs(d.st + slot);
+            Cd[q] = (uint32_t)__ldcs(cids + slot);
         }
     };
     const int ng = nsig >> 2;
@@ -1464,16 +1469,18 @@ __device__ __forceinline__ void lattice_forces(const Dev &d, int64_t n, bool val
         // pass 1: the fast path of the group's four entries, without branches
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const int4 t = stab[4 * g + q];
+            const int4 t = tab.e[4 * g + q];
             const uint32_t sv = Sc[q];
-            const bool present = !(sv & LST_ABSENT);
+            const bool present = valid && !(sv & LST_ABSENT);
             const int p = own + t.x;
             // absent entries get finite stand-ins for the branch-free pass
             const double xj = present ? sx[p] : xi + 1.0;
             const double yj = present ? sy[p] : yi;
             const double zj = present ? sz[p] : zi;
-            const uint32_t c = Cc[q];
-            const DictEntry gd = ((int)c < ncache) ? sdict[c] : ldg_dict(d.dict, c);
+            const uint32_t c = present ? Cc[q] : 0u;
+            DictEntry gd;
+            if ((int)c < ncache) gd = sdict[c];
+            else gd = ldg_dict(d.dict, c);
             const int64_t slot = (int64_t)t.y + n + t.z;
             const double scv = SCE ? (present ? __ldcs(d.sce + slot) : d.P.sc) : d.P.sc;
             const int bt = (sv >> LST_BT_SHIFT) & 3;
@@ -1498,7 +1505,7 @@ __device__ __forceinline__ void lattice_forces(const Dev &d, int64_t n, bool val
                 const int sig = 4 * g + q;
                 double3 r = make_double3(fx[q], fy[q], fz[q]);
                 if (slow & (1u << q)) {
-                    const int4 t = stab[sig];
+                    const int4 t = tab.e[sig];
                     const int64_t slot = (int64_t)t.y + n + t.z;
                     const uint32_t sv = Sc[q];
                     const int p = own + t.x;
@@ -1522,11 +1529,11 @@ __device__ __forceinline__ void lattice_forces(const Dev &d, int64_t n, bool val
     tx = tx + ax; ty = ty + ay; tz = tz + az;
 }
 
-// Dynamic shared memory: the dictionary cache (ncache entries of 32 bytes),
-// the chain table (n_sigma int4) and the staged positions of one tile (x, y, z
-// arrays over the lsx * lsy * lsz box).
+// Dynamic shared memory: the dictionary cache (ncache entries of 32 bytes)
+// and the staged positions of one tile (x, y, z arrays over the lsx * lsy *
+// lsz box).
 template <int LAW, int SCHEME, bool SCE>
-__global__ void __launch_bounds__(kBlock, 2) lstep_kernel(Dev d, int64_t step0, int64_t nsteps)
+__global__ void __launch_bounds__(kBlock, 2) lstep_kernel(Dev d, int64_t step0, int64_t nsteps, LTab tab)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int64_t s_tile;
@@ -1534,17 +1541,15 @@ __global__ void __launch_bounds__(kBlock, 2) lstep_kernel(Dev d, int64_t step0, 
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t nN = d.n_nodes, nsl = d.n_slices;
-    const int ncache = d.ncache, nsig = d.n_sigma;
+    const int ncache = d.ncache;
     const int sxn = d.lsx, syn = d.lsy, szn = d.lsz, H = d.lhalo;
     const int box = sxn * syn * szn;
     const int64_t ntx = d.ltiles[0], nty = d.ltiles[1], ntiles = d.ltiles[0] * d.ltiles[1] * d.ltiles[2];
 
     DictEntry *sdict = reinterpret_cast<DictEntry *>(smem);
-    int4 *stab = reinterpret_cast<int4 *>(smem + (size_t)32 * ncache);
-    double *sx = reinterpret_cast<double *>(stab + nsig), *sy = sx + box, *sz = sy + box;
+    double *sx = reinterpret_cast<double *>(smem + (size_t)32 * ncache), *sy = sx + box, *sz = sy + box;
 
     for (int c = threadIdx.x; c < ncache; c += blockDim.x) sdict[c] = ldg_dict(d.dict, c);
-    for (int c = threadIdx.x; c < nsig; c += blockDim.x) stab[c] = d.ltab[c];
 
     // this warp's row in a tile
     const int wy = warp % d.lty, wz = warp / d.lty;
@@ -1585,7 +1590,7 @@ __global__ void __launch_bounds__(kBlock, 2) lstep_kernel(Dev d, int64_t step0, 
                 const bool valid = gx < d.lnx && gy < d.lny && gz < d.lnz;
                 const int64_t n = valid ? gx + (int64_t)d.lnx * (gy + (int64_t)d.lny * gz) : 0;
                 double tx, ty, tz;
-                lattice_forces<LAW, SCE>(d, n, valid, own, safe, sx, sy, sz, stab, sdict, ncache, tx, ty, tz);
+                lattice_forces<LAW, SCE>(d, n, valid, own, safe, sx, sy, sz, tab, sdict, ncache, tx, ty, tz);
                 if (valid) {
                     if (SCHEME == BBPD_SCHEME_EULERCROMER) {
                         ec_integrate_node<kP64>(d, b, n, tx, ty, tz, it);
@@ -2095,15 +2100,18 @@ kernel_t pick_tkernel(int law, int scheme, int prec, bool sce)
     }
 }
 
+typedef void (*lkernel_t)(Dev, int64_t, int64_t, LTab);
+static_assert(sizeof(Dev) + 16 + sizeof(LTab) <= 4096, "lattice kernel parameters exceed 4 KB");
+
 template <int LAW>
-kernel_t pick_lscheme(int scheme, bool sce)
+lkernel_t pick_lscheme(int scheme, bool sce)
 {
     if (scheme == BBPD_SCHEME_ADR) return sce ? lstep_kernel<LAW, BBPD_SCHEME_ADR, true> : lstep_kernel<LAW, BBPD_SCHEME_ADR, false>;
     return sce ? lstep_kernel<LAW, BBPD_SCHEME_EULERCROMER, true> : lstep_kernel<LAW, BBPD_SCHEME_EULERCROMER, false>;
 }
 
 // Lattice form: FP64, 16-bit dictionary ids.
-kernel_t pick_lkernel(int law, int scheme, bool sce)
+lkernel_t pick_lkernel(int law, int scheme, bool sce)
 {
     switch (law) {
     case BBPD_LAW_LINEAR: return pick_lscheme<BBPD_LAW_LINEAR>(scheme, sce);
@@ -2353,6 +2361,7 @@ struct bbpd_solver {
     int grid = 0;
     bool tiled = false;                 // tiled kernel with shared-memory staging
     bool lattice = false;               // lattice form (lstep_kernel)
+    LTab ltab{};                        // its chain table, a launch argument
     size_t smem = 0;                    // its dynamic shared memory per block
     bbpd_batch *batch = nullptr;        // batch this solver is a member of
     bool has_density = false;          // DENSITY given (contact needs it)
@@ -3081,25 +3090,31 @@ static int lattice_layout(bbpd_solver *S, const bbpd_problem *pb, FwdIds fwd_ids
     }
     const int lsx = 32 + 2 * H, lsy = bty + 2 * H, lsz = btz + 2 * H;
     auto lin = [&](const int3 &f) { return (int64_t)f.x + nx * ((int64_t)f.y + ny * (int64_t)f.z); };
+    // slot rows: one per forward offset plus an all-absent row for the table's
+    // padding entries, each padded by the stencil's reach M on both sides
+    int64_t M = 0;
+    for (const int3 &f : foff) M = std::max<int64_t>(M, lin(f));
+    const int64_t R = nN + 2 * M;
+    if ((int64_t)(NF + 1) * R >= ((int64_t)1 << 31)) return BBPD_OK;
     std::vector<int> back(NF);
     std::iota(back.begin(), back.end(), 0);
     std::sort(back.begin(), back.end(), [&](int a, int b) { return lin(foff[a]) > lin(foff[b]); });
     std::vector<int4> tab;
     for (int a : back) {
         const int3 &f = foff[a];
-        tab.push_back(make_int4(-(f.x + lsx * (f.y + lsy * f.z)), a * (int)nN, (int)-lin(f), 0));
+        tab.push_back(make_int4(-(f.x + lsx * (f.y + lsy * f.z)), (int)(a * R + M), (int)-lin(f), 0));
     }
     for (int a : pi) {
         const int3 &f = foff[a];
-        tab.push_back(make_int4(f.x + lsx * (f.y + lsy * f.z), a * (int)nN, 0, 0));
+        tab.push_back(make_int4(f.x + lsx * (f.y + lsy * f.z), (int)(a * R + M), 0, 0));
     }
-    while (tab.size() % 4) tab.push_back(make_int4(0, 0, -(1 << 30), 0));   // padding: never present
+    while (tab.size() % 4) tab.push_back(make_int4(0, (int)(NF * R + M), 0, 0));   // padding: the absent row
     const int nsig = (int)tab.size();
-    if (nsig > 255) return BBPD_OK;
-    // shared memory: positions of the staged box, the chain table, and as many
-    // of the most used dictionary entries as fit two blocks per SM
+    if (nsig > kMaxSigma) return BBPD_OK;
+    // shared memory: positions of the staged box and as many of the most used
+    // dictionary entries as fit two blocks per SM
     const size_t box = (size_t)lsx * lsy * lsz;
-    const size_t fixed = 24 * box + 16 * (size_t)nsig;
+    const size_t fixed = 24 * box;
     const size_t budget = 110 * 1024;
     if (fixed > budget) return BBPD_OK;
     const int ncache = (int)std::min<size_t>({(size_t)kDictCache, dict.size(), (budget - fixed) / 32});
@@ -3119,13 +3134,13 @@ static int lattice_layout(bbpd_solver *S, const bbpd_problem *pb, FwdIds fwd_ids
     Dev &d = S->d;
     keep_layout_pool(S->device);
     TempBufs tmp(st);
-    const int64_t NS = (int64_t)NF * nN;
+    const int64_t NS = (int64_t)(NF + 1) * R;
     uint32_t *slot = nullptr, *slot_bond = nullptr;
     TRY(tmp.get(&slot, (size_t)nB));
     TRY(staging::upload(slot, nB, st, [&](int64_t k0, int64_t c, uint32_t *out) {
         for (int64_t q = 0; q < c; q++) {
             const int64_t k = k0 + q;
-            out[q] = (uint32_t)((int64_t)bf[k] * nN + (int64_t)bl[k] - 1);
+            out[q] = (uint32_t)((int64_t)bf[k] * R + M + (int64_t)bl[k] - 1);
         }
     }));
     TRY(tmp.get(&slot_bond, (size_t)NS));
@@ -3177,9 +3192,8 @@ static int lattice_layout(bbpd_solver *S, const bbpd_problem *pb, FwdIds fwd_ids
         for (size_t q = 0; q < order.size(); q++) nd[q] = dict[order[q]];
         dict.swap(nd);
     }
-    int4 *ltab = nullptr;
-    TRY(S->put(&ltab, tab));
-    d.ltab = ltab;
+    std::memset(&S->ltab, 0, sizeof(LTab));
+    std::copy(tab.begin(), tab.end(), S->ltab.e);
     uint64_t *lcpos = nullptr;
     TRY(S->alloc(&lcpos, (size_t)nN));
     BBPD_CUDA_TRY(cudaMemcpyAsync(lcpos, cpos, sizeof(uint64_t) * nN, cudaMemcpyDeviceToDevice, st));
@@ -3642,7 +3656,7 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
 
     // kernel and grid
     if (S->lattice) {
-        S->kernel = pick_lkernel(prm->law, prm->scheme, pb->sc != nullptr);
+        S->kernel = reinterpret_cast<kernel_t>(pick_lkernel(prm->law, prm->scheme, pb->sc != nullptr));
         BBPD_CUDA_TRY(cudaFuncSetAttribute((const void *)S->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)S->smem));
     } else if (S->tiled) {
@@ -3706,7 +3720,7 @@ extern "C" int bbpd_step_async(bbpd_solver *S, int64_t nsteps)
     if (nsteps == 0) return BBPD_OK;
     BBPD_CUDA_TRY(cudaSetDevice(S->device));
     int64_t step0 = S->step;
-    void *args[] = {(void *)&S->d, (void *)&step0, (void *)&nsteps};
+    void *args[] = {(void *)&S->d, (void *)&step0, (void *)&nsteps, (void *)&S->ltab};   // lattice kernels take the table
     BBPD_CUDA_TRY(cudaMemsetAsync(S->d.work, 0, sizeof(unsigned long long), S->stream));
     BBPD_CUDA_TRY(cudaEventRecord(S->ev0, S->stream));
     BBPD_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)S->kernel, dim3(S->grid), dim3(kBlock), args, S->smem, S->stream));
