@@ -1432,38 +1432,43 @@ __global__ void __launch_bounds__(kBlock, 2) tstep_kernel(Dev d, int64_t step0, 
 // the Rayleigh-quotient sums run over 32-node slices after a grid barrier, in
 // the same tree as the other kernels.
 
-// Forces of lane's node n (own: its index in the staged box).
+// Forces of lane's node n (own: its index in the staged box). Every chain
+// position is computed without branches, absent ones included: their slot
+// holds dictionary id 0 and their staged partner a finite position (or 0
+// outside the lattice), and only present entries enter the sum.
 template <int LAW, bool SCE>
-__device__ __forceinline__ void lattice_forces(const Dev &d, int64_t n, bool valid, int own, bool safe,
+__device__ __forceinline__ void lattice_forces(const Dev &d, int n, bool valid, int own, bool safe,
                                                const double *sx, const double *sy, const double *sz,
                                                const LTab &tab, const DictEntry *sdict, int ncache,
                                                double &tx, double &ty, double &tz)
 {
-    const int64_t nN = d.n_nodes;
     const uint16_t *cids = reinterpret_cast<const uint16_t *>(d.cid);
+    const uint8_t *sts = d.st;
     const double xi = sx[own], yi = sy[own], zi = sz[own];
     uint64_t cp = valid ? __ldg(d.lcpos + n) : ~0ull;
     int nextc = (int)(cp & 0xFFu);
     tx = 0.0; ty = 0.0; tz = 0.0;
     double ax = 0.0, ay = 0.0, az = 0.0;
-    const int nsig = d.n_sigma;
-    // state bytes and dictionary ids of one group of 4 chain positions
+    const int ng = d.n_sigma >> 2;
+    // state bytes and dictionary ids of one group of 4 chain positions; slot
+    // rows are padded by the stencil's reach on both sides, so every
+    // n + lower-node offset addresses a slot of its row (padding is absent)
     uint32_t Sc[4], Cc[4], Sn[4], Cn[4];
-    // slot rows are padded by the stencil's reach on both sides, so every
-    // n + lower-node offset addresses a slot of the row (padding is absent)
-    auto fetch = [&](int g, uint32_t *S, uint32_t *Cd) {
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int4 t = tab.e[4 * g + q];
-            const int64_t slot = (int64_t)t.y + n + t.z;
-            S[q] = (uint32_t)__ldcs(d.st + slot);
-            Cd[q] = (uint32_t)__ldcs(cids + slot);
-        }
-    };
-    const int ng = nsig >> 2;
-    fetch(0, Sc, Cc);
+    for (int q = 0; q < 4; q++) {
+        const int slot = tab.e[q].y + n + tab.e[q].z;
+        Sc[q] = __ldcs(sts + slot);
+        Cc[q] = __ldcs(cids + slot);
+    }
     for (int g = 0; g < ng; g++) {
-        if (g + 1 < ng) fetch(g + 1, Sn, Cn);
+        if (g + 1 < ng) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int slot = tab.e[4 * g + 4 + q].y + n + tab.e[4 * g + 4 + q].z;
+                Sn[q] = __ldcs(sts + slot);
+                Cn[q] = __ldcs(cids + slot);
+            }
+        }
         double fx[4], fy[4], fz[4];
         unsigned slow = 0, pres = 0;
         // pass 1: the fast path of the group's four entries, without branches
@@ -1471,20 +1476,14 @@ __device__ __forceinline__ void lattice_forces(const Dev &d, int64_t n, bool val
         for (int q = 0; q < 4; q++) {
             const int4 t = tab.e[4 * g + q];
             const uint32_t sv = Sc[q];
-            const bool present = valid && !(sv & LST_ABSENT);
             const int p = own + t.x;
-            // absent entries get finite stand-ins for the branch-free pass
-            const double xj = present ? sx[p] : xi + 1.0;
-            const double yj = present ? sy[p] : yi;
-            const double zj = present ? sz[p] : zi;
-            const uint32_t c = present ? Cc[q] : 0u;
+            const double dX = sx[p] - xi, dY = sy[p] - yi, dZ = sz[p] - zi;
+            const uint32_t c = Cc[q];
             DictEntry gd;
             if ((int)c < ncache) gd = sdict[c];
             else gd = ldg_dict(d.dict, c);
-            const int64_t slot = (int64_t)t.y + n + t.z;
-            const double scv = SCE ? (present ? __ldcs(d.sce + slot) : d.P.sc) : d.P.sc;
+            const double scv = SCE ? __ldcs(d.sce + (t.y + n + t.z)) : d.P.sc;
             const int bt = (sv >> LST_BT_SHIFT) & 3;
-            const double dX = xj - xi, dY = yj - yi, dZ = zj - zi;
             const double L = sqrt(dX * dX + dY * dY + dZ * dZ);
             const double s = quot_rn(L - gd.l0, gd.l0, gd.rl0);
             bool okr;
@@ -1495,8 +1494,9 @@ __device__ __forceinline__ void lattice_forces(const Dev &d, int64_t n, bool val
             fx[q] = tt * quot_rn(dX, L, rL);
             fy[q] = tt * quot_rn(dY, L, rL);
             fz[q] = tt * quot_rn(dZ, L, rL);
-            if (present) pres |= 1u << q;
-            if (present && !fast) slow |= 1u << q;
+            const bool present = valid && !(sv & LST_ABSENT);
+            pres |= (present ? 1u : 0u) << q;
+            slow |= (present && !fast ? 1u : 0u) << q;
         }
         // pass 2: the rare general entries, and the sum in the reference's order
 #pragma unroll
@@ -1506,7 +1506,7 @@ __device__ __forceinline__ void lattice_forces(const Dev &d, int64_t n, bool val
                 double3 r = make_double3(fx[q], fy[q], fz[q]);
                 if (slow & (1u << q)) {
                     const int4 t = tab.e[sig];
-                    const int64_t slot = (int64_t)t.y + n + t.z;
+                    const int slot = t.y + n + t.z;
                     const uint32_t sv = Sc[q];
                     const int p = own + t.x;
                     const double scv = SCE ? __ldcs(d.sce + slot) : d.P.sc;
@@ -1588,7 +1588,7 @@ __global__ void __launch_bounds__(kBlock, 2) lstep_kernel(Dev d, int64_t step0, 
             if (wrow) {
                 const int gx = x0 + lane, gy = y0 + wy, gz = z0 + wz;
                 const bool valid = gx < d.lnx && gy < d.lny && gz < d.lnz;
-                const int64_t n = valid ? gx + (int64_t)d.lnx * (gy + (int64_t)d.lny * gz) : 0;
+                const int n = valid ? gx + d.lnx * (gy + d.lny * gz) : 0;
                 double tx, ty, tz;
                 lattice_forces<LAW, SCE>(d, n, valid, own, safe, sx, sy, sz, tab, sdict, ncache, tx, ty, tz);
                 if (valid) {

@@ -378,7 +378,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=list(CONFIGS))
     ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--node-order", default="lattice", choices=["input", "morton", "tiled", "lattice"])
+    ap.add_argument("--node-order", default="input", choices=["input", "morton", "tiled", "lattice"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving sample of the default line")
