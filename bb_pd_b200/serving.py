@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import dataclasses
 import time
+from typing import Any
 from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
@@ -37,11 +38,24 @@ LAWKW = {
 class Request:
     id: int
     arrival: float              # seconds after the start of the run
-    inp: dict                   # beam arrays (beam.build)
+    inp: Any                    # beam arrays (beam.build), or a callable that builds them on admission
     law: str
     rate: float                 # prescribed displacement per step (m)
     max_steps: int
     post_peak: float = 0.8      # stop once |load| <= post_peak * peak after the peak
+    sizes: tuple | None = None  # (nodes, bonds, per-bond sc) when inp is built on admission
+
+    def counts(self) -> tuple:
+        """(nodes, bonds, per-bond critical stretch) without building the arrays."""
+        if isinstance(self.inp, dict):
+            return int(self.inp["nNodes"]), int(self.inp["nBonds"]), "sc" in self.inp
+        return self.sizes
+
+    def arrays(self) -> dict:
+        """The beam arrays (built now when the request holds a builder): a
+        stream of large solves then keeps only admitted requests' arrays on
+        the host, and only until their solvers exist."""
+        return self.inp if isinstance(self.inp, dict) else self.inp()
 
 
 @dataclasses.dataclass
@@ -99,7 +113,7 @@ class _Track:
 
 
 def _new_solver(req: Request, precision: str, device: int) -> Solver:
-    return Solver(req.inp, device=device, scheme="adr", rate=req.rate, precision=precision,
+    return Solver(req.arrays(), device=device, scheme="adr", rate=req.rate, precision=precision,
                   **LAWKW[req.law])
 
 
@@ -126,7 +140,8 @@ def run_batched(requests: list[Request], *, hbm_budget: float = 150e9, precision
             now = time.perf_counter() - t0
             while pending and pending[0].arrival <= now:
                 r = pending[0]
-                est = device_bytes_estimate(r.inp, "sc" in r.inp)
+                nn, nb, sc = r.counts()
+                est = device_bytes_estimate({"nNodes": nn, "nBonds": nb}, sc)
                 if (active or creating) and used + reserved + est > hbm_budget:
                     break                   # wait for a solve to finish
                 creating.append((r, pool.submit(_new_solver, r, precision, device), est))
@@ -168,7 +183,7 @@ def run_batched(requests: list[Request], *, hbm_budget: float = 150e9, precision
                 used -= nbytes
                 active.remove(item)
                 results.append(Result(r.id, r.arrival, ta, tnow, tr.steps, tr.peak, tr.peak_step,
-                                      float(r.inp["nBonds"]) * tr.steps, np.concatenate(tr.hist)))
+                                      float(r.counts()[1]) * tr.steps, np.concatenate(tr.hist)))
     finally:
         pool.shutdown(wait=True)
         batch.close()
@@ -195,7 +210,7 @@ def run_sequential(requests: list[Request], *, precision: str = "fp64", chunk: i
                 break
         s.close()
         results.append(Result(r.id, r.arrival, ta, time.perf_counter() - t0, tr.steps, tr.peak,
-                              tr.peak_step, float(r.inp["nBonds"]) * tr.steps, np.concatenate(tr.hist)))
+                              tr.peak_step, float(r.counts()[1]) * tr.steps, np.concatenate(tr.hist)))
     return results, dict(wall=time.perf_counter() - t0)
 
 

@@ -256,8 +256,11 @@ def run_serve(args):
     import bb_pd_b200 as bb
     from bb_pd_b200 import serving
     stream = bb.beam.serving_stream(args.requests, nodes_range=(1e4, args.max_nodes), rate_hz=args.arrival_hz)
-    reqs = [serving.Request(k, r["arrival"], bb.beam.build(r["spec"]), r["law"], args.serve_rate, args.max_steps)
-            for k, r in enumerate(stream)]
+    reqs = []
+    for k, r in enumerate(stream):   # arrays built on admission: the full stream does not fit host memory
+        c = bb.beam.count(r["spec"])
+        reqs.append(serving.Request(k, r["arrival"], (lambda sp=r["spec"]: bb.beam.build(sp)), r["law"],
+                                    args.serve_rate, args.max_steps, sizes=(c.n_nodes, c.n_bonds, False)))
     clocks = Clocks(0)
     clocks.start()
     res, st = serving.run_batched(reqs, precision=args.form, chunk=100)
