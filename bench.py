@@ -196,6 +196,7 @@ def run_batch(args):
     t_create = time.perf_counter() - t_create
     tot_b = float(sum(bonds))
     batch = bb.Batch(args.form)
+    batch.set_mixing(args.batch_mixed != 0)
     for s in sol:
         batch.add(s)
     if args.batch_schedule:   # a fixed schedule instead of the autotuner (profiling one kernel)
@@ -218,13 +219,13 @@ def run_batch(args):
     seq_ms = 0.0
     for s in sol:
         s.close()
-    for sp, law in series:
+    for sp, law in ([] if args.no_sequential else series):
         s = mk(bb.beam.build(sp), law, "fp64")
         s.step(args.warmup)
         s.step(args.steps)
         seq_ms += s.last_kernel_ms()
         s.close()
-    seq = tot_b * args.steps / (seq_ms / 1e3)
+    seq = tot_b * args.steps / (seq_ms / 1e3) if seq_ms > 0 else float("nan")
     peak, kind = peak_hbm()
     alg = sum(algorithmic_bytes(n, b, True) for n, b in zip(nodes, bonds))
     ach = alg / (ms / args.steps / 1e3) / 1e9
@@ -391,6 +392,8 @@ def main():
     ap.add_argument("--members", type=int, default=64, help="batch: beams in the size-effect series")
     ap.add_argument("--dx", type=float, default=5e-3, help="batch: lattice spacing of the series (m)")
     ap.add_argument("--batch-schedule", default="", help="batch: 'blocks_per_sm,grab' instead of autotuning")
+    ap.add_argument("--batch-mixed", type=int, default=1, help="batch: 1 one launch for all laws, 0 one per law")
+    ap.add_argument("--no-sequential", action="store_true", help="batch: skip the one-beam-at-a-time baseline")
     ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")
     ap.add_argument("--max-nodes", type=float, default=3e5, help="serve: largest beam (nodes)")
     ap.add_argument("--arrival-hz", type=float, default=4.0, help="serve: Poisson arrival rate")
