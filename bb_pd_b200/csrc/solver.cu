@@ -684,133 +684,6 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
     tx = tx + ax; ty = ty + ay; tz = tz + az;
 }
 
-// Asynchronous copies (cp.async, Ampere and later) of 16 bytes into shared
-// memory: the data in flight holds no registers.
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc)
-{
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-// Shared memory per warp of slice_forces_async: two stages x 4 entries x 32
-// lanes of 32-byte position records.
-constexpr int kPosStageBytes = 4 * 32 * 32;
-constexpr size_t kAsyncSmem = (size_t)(kBlock / 32) * 2 * kPosStageBytes;
-
-// slice_forces with the neighbour positions of the next group of 4 entries
-// copied asynchronously into this warp's shared memory while the current
-// group is computed (streams load two groups ahead). Each lane copies and
-// reads only its own slots, so its own wait orders them; the arithmetic and
-// the order of the sums are those of slice_forces.
-template <int LAW, int PREC, class CID, int SCE>
-__device__ __forceinline__ void slice_forces_async(const Dev &d, int64_t sl, int lane, bool safe,
-                                                   const double *xs, const double4 *xa, double4 *pbuf,
-                                                   double &tx, double &ty, double &tz)
-{
-    const int64_t nN = d.n_nodes;
-    const int64_t i = sl * 32 + lane;
-    const int dg = (i < nN) ? d.deg[i] : 0;
-    const int64_t sb = d.slice_ptr[sl];
-    const double *x0 = xs, *x1 = xs + nN, *x2 = xs + 2 * nN;
-
-    double xi = 0, yi = 0, zi = 0;
-    if (i < nN) { xi = x0[i]; yi = x1[i]; zi = x2[i]; }
-    tx = 0.0; ty = 0.0; tz = 0.0;
-    double ax = 0.0, ay = 0.0, az = 0.0;
-
-    const int ng = (dg + 3) >> 2;
-    // copy the position records of group gg (streams G) into stage gg & 1
-    auto issue = [&](int gg, const Group<CID> &G) {
-        const int nq = min(4, dg - 4 * gg);
-        double4 *st = pbuf + (gg & 1) * 128;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (q < nq) {
-                const uint32_t j = group_w(G, q) & COL_MASK;
-                cp_async16(st + q * 32 + lane, xa + j);
-                cp_async16(reinterpret_cast<char *>(st + q * 32 + lane) + 16,
-                           reinterpret_cast<const char *>(xa + j) + 16);
-            }
-        }
-        cp_async_commit();
-    };
-    Group<CID> Gc, Gn, Gnn;
-    int64_t e0 = entry_pos(sb, 0, lane);
-    if (ng > 0) load_group<CID>(d, e0, Gc);
-    if (ng > 1) load_group<CID>(d, e0 + 128, Gn);
-    if (ng > 0) issue(0, Gc);
-    for (int g = 0; g < ng; g++, e0 += 128) {
-        if (g + kPrefetch < ng) prefetch_group<CID, SCE>(d, e0 + 128 * kPrefetch);
-        if (g + 2 < ng) load_group<CID>(d, e0 + 256, Gnn);
-        if (g + 1 < ng) {
-            issue(g + 1, Gn);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        const double4 *st = pbuf + (g & 1) * 128;
-        const int nq = min(4, dg - 4 * g);
-        double xj[4], yj[4], zj[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (q < nq) {
-                const double4 r = st[q * 32 + lane];
-                xj[q] = r.x; yj[q] = r.y; zj[q] = r.z;
-            } else {   // unused slot: finite values for the branch-free pass
-                xj[q] = xi + 1.0; yj[q] = yi; zj[q] = zi;
-            }
-        }
-        // pass 1: the fast path of all entries of the group, without branches
-        double fx[4], fy[4], fz[4];
-        unsigned slow = 0;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const bool valid = q < nq;
-            const uint32_t w = group_w(Gc, q), c = valid ? Gc.cid(q) : 0u, sv = (Gc.s >> (8 * q)) & 0xFFu;
-            const DictEntry gd = ldg_dict(d.dict, c);
-            const double scv = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
-            const double s0b = d.s0e ? __ldg(d.s0e + e0 + q) : d.P.s0;
-            const int bt = (w >> BT_SHIFT) & 3;
-            const double dX = xj[q] - xi, dY = yj[q] - yi, dZ = zj[q] - zi;
-            const double L = sqrt(dX * dX + dY * dY + dZ * dZ);
-            const double s = quot_rn(L - gd.l0, gd.l0, gd.rl0);
-            bool okr;
-            const double rL = recip_rn(L, okr);
-            const bool fast = safe && okr && sv == 0 && gd.rl0 > 0 && L > 0 && law_quiet<LAW>(d.P, bt, s, s0b, scv);
-            const double t = ((gd.bs * s) * d.V) * gd.vcf;
-            fx[q] = t * quot_rn(dX, L, rL);
-            fy[q] = t * quot_rn(dY, L, rL);
-            fz[q] = t * quot_rn(dZ, L, rL);
-            if (valid && !fast) slow |= 1u << q;
-        }
-        // pass 2: the rare general entries, and the sum in the reference's order
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (q < nq) {
-                const uint32_t w = group_w(Gc, q);
-                double3 r = make_double3(fx[q], fy[q], fz[q]);
-                if (slow & (1u << q)) {
-                    const uint32_t j = w & COL_MASK;
-                    const double scv = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
-                    r = entry_general<LAW, PREC>(d, e0 + q, w, (Gc.s >> (8 * q)) & 0xFFu,
-                                                 ldg_dict(d.dict, Gc.cid(q)), scv, xi, yi, zi, x0[j], x1[j], x2[j]);
-                }
-                if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
-                    tx = tx + ax; ty = ty + ay; tz = tz + az;
-                    ax = 0.0; ay = 0.0; az = 0.0;
-                }
-                ax = ax + r.x; ay = ay + r.y; az = az + r.z;
-            }
-        }
-        Gc = Gn;
-        Gn = Gnn;
-    }
-    tx = tx + ax; ty = ty + ay; tz = tz + az;
-}
-
 // General path of the FP32 dictionary-vector form: FP64 positions of both
 // nodes, then the general entry in difference form.
 template <int LAW>
@@ -938,136 +811,6 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
 }
 
 
-
-// slice_forces_x with the neighbours' FP32 displacement records (16 + 8 bytes)
-// of the next group copied asynchronously into this warp's shared memory
-// while the current group is computed; arithmetic and order of the sums are
-// those of slice_forces_x.
-template <int LAW, class CID, int SCE>
-__device__ __forceinline__ void slice_forces_x_async(const Dev &d, int64_t sl, int lane, const double *xs,
-                                                     const float4 *urh, const float2 *url, double4 *pbuf,
-                                                     double &tx, double &ty, double &tz)
-{
-    const int64_t nN = d.n_nodes;
-    const int64_t i = sl * 32 + lane;
-    const int dg = (i < nN) ? d.deg[i] : 0;
-    const int64_t sb = d.slice_ptr[sl];
-    // stage layout: 4 x 32 float4, then 4 x 32 float2 (3 KB of the stage's 4 KB)
-    float4 *ph = reinterpret_cast<float4 *>(pbuf);
-    auto stage_h = [&](int gg) { return ph + (gg & 1) * 256; };
-    auto stage_l = [&](int gg) { return reinterpret_cast<float2 *>(ph + (gg & 1) * 256 + 128); };
-
-    float4 ui = make_float4(0.f, 0.f, 0.f, 0.f);
-    float2 li = make_float2(0.f, 0.f);
-    if (i < nN) { ui = urh[i]; li = url[i]; }
-    tx = 0.0; ty = 0.0; tz = 0.0;
-    double ax = 0.0, ay = 0.0, az = 0.0;
-    const float s0f = (float)d.P.s0, guardf = (float)d.guard, scf0 = (float)d.P.sc;
-    const float steelf = (float)d.P.sc_steel;
-
-    const int ng = (dg + 3) >> 2;
-    auto issue = [&](int gg, const Group<CID> &G) {
-        const int nq = min(4, dg - 4 * gg);
-        float4 *h = stage_h(gg);
-        float2 *l = stage_l(gg);
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (q < nq) {
-                const uint32_t j = group_w(G, q) & COL_MASK;
-                cp_async16(h + q * 32 + lane, urh + j);
-                const unsigned sa = (unsigned)__cvta_generic_to_shared(l + q * 32 + lane);
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(url + j) : "memory");
-            }
-        }
-        cp_async_commit();
-    };
-    Group<CID> Gc, Gn, Gnn;
-    int64_t e0 = entry_pos(sb, 0, lane);
-    if (ng > 0) load_group<CID>(d, e0, Gc);
-    if (ng > 1) load_group<CID>(d, e0 + 128, Gn);
-    if (ng > 0) issue(0, Gc);
-    for (int g = 0; g < ng; g++, e0 += 128) {
-        if (g + kPrefetch < ng) prefetch_group<CID, SCE>(d, e0 + 128 * kPrefetch);
-        if (g + 2 < ng) load_group<CID>(d, e0 + 256, Gnn);
-        if (g + 1 < ng) {
-            issue(g + 1, Gn);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        const int nq = min(4, dg - 4 * g);
-        const float4 *h = stage_h(g);
-        const float2 *l = stage_l(g);
-        float4 uj[4];
-        float2 lj[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (q < nq) {
-                uj[q] = h[q * 32 + lane];
-                lj[q] = l[q * 32 + lane];
-            } else {   // unused slot: finite values for the branch-free pass
-                uj[q] = ui;
-                lj[q] = li;
-            }
-        }
-        float fxq[4], fyq[4], fzq[4];
-        unsigned slow = 0;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const bool valid = q < nq;
-            const int64_t e = e0 + q;
-            const uint32_t w = group_w(Gc, q), c = valid ? Gc.cid(q) : 0u, sv = (Gc.s >> (8 * q)) & 0xFFu;
-            const int bt = (w >> BT_SHIFT) & 3;
-            float4 A, Bv;
-            ldg_dictx(d.dictx, c, A, Bv);
-            const float etx = (uj[q].x - ui.x) + (uj[q].w - ui.w);
-            const float ety = (uj[q].y - ui.y) + (lj[q].x - li.x);
-            const float etz = (uj[q].z - ui.z) + (lj[q].y - li.y);
-            const float ex = A.x + etx, ey = A.y + ety, ez = A.z + etz;
-            const float L2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
-            const float rL = rsqrtf(L2);
-            const float L = L2 * rL;
-            const float num = __fmaf_rn(etz, A.z + ez, __fmaf_rn(ety, A.y + ey, __fmaf_rn(etx, A.x + ex, Bv.y)));
-            const float sf = __fdividef(num, A.w * (L + A.w));
-            const float scf = has_sce<SCE>(d) ? (float)__ldcs(d.sce + e) : scf0;
-            bool fast;
-            if (LAW == BBPD_LAW_LINEAR) {
-                const float critf = (bt == 0) ? scf : (bt == 1 ? 3.f * scf : steelf);
-                fast = sf <= __fsub_rd(critf, guardf);
-            } else {
-                const float top = (bt == 0) ? (d.s0e ? (float)__ldg(d.s0e + e) : s0f) : INFINITY;
-                fast = sf <= top && (sf <= __fsub_rd(scf, guardf) || sf >= __fadd_ru(scf, guardf));
-            }
-            fast = fast && sv == 0 && Bv.z != 0.f;
-            const float qf = Bv.x * sf * rL;
-            fxq[q] = qf * ex;
-            fyq[q] = qf * ey;
-            fzq[q] = qf * ez;
-            if (valid && !fast) slow |= 1u << q;
-        }
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (q < nq) {
-                const uint32_t w = group_w(Gc, q);
-                double3 r;
-                if (slow & (1u << q)) {
-                    const double scd = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
-                    r = entry_general_x<LAW>(d, e0 + q, w, (Gc.s >> (8 * q)) & 0xFFu, Gc.cid(q), scd, i, xs);
-                } else {
-                    r = make_double3((double)fxq[q], (double)fyq[q], (double)fzq[q]);
-                }
-                if (w & F_CHUNK) {  // partial of the previous OpenMP thread is complete
-                    tx = tx + ax; ty = ty + ay; tz = tz + az;
-                    ax = 0.0; ay = 0.0; az = 0.0;
-                }
-                ax = ax + r.x; ay = ay + r.y; az = az + r.z;
-            }
-        }
-        Gc = Gn;
-        Gn = Gnn;
-    }
-    tx = tx + ax; ty = ty + ay; tz = tz + az;
-}
 
 // Coordinates for which the shared-divisor division of divide.cuh is exact:
 // +0, or a magnitude in [2^-100, 2^100] (a -0 coordinate could make a -0
@@ -1345,12 +1088,10 @@ __device__ __forceinline__ void adr_update(const Dev &d, const StepBufs &b, int 
 // Global-gather kernel: neighbour data read from HBM/L2 per entry. Used for
 // inputs whose tiles do not fit shared memory, and for input or plain Morton
 // node order.
-template <int LAW, int SCHEME, int PREC, class CID, bool SCE, bool ASYNC = false>
+template <int LAW, int SCHEME, int PREC, class CID, bool SCE>
 __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : BBPD_MIN_BLOCKS) step_kernel(Dev d, int64_t step0, int64_t nsteps)
 {
-    extern __shared__ __align__(16) unsigned char smem[];   // ASYNC: the warps' position stages
     const int lane = threadIdx.x & 31;
-    double4 *pbuf = reinterpret_cast<double4 *>(smem) + (threadIdx.x >> 5) * (2 * 128);
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t nsl = d.n_slices;
@@ -1373,10 +1114,7 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
             const int64_t sl_next = grab_slice(d, lane) - base;
             prefetch_slice_head<CID, SCE>(d, sl_next, lane);
             double tx, ty, tz;
-            if (PREC == kP32X && ASYNC)
-                slice_forces_x_async<LAW, CID, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, pbuf, tx, ty, tz);
-            else if (PREC == kP32X) slice_forces_x<LAW, CID, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
-            else if (ASYNC) slice_forces_async<LAW, PREC, CID, SCE>(d, sl, lane, safe, b.xs, b.xas, pbuf, tx, ty, tz);
+            if (PREC == kP32X) slice_forces_x<LAW, CID, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
             else slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, b.xs, b.xas, tx, ty, tz);
             finish_slice<SCHEME, PREC>(d, b, sl, lane, tx, ty, tz, it);
             sl = sl_next;
@@ -2321,29 +2059,6 @@ kernel_t pick_cid(bool wide, bool sce)
         if (wide) return step_kernel<LAW, SCHEME, PREC, uint32_t, true>;
     }
     return sce ? step_kernel<LAW, SCHEME, PREC, uint16_t, true> : step_kernel<LAW, SCHEME, PREC, uint16_t, false>;
-}
-
-// FP64 form with the neighbour positions prefetched asynchronously
-// (slice_forces_async, kAsyncSmem bytes of shared memory per block).
-template <int LAW, int SCHEME>
-kernel_t pick_async(int prec, bool sce)
-{
-    if (prec == kP32X)
-        return sce ? step_kernel<LAW, SCHEME, kP32X, uint16_t, true, true>
-                   : step_kernel<LAW, SCHEME, kP32X, uint16_t, false, true>;
-    return sce ? step_kernel<LAW, SCHEME, kP64, uint16_t, true, true>
-               : step_kernel<LAW, SCHEME, kP64, uint16_t, false, true>;
-}
-
-kernel_t pick_async_kernel(int law, int scheme, int prec, bool sce)
-{
-    const bool adr = scheme == BBPD_SCHEME_ADR;
-    switch (law) {
-    case BBPD_LAW_LINEAR: return adr ? pick_async<BBPD_LAW_LINEAR, BBPD_SCHEME_ADR>(prec, sce) : pick_async<BBPD_LAW_LINEAR, BBPD_SCHEME_EULERCROMER>(prec, sce);
-    case BBPD_LAW_BILINEAR: return adr ? pick_async<BBPD_LAW_BILINEAR, BBPD_SCHEME_ADR>(prec, sce) : pick_async<BBPD_LAW_BILINEAR, BBPD_SCHEME_EULERCROMER>(prec, sce);
-    case BBPD_LAW_TRILINEAR: return adr ? pick_async<BBPD_LAW_TRILINEAR, BBPD_SCHEME_ADR>(prec, sce) : pick_async<BBPD_LAW_TRILINEAR, BBPD_SCHEME_EULERCROMER>(prec, sce);
-    default: return adr ? pick_async<BBPD_LAW_EXPONENTIAL, BBPD_SCHEME_ADR>(prec, sce) : pick_async<BBPD_LAW_EXPONENTIAL, BBPD_SCHEME_EULERCROMER>(prec, sce);
-    }
 }
 
 template <int LAW, int SCHEME>
@@ -3948,14 +3663,6 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
         S->kernel = pick_tkernel(prm->law, prm->scheme, S->prec, pb->sc != nullptr);
         BBPD_CUDA_TRY(cudaFuncSetAttribute((const void *)S->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)S->smem));
-    } else if (!S->wide && !(std::getenv("BBPD_ASYNC_GATHER") &&
-                             std::strcmp(std::getenv("BBPD_ASYNC_GATHER"), "0") == 0)) {
-        // 16-bit ids: neighbour records prefetched asynchronously
-        // (BBPD_ASYNC_GATHER=0 selects the register-gather kernels)
-        S->kernel = pick_async_kernel(prm->law, prm->scheme, S->prec, pb->sc != nullptr);
-        S->smem = kAsyncSmem;
-        BBPD_CUDA_TRY(cudaFuncSetAttribute((const void *)S->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)S->smem));
     } else {
         S->kernel = pick_kernel(prm->law, prm->scheme, S->prec, S->wide, pb->sc != nullptr);
     }
@@ -4393,6 +4100,7 @@ struct bbpd_batch {
     double timeout_s = 2.0;
     bool use_graph = true;                 // replay the launches from a captured CUDA graph
     bool mixed = true;                     // all laws of a precision variant in one launch
+    bool mixing_fixed = false;             // set by bbpd_batch_set_mixing; else the tuner chooses
     cudaGraphExec_t gexec = nullptr;
     int64_t g_nsteps = -1;
     int g_bps = 0, g_grab = 0;
@@ -4697,24 +4405,39 @@ extern "C" int bbpd_batch_tune(bbpd_batch *B, int64_t nsteps_per_trial, int *blo
     if (B->members.empty()) return fail(BBPD_ERR_ARG, "empty batch");
     BBPD_CUDA_TRY(cudaSetDevice(B->device));
     if (B->dirty) TRY(batch_rebuild(B));
-    // Candidate schedules: resident blocks per SM x slices per grab. Every
-    // trial runs real steps of the members, so tuning costs no extra work.
+    // Candidate schedules: resident blocks per SM x slices per grab, and,
+    // unless the caller fixed it, one launch for all laws or one per law.
+    // Every trial runs real steps of the members, so tuning costs no extra
+    // work; trials of the same length compare the same steps' work.
     float best = 0;
     int bb = B->occ, bg = 1;
-    bool first = true;
-    for (int bps = 1; bps <= B->occ; bps++)
-        for (int g : {1, 2, 4}) {
-            TRY(batch_launch(B, nsteps_per_trial, bps, g, false));
-            TRY(batch_finish(B, nsteps_per_trial));
-            float ms = 0;
-            BBPD_CUDA_TRY(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
-            if (first || ms < best) {
-                best = ms;
-                bb = bps;
-                bg = g;
-                first = false;
-            }
+    bool bmix = B->mixed, first = true;
+    std::vector<bool> mixes = {B->mixed};
+    if (!B->mixing_fixed) mixes = {true, false};
+    for (bool mix : mixes) {
+        if (mix != B->mixed) {
+            B->mixed = mix;
+            TRY(batch_rebuild(B));
         }
+        for (int bps = 1; bps <= B->occ; bps++)
+            for (int g : {1, 2, 4}) {
+                TRY(batch_launch(B, nsteps_per_trial, bps, g, false));
+                TRY(batch_finish(B, nsteps_per_trial));
+                float ms = 0;
+                BBPD_CUDA_TRY(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
+                if (first || ms < best) {
+                    best = ms;
+                    bb = bps;
+                    bg = g;
+                    bmix = mix;
+                    first = false;
+                }
+            }
+    }
+    if (bmix != B->mixed) {
+        B->mixed = bmix;
+        TRY(batch_rebuild(B));
+    }
     B->blocks_per_sm = bb;
     B->grab = bg;
     B->tuned = true;
@@ -4739,6 +4462,7 @@ extern "C" int bbpd_batch_set_mixing(bbpd_batch *B, int mixed)
     if (!B) return fail(BBPD_ERR_ARG, "null batch");
     TRY(batch_member_changed(B));
     B->mixed = mixed != 0;
+    B->mixing_fixed = true;
     return BBPD_OK;
 }
 
