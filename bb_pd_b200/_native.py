@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
         L.bbpd_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
         L.bbpd_selftest_wait_timeout.argtypes = [C.c_double]
         L.bbpd_selftest_division.argtypes = [C.c_int64, C.c_uint64] + [C.POINTER(C.c_int64)] * 3 + [_P]
+        L.bbpd_selftest_fp64_peak.argtypes = [C.c_double, _P]
         L.bbpd_selftest_exp.argtypes = [C.c_double, C.c_double, C.c_int64, C.c_uint64, C.POINTER(C.c_int64),
                                         C.POINTER(C.c_uint64)]
         L.bbpd_get_reaction.argtypes = [C.c_void_p, C.c_int64, _P]

@@ -3,6 +3,7 @@
 #include "crexp.cuh"
 #include "divide.cuh"
 
+#include <algorithm>
 #include <cstring>
 
 using namespace bbpd;
@@ -102,7 +103,61 @@ __global__ void exp_selftest_kernel(double lo, double hi, int64_t n, uint64_t se
     atomicAdd(&out[1], sum);
 }
 
+// FP64 issue rate: every thread runs 8 independent chains of dependent
+// fused multiply-adds (enough to cover the pipe's latency at 8 warps per
+// SMSP); the result is written so that nothing is optimised away.
+__global__ void fp64_peak_kernel(int64_t iters, double seed, double *out)
+{
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = seed + k * 1e-3 + threadIdx.x * 1e-9;
+    const double m = 0.999999999, c = 1e-12;
+    for (int64_t it = 0; it < iters; it++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = __fma_rn(a[k], m, c);
+    }
+    double t = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) t += a[k];
+    if (t == 42.0) out[0] = t;   // practically never; keeps the chains live
+}
+
 }  // namespace
+
+extern "C" int bbpd_selftest_fp64_peak(double seconds_target, double *fma_lanes_per_s)
+{
+    int rc = require_device();
+    if (rc) return rc;
+    if (!fma_lanes_per_s || !(seconds_target > 0)) return fail(BBPD_ERR_ARG, "bad argument");
+    int nsm = 0, dev = 0;
+    BBPD_CUDA_TRY(cudaGetDevice(&dev));
+    BBPD_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    double *dout = nullptr;
+    BBPD_CUDA_TRY(cudaMalloc(&dout, sizeof(double)));
+    cudaEvent_t e0, e1;
+    BBPD_CUDA_TRY(cudaEventCreate(&e0));
+    BBPD_CUDA_TRY(cudaEventCreate(&e1));
+    const int blocks = nsm * 8, threads = 256;
+    int64_t iters = 1 << 14;
+    float ms = 0;
+    cudaError_t e = cudaSuccess;
+    for (int round = 0; round < 6 && e == cudaSuccess; round++) {   // grow until the target time
+        cudaEventRecord(e0);
+        fp64_peak_kernel<<<blocks, threads>>>(iters, 1.0, dout);
+        cudaEventRecord(e1);
+        e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess || ms >= 1e3 * seconds_target) break;
+        iters = (int64_t)(iters * std::max(2.0, 1e3 * seconds_target / std::max(ms, 0.01f)));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(BBPD_ERR_CUDA, "fp64 peak: %s", cudaGetErrorString(e));
+    *fma_lanes_per_s = (double)blocks * threads * 8.0 * (double)iters / (ms * 1e-3);
+    return BBPD_OK;
+}
 
 extern "C" int bbpd_selftest_exp(double lo, double hi, int64_t n, uint64_t seed, int64_t *fast_vs_accurate,
                                  uint64_t *bits_sum)

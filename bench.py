@@ -55,6 +55,27 @@ def peak_hbm():
         return 6650.0, "fallback"
 
 
+def fp64_per_step(cfg, form, node_order):
+    """FP64 thread-instructions per time step of the step kernel from an ncu
+    count of this workload (profiles/step_kernel_fp64_inst.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "step_kernel_fp64_inst.json")) as f:
+            t = json.load(f)[cfg][form][node_order]
+        return float(t["fp64_thread_inst_per_step"]), t.get("source")
+    except Exception:
+        return None, None
+
+
+def fp64_peak():
+    """Measured FP64 FMA lane-operations per second of this device
+    (bbpd_selftest_fp64_peak: independent FMA chains, CUDA events)."""
+    import ctypes as C
+    from bb_pd_b200 import _native as N
+    v = C.c_double()
+    N.check(N.lib().bbpd_selftest_fp64_peak(0.3, C.byref(v)))
+    return v.value
+
+
 def measured_traffic(cfg, form):
     """DRAM bytes (read + write) per time step of the step kernel from an ncu
     capture of this workload (profiles/step_kernel_traffic.json), or None."""
@@ -522,6 +543,13 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic, "traffic_source": tsrc, "per": "time step",
                 "algorithmic_bytes_per_step": alg, "layout_bytes_per_step": info["bytes_per_step"]}
+    f64, f64src = fp64_per_step(args.config, args.form, args.node_order)
+    if f64 is not None:
+        pk = fp64_peak()
+        ach64 = f64 / (ms_step / 1e3)
+        roofline["fp64"] = {"achieved": ach64, "peak": pk, "unit": "FP64 thread-instructions/s",
+                            "frac": ach64 / pk, "inst_per_step": f64, "source": f64src,
+                            "peak_kind": "measured now (bbpd_selftest_fp64_peak: FMA chains)"}
 
     cpu = None
     if not args.no_cpu_baseline and world == 1:

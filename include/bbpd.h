@@ -607,6 +607,13 @@ int bbpd_selftest_division(int64_t n, uint64_t seed, int64_t *recip_mismatches,
 int bbpd_selftest_exp(double lo, double hi, int64_t n, uint64_t seed, int64_t *fast_vs_accurate,
                       uint64_t *bits_sum);
 
+/* Measurement: the device's FP64 issue rate, from independent chains of
+ * fused multiply-adds timed with CUDA events over about seconds_target
+ * seconds; reports FP64 FMA lane-operations per second (each one FP64
+ * instruction for one thread; FLOP/s is twice that). The denominator of the
+ * bench line's FP64 roofline. */
+int bbpd_selftest_fp64_peak(double seconds_target, double *fma_lanes_per_s);
+
 /* ===================================================================== *
  *  Synthetic beam builder (the inputs of input/scripts/Gregoire_beam_    *
  *  tests.m and the functions it calls, for a regular lattice).          *
