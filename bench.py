@@ -217,7 +217,8 @@ def run_batch(args):
     t_create = time.perf_counter() - t_create
     tot_b = float(sum(bonds))
     batch = bb.Batch(args.form)
-    batch.set_mixing(args.batch_mixed != 0)
+    if args.batch_mixed >= 0:
+        batch.set_mixing(args.batch_mixed != 0)
     for s in sol:
         batch.add(s)
     if args.batch_schedule:   # a fixed schedule instead of the autotuner (profiling one kernel)
@@ -263,7 +264,9 @@ def run_batch(args):
         "speedup_vs_sequential_fp64": value / seq if seq else None,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                      "peak_kind": peak_kind_str(kind), "traffic": None},
-        "schedule": {"blocks_per_sm": bps, "grab": grab, "graph": bool(info["graph"])},
+        "schedule": {"blocks_per_sm": bps, "grab": grab, "graph": bool(info["graph"]),
+                     "launches_per_replay": info["n_classes"],
+                     "mixing": "fixed" if args.batch_mixed >= 0 else "autotuned"},
         "gpu_launches": info["n_classes"], "clocks": clk, "cpu_baseline": None, "e2e": None})
 
 
@@ -412,9 +415,10 @@ def main():
                     help="single: one beam (--config); batch: the size-effect series in one "
                          "persistent batch launch; serve: a Poisson stream of solves, continuous batching")
     ap.add_argument("--members", type=int, default=64, help="batch: beams in the size-effect series")
-    ap.add_argument("--dx", type=float, default=5e-3, help="batch: lattice spacing of the series (m)")
+    ap.add_argument("--dx", type=float, default=2.5e-3, help="batch: lattice spacing of the series (m)")
     ap.add_argument("--batch-schedule", default="", help="batch: 'blocks_per_sm,grab' instead of autotuning")
-    ap.add_argument("--batch-mixed", type=int, default=1, help="batch: 1 one launch for all laws, 0 one per law")
+    ap.add_argument("--batch-mixed", type=int, default=-1,
+                    help="batch: 1 one launch for all laws, 0 one per law, -1 the autotuner chooses")
     ap.add_argument("--no-sequential", action="store_true", help="batch: skip the one-beam-at-a-time baseline")
     ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")
     ap.add_argument("--max-nodes", type=float, default=3e5, help="serve: largest beam (nodes)")
