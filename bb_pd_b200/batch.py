@@ -46,8 +46,9 @@ class Batch:
         N.check(N.lib().bbpd_batch_set_schedule(self._h, blocks_per_sm, grab, int(use_graph)))
 
     def set_mixing(self, mixed: bool) -> None:
-        """True (default): all laws in one launch per kernel variant; False: one
-        specialised launch per law and critical-stretch form."""
+        """True: all laws in one launch per kernel variant; False (the default
+        until tune() or this call chooses): one specialised launch per law and
+        critical-stretch form."""
         N.check(N.lib().bbpd_batch_set_mixing(self._h, int(mixed)))
 
     def info(self) -> dict:

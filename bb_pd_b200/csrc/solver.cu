@@ -4099,7 +4099,7 @@ struct bbpd_batch {
     int64_t total = 0;
     double timeout_s = 2.0;
     bool use_graph = true;                 // replay the launches from a captured CUDA graph
-    bool mixed = true;                     // all laws of a precision variant in one launch
+    bool mixed = false;                    // true: all laws of a precision variant in one launch
     bool mixing_fixed = false;             // set by bbpd_batch_set_mixing; else the tuner chooses
     cudaGraphExec_t gexec = nullptr;
     int64_t g_nsteps = -1;
@@ -4223,8 +4223,8 @@ extern "C" int bbpd_batch_remove(bbpd_batch *B, bbpd_solver *S)
 }
 
 // Class tables (member descriptors, slice prefix, step numbers) of the
-// current membership, members grouped by (precision variant, law) in the
-// order they joined.
+// current membership: one class per precision variant (and per law and
+// critical-stretch form when mixing is off), members in the order they joined.
 static int batch_rebuild(bbpd_batch *B)
 {
     std::vector<BatchClass> old;

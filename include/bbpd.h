@@ -566,16 +566,18 @@ int bbpd_batch_remove(bbpd_batch *b, bbpd_solver *s);
 /* Advance every member by nsteps in one launch, then synchronize. */
 int bbpd_batch_step(bbpd_batch *b, int64_t nsteps);
 /* Autotuner: time candidate schedules (resident blocks per SM x slices per
- * grab), each on nsteps_per_trial real steps of the members, and keep the
- * fastest. */
+ * grab and, unless bbpd_batch_set_mixing fixed it, one launch for all laws or
+ * one per law), each on nsteps_per_trial real steps of the members, and keep
+ * the fastest. */
 int bbpd_batch_tune(bbpd_batch *b, int64_t nsteps_per_trial, int *blocks_per_sm, int *grab);
 int bbpd_batch_set_schedule(bbpd_batch *b, int blocks_per_sm, int grab, int use_graph);
 int bbpd_batch_get_info(bbpd_batch *b, bbpd_batch_info *info);
-/* Mixing (the default, 1): members of every law, with or without a per-entry
- * critical stretch, step in one persistent launch per kernel precision
- * variant, each slice taking its member's law. 0: one launch per law and
- * critical-stretch form, each specialised to it. The reference's batch is
- * the sequential loop over random-field realisations
+/* Mixing 1: members of every law, with or without a per-entry critical
+ * stretch, step in one persistent launch per kernel precision variant, each
+ * slice taking its member's law. 0 (the default until the autotuner or this
+ * call chooses): one launch per law and critical-stretch form, each
+ * specialised to it. The reference's batch is the sequential loop over
+ * random-field realisations
  * (randomfield/dynamicsolverdisplacementcontrolledRF.m:20). */
 int bbpd_batch_set_mixing(bbpd_batch *b, int mixed);
 int bbpd_batch_last_kernel_ms(bbpd_batch *b, float *ms);
