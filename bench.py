@@ -76,12 +76,12 @@ def fp64_peak():
     return v.value
 
 
-def measured_traffic(cfg, form):
+def measured_traffic(cfg, form, node_order):
     """DRAM bytes (read + write) per time step of the step kernel from an ncu
     capture of this workload (profiles/step_kernel_traffic.json), or None."""
     try:
         with open(os.path.join(ROOT, "profiles", "step_kernel_traffic.json")) as f:
-            t = json.load(f)[cfg][form]
+            t = json.load(f)[cfg][form][node_order]
         return float(t["dram_bytes_per_step"]), t.get("source")
     except Exception:
         return None, None
@@ -544,7 +544,7 @@ def main():
     peak, peak_kind = peak_hbm()
     alg = algorithmic_bytes(nN, nB, per_bond_sc)
     achieved = alg / (ms_step / 1e3) / 1e9
-    traffic, tsrc = measured_traffic(args.config, args.form)
+    traffic, tsrc = measured_traffic(args.config, args.form, args.node_order)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic, "traffic_source": tsrc, "per": "time step",
                 "algorithmic_bytes_per_step": alg, "layout_bytes_per_step": info["bytes_per_step"]}
