@@ -87,6 +87,18 @@ def measured_traffic(cfg, form, node_order):
         return None, None
 
 
+def batch_traffic(form, mixed, bonds):
+    """DRAM bytes per step of the batch launches, from the bytes per
+    bond-update of an ncu capture of a smaller batch of the same series
+    (profiles/batch_kernel_traffic.json) times the run's bonds, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "batch_kernel_traffic.json")) as f:
+            t = json.load(f)[form]["mixed" if mixed else "per_law"]
+        return float(t["dram_bytes_per_bond_update"]) * bonds, t.get("source")
+    except Exception:
+        return None, None
+
+
 def max_over_ranks(x, dist, device=None):
     """The largest of every rank's x (every rank gets it); x itself without a
     process group. Timings of a multi-GPU run are the slowest rank's."""
@@ -251,6 +263,7 @@ def run_batch(args):
     peak, kind = peak_hbm()
     alg = sum(algorithmic_bytes(n, b, True) for n, b in zip(nodes, bonds))
     ach = alg / (ms / args.steps / 1e3) / 1e9
+    traffic, tsrc = batch_traffic(args.form, info["n_classes"] == 1 and len(set(l for _, l in series)) > 1, tot_b)
     config = {"workload": f"size-effect series: {args.members} beams, depth 50-400 mm log-uniform, span/depth 5, "
                           f"width 50 mm, dx {args.dx * 1e3:g} mm, linear/trilinear, lognormal sc, ADR, "
                           f"1e-7 mm/step", "nodes": int(sum(nodes)), "bonds": int(tot_b),
@@ -263,7 +276,8 @@ def run_batch(args):
                                   "ms_per_step": seq_ms / args.steps if seq else None},
         "speedup_vs_sequential_fp64": value / seq if seq else None,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                     "peak_kind": peak_kind_str(kind), "traffic": None},
+                     "peak_kind": peak_kind_str(kind), "traffic": traffic, "traffic_source": tsrc,
+                     "per": "time step of the whole batch"},
         "schedule": {"blocks_per_sm": bps, "grab": grab, "graph": bool(info["graph"]),
                      "launches_per_replay": info["n_classes"],
                      "mixing": "fixed" if args.batch_mixed >= 0 else "autotuned"},
