@@ -626,15 +626,14 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
         if (g + kPrefetch < ng) prefetch_group<CID, SCE>(d, e0 + 128 * kPrefetch);
         if (g + 1 < ng) load_group<CID>(d, e0 + 128, Gn);
         const int nq = min(4, dg - 4 * g);
+        // Slots past the lane's list are layout padding (all streams zero):
+        // they name node 0 and dictionary entry 0, so every slot gathers a
+        // valid record and the pass below needs no per-slot selects.
         double xj[4], yj[4], zj[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            if (q < nq) {
-                const uint32_t j = group_w(Gc, q) & COL_MASK;
-                load_pos(xa + j, xj[q], yj[q], zj[q]);
-            } else {   // unused slot: finite values for the branch-free pass
-                xj[q] = xi + 1.0; yj[q] = yi; zj[q] = zi;
-            }
+            const uint32_t j = group_w(Gc, q) & COL_MASK;
+            load_pos(xa + j, xj[q], yj[q], zj[q]);
         }
         // pass 1: the fast path of all entries of the group, without
         // branches, so that the four dependency chains interleave
@@ -643,7 +642,7 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const bool valid = q < nq;
-            const uint32_t w = group_w(Gc, q), c = valid ? Gc.cid(q) : 0u, sv = (Gc.s >> (8 * q)) & 0xFFu;
+            const uint32_t w = group_w(Gc, q), c = Gc.cid(q), sv = (Gc.s >> (8 * q)) & 0xFFu;
             const DictEntry g = ldg_dict(d.dict, c);
             const double scv = has_sce<SCE>(d) ? __ldcs(d.sce + e0 + q) : d.P.sc;
             const double s0b = d.s0e ? __ldg(d.s0e + e0 + q) : d.P.s0;
@@ -660,7 +659,16 @@ __device__ __forceinline__ void slice_forces(const Dev &d, int64_t sl, int lane,
             fz[q] = t * quot_rn(dZ, L, rL);
             if (valid && !fast) slow |= 1u << q;
         }
-        // pass 2: the rare general entries, and the sum in the reference's order
+        // pass 2: the sum in the reference's order. A full group with no
+        // general entry and no chunk start (nearly every group) adds its four
+        // forces straight; otherwise each entry is taken in turn.
+        const uint32_t chunk = (Gc.w.x | Gc.w.y | Gc.w.z | Gc.w.w) & F_CHUNK;
+        if (nq == 4 && (slow | chunk) == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) { ax = ax + fx[q]; ay = ay + fy[q]; az = az + fz[q]; }
+            Gc = Gn;
+            continue;
+        }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             if (q < nq) {
@@ -733,18 +741,14 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
         if (g + kPrefetch < ng) prefetch_group<CID, SCE>(d, e0 + 128 * kPrefetch);
         if (g + 1 < ng) load_group<CID>(d, e0 + 128, Gn);
         const int nq = min(4, dg - 4 * g);
+        // padding slots name node 0 and dictionary entry 0 (see slice_forces)
         float4 uj[4];
         float2 lj[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            if (q < nq) {
-                const uint32_t j = group_w(Gc, q) & COL_MASK;
-                uj[q] = urh[j];
-                lj[q] = url[j];
-            } else {   // unused slot: finite values for the branch-free pass
-                uj[q] = ui;
-                lj[q] = li;
-            }
+            const uint32_t j = group_w(Gc, q) & COL_MASK;
+            uj[q] = urh[j];
+            lj[q] = url[j];
         }
         // pass 1: the fast path of all entries of the group, without branches,
         // so that the four dependency chains interleave
@@ -754,7 +758,7 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
         for (int q = 0; q < 4; q++) {
             const bool valid = q < nq;
             const int64_t e = e0 + q;
-            const uint32_t w = group_w(Gc, q), c = valid ? Gc.cid(q) : 0u, sv = (Gc.s >> (8 * q)) & 0xFFu;
+            const uint32_t w = group_w(Gc, q), c = Gc.cid(q), sv = (Gc.s >> (8 * q)) & 0xFFu;
             const int bt = (w >> BT_SHIFT) & 3;
             float4 A, Bv;
             ldg_dictx(d.dictx, c, A, Bv);
@@ -786,7 +790,17 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
             fzq[q] = qf * ez;
             if (valid && !fast) slow |= 1u << q;
         }
-        // pass 2: the rare general entries, and the sum in the reference's order
+        // pass 2: the sum in the reference's order; a full group with no
+        // general entry and no chunk start adds its four forces straight
+        const uint32_t chunk = (Gc.w.x | Gc.w.y | Gc.w.z | Gc.w.w) & F_CHUNK;
+        if (nq == 4 && (slow | chunk) == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                ax = ax + (double)fxq[q]; ay = ay + (double)fyq[q]; az = az + (double)fzq[q];
+            }
+            Gc = Gn;
+            continue;
+        }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             if (q < nq) {
