@@ -141,6 +141,8 @@ struct Dev {
     float4 *urh0, *urh1;             // FP32 form: per node (uh_x, uh_y, uh_z, ul_x), ping-pong like positions
     float2 *url0, *url1;             // FP32 form: per node (ul_y, ul_z); uh + ul is the FP32 split of u
     const double *s0e, *s1e, *sce;   // per-entry law stretches or null
+    double s0q;                      // FP32 fast path's s0: the scalar s0, or the least per-entry s0
+                                     // (entries above it take the general path, which reads their own)
     double *smax;                    // damage-energy tracking: largest stretch of each concrete entry past s0, or null
     const double *X;
     double *xb0, *xb1;               // positions: step n reads xb[(n-1)&1], writes xb[n&1]
@@ -715,7 +717,11 @@ __device__ __forceinline__ double3 entry_general_x(const Dev &d, int64_t e, uint
 // FP64 in the reference's order. Bonds whose stretch lies within the guard band
 // of the critical stretch, damaged or broken bonds and bonds whose law is active
 // take the general path with FP64 positions.
-template <int LAW, class CID, int SCE>
+// PF: L2 prefetch of the streams ahead of the next group's loads. The single-
+// beam kernel runs faster without it (0.731 against 0.773 ms/step on the
+// 1.28M-node beam), the batch kernel with it (0.897 against 1.020 ms/step on a
+// 16-beam batch).
+template <int LAW, class CID, int SCE, bool PF>
 __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lane, const double *xs,
                                                const float4 *urh, const float2 *url, double &tx,
                                                double &ty, double &tz)
@@ -730,7 +736,7 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
     if (i < nN) { ui = urh[i]; li = url[i]; }
     tx = 0.0; ty = 0.0; tz = 0.0;
     double ax = 0.0, ay = 0.0, az = 0.0;
-    const float s0f = (float)d.P.s0, guardf = (float)d.guard, scf0 = (float)d.P.sc;
+    const float s0f = (float)d.s0q, guardf = (float)d.guard, scf0 = (float)d.P.sc;
     const float steelf = (float)d.P.sc_steel;
 
     const int ng = (dg + 3) >> 2;
@@ -738,7 +744,7 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
     int64_t e0 = entry_pos(sb, 0, lane);
     if (ng > 0) load_group<CID>(d, e0, Gc);
     for (int g = 0; g < ng; g++, e0 += 128) {
-        if (g + kPrefetch < ng) prefetch_group<CID, SCE>(d, e0 + 128 * kPrefetch);
+        if (PF && g + kPrefetch < ng) prefetch_group<CID, SCE>(d, e0 + 128 * kPrefetch);
         if (g + 1 < ng) load_group<CID>(d, e0 + 128, Gn);
         const int nq = min(4, dg - 4 * g);
         // padding slots name node 0 and dictionary entry 0 (see slice_forces)
@@ -780,7 +786,7 @@ __device__ __forceinline__ void slice_forces_x(const Dev &d, int64_t sl, int lan
                 const float critf = (bt == 0) ? scf : (bt == 1 ? 3.f * scf : steelf);
                 fast = sf <= __fsub_rd(critf, guardf);
             } else {
-                const float top = (bt == 0) ? (d.s0e ? (float)__ldg(d.s0e + e) : s0f) : INFINITY;
+                const float top = (bt == 0) ? s0f : INFINITY;
                 fast = sf <= top && (sf <= __fsub_rd(scf, guardf) || sf >= __fadd_ru(scf, guardf));
             }
             fast = fast && sv == 0 && Bv.z != 0.f;
@@ -1123,12 +1129,12 @@ __global__ void __launch_bounds__(kBlock, PREC == kP32X ? BBPD_MIN_BLOCKS_F32 : 
         // slice indices only, not on which warp computes a slice.
         const int64_t base = it * (nsl + nwarps);
         int64_t sl = grab_slice(d, lane) - base;
-        prefetch_slice_head<CID, SCE>(d, sl, lane);
+        if (PREC != kP32X) prefetch_slice_head<CID, SCE>(d, sl, lane);   // FP32: see slice_forces_x
         while (sl < nsl) {
             const int64_t sl_next = grab_slice(d, lane) - base;
-            prefetch_slice_head<CID, SCE>(d, sl_next, lane);
+            if (PREC != kP32X) prefetch_slice_head<CID, SCE>(d, sl_next, lane);
             double tx, ty, tz;
-            if (PREC == kP32X) slice_forces_x<LAW, CID, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
+            if (PREC == kP32X) slice_forces_x<LAW, CID, SCE, false>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
             else slice_forces<LAW, PREC, CID, SCE>(d, sl, lane, safe, b.xs, b.xas, tx, ty, tz);
             finish_slice<SCHEME, PREC>(d, b, sl, lane, tx, ty, tz, it);
             sl = sl_next;
@@ -1266,7 +1272,7 @@ __device__ __forceinline__ void tslice_forces_x(const Dev &d, int64_t sl, int li
     if (dg > 0) { ui = suh[li]; vi = sul[li]; }
     tx = 0.0; ty = 0.0; tz = 0.0;
     double ax = 0.0, ay = 0.0, az = 0.0;
-    const float s0f = (float)d.P.s0, guardf = (float)d.guard;
+    const float s0f = (float)d.s0q, guardf = (float)d.guard;
     const int ng = (dg + 3) >> 2;
     TGroup Gc, Gn;
     int64_t e0 = entry_pos(sb, 0, lane);
@@ -1298,7 +1304,7 @@ __device__ __forceinline__ void tslice_forces_x(const Dev &d, int64_t sl, int li
                 const float num = __fmaf_rn(etz, A.z + ez, __fmaf_rn(ety, A.y + ey, __fmaf_rn(etx, A.x + ex, Bv.y)));
                 const float sf = __fdividef(num, A.w * (L + A.w));
                 const float crit = (float)((LAW == BBPD_LAW_LINEAR) ? linear_crit(d.P, bt, scd) : scd);
-                const float s0b = d.s0e ? (float)__ldg(d.s0e + e) : s0f;
+                const float s0b = s0f;   // least per-entry s0: entries above it take the general path
                 const bool quiet = (LAW == BBPD_LAW_LINEAR) ? !(sf > crit) : !(bt == 0 && sf > s0b);
                 double3 r;
                 if (sv == 0 && Bv.z != 0.f && L2 > 0.f && L2 < INFINITY && !(fabsf(sf - crit) < guardf) && quiet) {
@@ -1716,7 +1722,7 @@ __global__ void __launch_bounds__(kBlock, BBPD_MIN_BLOCKS) batch_kernel(BatchCtl
                 const StepBufs b = step_bufs(d, __ldg(&B.mstep[m]) + it);
                 const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
                 double tx, ty, tz;
-                if (PREC == kP32X) slice_forces_x<LAW, uint16_t, SCE>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
+                if (PREC == kP32X) slice_forces_x<LAW, uint16_t, SCE, true>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
                 else slice_forces<LAW, PREC, uint16_t, SCE>(d, sl, lane, safe, b.xs, b.xas, tx, ty, tz);
                 finish_slice<BBPD_SCHEME_ADR, PREC>(d, b, sl, lane, tx, ty, tz, it);
             }
@@ -1747,7 +1753,7 @@ __device__ __noinline__ void mixed_law_slice(const Dev &d, const StepBufs &b, in
 {
     const bool safe = (*(volatile unsigned *)d.sticky & 1u) == 0;
     double tx, ty, tz;
-    if (PREC == kP32X) slice_forces_x<LAW, uint16_t, 2>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
+    if (PREC == kP32X) slice_forces_x<LAW, uint16_t, 2, true>(d, sl, lane, b.xs, b.urhs, b.urls, tx, ty, tz);
     else slice_forces<LAW, PREC, uint16_t, 2>(d, sl, lane, safe, b.xs, b.xas, tx, ty, tz);
     finish_slice<BBPD_SCHEME_ADR, PREC>(d, b, sl, lane, tx, ty, tz, it);
 }
@@ -3648,6 +3654,16 @@ extern "C" int bbpd_create(const bbpd_problem *pb, const bbpd_params *prm, int d
     // scalars
     LawScalars &P = d.P;
     P.s0 = prm->s0; P.s1 = prm->s1; P.sc = prm->sc;
+    // FP32 fast-path s0: an entry whose stretch exceeds the least per-bond s0
+    // goes to the general path, which reads its own s0 (NaN values are
+    // skipped; an all-NaN array gives NaN, which like each NaN s0 keeps every
+    // entry quiet)
+    d.s0q = prm->s0;
+    if (pb->s0 && nB > 0) {
+        double m = NAN;
+        for (int64_t k = 0; k < nB; k++) m = std::fmin(m, pb->s0[k]);
+        d.s0q = m;
+    }
     P.beta = prm->beta_tri;
     double eta = prm->s1 / prm->s0;
     P.tri_c1 = (eta - P.beta) / (eta - 1);
