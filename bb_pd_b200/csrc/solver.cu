@@ -718,7 +718,7 @@ __device__ __forceinline__ double3 entry_general_x(const Dev &d, int64_t e, uint
 // of the critical stretch, damaged or broken bonds and bonds whose law is active
 // take the general path with FP64 positions.
 // PF: L2 prefetch of the streams ahead of the next group's loads. The single-
-// beam kernel runs faster without it (0.731 against 0.773 ms/step on the
+// beam kernel runs faster without it (0.72 against 0.77 ms/step on the
 // 1.28M-node beam), the batch kernel with it (0.897 against 1.020 ms/step on a
 // 16-beam batch).
 template <int LAW, class CID, int SCE, bool PF>
